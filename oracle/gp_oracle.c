@@ -1,0 +1,1153 @@
+/*
+ * gp_oracle.c -- CPU restatement of the gPLUTO Godunov step (TEST
+ * INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+ * bench's cpu_baseline leg as the checker; never linked into the product).
+ *
+ * Plain C, straight loops over ghost-zone arrays, in the reference's own
+ * operation order so that results agree bit for bit with the reference
+ * serial build (Config/linux.g++.defs, g++ -O3 on x86-64 without FMA
+ * contraction).  Compile with -ffp-contract=off and no fast-math.
+ *
+ * Scope: Cartesian uniform grid, periodic boundaries, PLM reconstruction
+ * (MC / van Leer / minmod), RK2, ideal EOS, physics HD (HLLC, HLL),
+ * MHD (HLLD, HLL) with constrained transport (UCT_HLLD, UCT_HLL), RMHD
+ * (HLLD, HLL, UCT_HLL) with the Newton energy inversion.
+ *
+ * Each function cites the reference source it restates (paths relative to
+ * the gPLUTO tree).  Parity is pinned against the reference binary through
+ * the committed fixtures in tests/golden/.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "gp_oracle.h"
+
+#define MAX(a,b)  ( (a) >= (b) ? (a) : (b) )      /* Src/macros.hpp:188 */
+#define MIN(a,b)  ( (a) <= (b) ? (a) : (b) )      /* Src/macros.hpp:191 */
+#define ABS_MIN(a,b)  (fabs(a) < fabs(b) ? (a):(b))   /* Src/macros.hpp:14 */
+#define MINMOD_LIMITER(a,b)  ((a)*(b) > 0.0 ? (fabs(a) < fabs(b) ? (a):(b)):0.0)
+
+/* variable indices: MHD/RMHD (Src/MHD/mhd.hpp:21-33), HD (Src/HD/hd.hpp:21-27) */
+enum { RHO = 0, MX1 = 1, MX2 = 2, MX3 = 3, BX1 = 4, BX2 = 5, BX3 = 6 };
+#define VX1 MX1
+
+/* error bits, Src/gpluto.hpp:247-262 */
+#define ERR_NEGATIVE_RHO   (1u<<0)
+#define ERR_NEGATIVE_ENG   (1u<<1)
+#define ERR_NEGATIVE_PRS   (1u<<2)
+#define ERR_CONS2PRIM_FAIL (1u<<4)
+#define ERR_ENG_SOLVE_INACCURATE  (1u<<6)
+#define ERR_ENG_SOLVE_NO_SOLUTION (1u<<7)
+#define ERR_SUPERLUMINAL_SPEED    (1u<<8)
+#define ERR_TOO_MANY_ITERATIONS   (1u<<9)
+#define ERR_NAN            (1u<<11)
+#define ERR_QUIT           (1u<<15)
+
+typedef struct {
+  orc_cfg c;
+  int nvar, eng, ng;
+  int nt[3], beg[3], end[3];
+  long ncell;
+  double *Vc, *Uc, *U0, *Rc, *Cdt;
+  double *Vs[3], *Bs0[3], *Rs[3];
+  int ns[3][3];
+  /* CT face data, indexed on a (nt+1)^3 box */
+  int ne[3];
+  double *e[3][3], *aL[3], *aR[3], *dL[3], *dR[3], *Ee[3];
+  /* pencil buffers */
+  int pmax;
+  double *pv, *pvL, *pvR, *pflux, *pcmax, *pBn, *pq, *pqL, *pqR;
+  uint32_t err;
+} orc_t;
+
+static void orc_rmhd_init(orc_t *o);
+static double orc_rmhd_riemann(orc_t *o, int dir, double *vl, double *vr, double *f, long e);
+static uint32_t orc_rmhd_cons_to_prim(orc_t *o, double *u, double *v, int i, int j, int k);
+static void orc_rmhd_prim_to_cons(const double *v, double *u, double gamma);
+
+/* ------------------------------------------------------------------ */
+/* indexing                                                            */
+/* ------------------------------------------------------------------ */
+static inline long CI(const orc_t *o, int i, int j, int k) {
+  return ((long)k*o->nt[1] + j)*o->nt[0] + i;
+}
+static inline double *VC(orc_t *o, double *A, int nv, int i, int j, int k) {
+  return A + (long)nv*o->ncell + CI(o, i, j, k);
+}
+static inline long SI(const orc_t *o, int d, int i, int j, int k) {
+  return ((long)k*o->ns[d][1] + j)*o->ns[d][0] + i;
+}
+static inline long EI(const orc_t *o, int i, int j, int k) {
+  return ((long)k*o->ne[1] + j)*o->ne[0] + i;
+}
+/* map pencil coordinates (along dir) to (i,j,k): Src/macros.hpp ARRAY_STRIDES,
+   RBoxPermuteIndices (dir=IDIR: (i,j,k); JDIR: (j,i,k); KDIR: (j,k,i)) */
+static inline void TrueIdx(int dir, int i, int t1, int t2, int *ti, int *tj, int *tk) {
+  if (dir == 0) { *ti = i;  *tj = t1; *tk = t2; }
+  else if (dir == 1) { *ti = t1; *tj = i;  *tk = t2; }
+  else { *ti = t1; *tj = t2; *tk = i; }
+}
+
+/* ------------------------------------------------------------------ */
+/* physics: MHD                                                        */
+/* ------------------------------------------------------------------ */
+
+/* Src/MHD/mhd.hpp:906-948 */
+static void MHD_PrimToCons(const double *v, double *u, double gamma) {
+  double gmm1 = gamma - 1.0, kinb2;
+  u[RHO] = v[RHO];
+  u[MX1] = v[RHO]*v[VX1];
+  u[MX2] = v[RHO]*v[VX1+1];
+  u[MX3] = v[RHO]*v[VX1+2];
+  u[BX1] = v[BX1]; u[BX2] = v[BX2]; u[BX3] = v[BX3];
+  kinb2  = v[VX1]*v[VX1] + v[VX1+1]*v[VX1+1] + v[VX1+2]*v[VX1+2];
+  kinb2  = v[RHO]*kinb2  + v[BX1]*v[BX1] + v[BX2]*v[BX2] + v[BX3]*v[BX3];
+  kinb2 *= 0.5;
+  u[7] = kinb2 + v[7]/gmm1;
+}
+
+/* Src/HD/hd.hpp:392-416 */
+static void HD_PrimToCons(const double *v, double *u, double gamma) {
+  double kin;
+  u[RHO] = v[RHO];
+  u[MX1] = v[RHO]*v[VX1];
+  u[MX2] = v[RHO]*v[VX1+1];
+  u[MX3] = v[RHO]*v[VX1+2];
+  kin    = v[VX1]*v[VX1] + v[VX1+1]*v[VX1+1] + v[VX1+2]*v[VX1+2];
+  kin    = v[RHO]*kin*0.5;
+  u[4]   = kin + v[4]/(gamma - 1.0);
+}
+
+/* Src/MHD/mappers.cpp:32-150 (ENERGY_SOLVE branch) */
+static uint32_t MHD_ConsToPrim(double *u, double *v, double gamma, double small_rho, double small_prs) {
+  uint32_t err = 0;
+  double gmm1 = gamma - 1.0, tau, m2, b2, kinb2;
+  if (u[RHO] < 0.0) { u[RHO] = small_rho; err |= ERR_NEGATIVE_RHO | ERR_CONS2PRIM_FAIL; }
+  v[RHO] = u[RHO];
+  tau    = 1.0/u[RHO];
+  v[VX1]   = u[MX1]*tau;
+  v[VX1+1] = u[MX2]*tau;
+  v[VX1+2] = u[MX3]*tau;
+  v[BX1] = u[BX1]; v[BX2] = u[BX2]; v[BX3] = u[BX3];
+  m2 = u[MX1]*u[MX1] + u[MX2]*u[MX2] + u[MX3]*u[MX3];
+  b2 = u[BX1]*u[BX1] + u[BX2]*u[BX2] + u[BX3]*u[BX3];
+  kinb2 = 0.5*(m2*tau + b2);
+  if (u[7] > 0.0) {
+    v[7] = gmm1*(u[7] - kinb2);
+    if (v[7] < 0.0) {
+      v[7] = small_prs;
+      u[7] = v[7]/gmm1 + kinb2;
+      err |= ERR_NEGATIVE_PRS;
+    }
+  } else {
+    u[7] = small_prs/gmm1 + kinb2;
+    v[7] = small_prs;
+    err |= ERR_NEGATIVE_ENG;
+  }
+  return err;
+}
+
+/* Src/HD/mappers.cpp:33-140 (ENERGY_SOLVE branch) */
+static uint32_t HD_ConsToPrim(double *u, double *v, double gamma, double small_rho, double small_prs) {
+  uint32_t err = 0;
+  double gmm1 = gamma - 1.0, tau, m2, kin;
+  if (u[RHO] < 0.0) { u[RHO] = small_rho; err |= ERR_NEGATIVE_RHO | ERR_CONS2PRIM_FAIL; }
+  v[RHO] = u[RHO];
+  tau    = 1.0/u[RHO];
+  v[VX1]   = u[MX1]*tau;
+  v[VX1+1] = u[MX2]*tau;
+  v[VX1+2] = u[MX3]*tau;
+  m2  = u[MX1]*u[MX1] + u[MX2]*u[MX2] + u[MX3]*u[MX3];
+  kin = 0.5*m2*tau;
+  if (u[4] > 0.0) {
+    v[4] = gmm1*(u[4] - kin);
+    if (v[4] < 0.0) {
+      v[4] = small_prs;
+      u[4] = v[4]/gmm1 + kin;
+      err |= ERR_NEGATIVE_PRS;
+    }
+  } else {
+    u[4] = small_prs/gmm1 + kin;
+    v[4] = small_prs;
+    err |= ERR_NEGATIVE_ENG;
+  }
+  return err;
+}
+
+/* Src/MHD/mhd.hpp:163-223 (no background field) */
+static void MHD_Flux(int dir, const double *v, const double *u, double *flux, double *pt) {
+  int VXn = VX1 + dir, BXn = BX1 + dir, MXn = MX1 + dir;
+  double vB = v[VX1]*v[BX1] + v[VX1+1]*v[BX2] + v[VX1+2]*v[BX3];
+  *pt = v[7] + 0.5*(v[BX1]*v[BX1] + v[BX2]*v[BX2] + v[BX3]*v[BX3]);
+  flux[RHO] = u[MXn];
+  flux[MX1] = u[MX1]*v[VXn] - v[BX1]*v[BXn];
+  flux[MX2] = u[MX2]*v[VXn] - v[BX2]*v[BXn];
+  flux[MX3] = u[MX3]*v[VXn] - v[BX3]*v[BXn];
+  flux[BX1] = v[BX1]*v[VXn] - v[BXn]*v[VX1];
+  flux[BX2] = v[BX2]*v[VXn] - v[BXn]*v[VX1+1];
+  flux[BX3] = v[BX3]*v[VXn] - v[BXn]*v[VX1+2];
+  flux[7]   = (u[7] + *pt)*v[VXn] - v[BXn]*vB;
+  flux[MXn] += *pt;
+}
+
+/* Src/HD/hd.hpp:105-125 */
+static void HD_Flux(int dir, const double *v, const double *u, double *flux, double *p) {
+  int VXn = VX1 + dir, MXn = MX1 + dir;
+  flux[RHO] = u[MXn];
+  flux[MX1] = u[MX1]*v[VXn];
+  flux[MX2] = u[MX2]*v[VXn];
+  flux[MX3] = u[MX3]*v[VXn];
+  flux[4] = (u[4] + v[4])*v[VXn];
+  *p = v[4];
+  flux[MXn] += *p;
+}
+
+/* Src/MHD/mhd.hpp:241-277 (MaxSignalSpeed) with a2 from Src/eos.hpp:96 */
+static void MHD_MaxSignalSpeed(int dir, const double *v, double a2, double *cmin, double *cmax) {
+  int VXn = VX1 + dir;
+  double b1 = v[BX1 + dir], b2 = v[BX1 + (dir+1)%3], b3 = v[BX1 + (dir+2)%3];
+  double gpr = a2*v[RHO];
+  double Btmag2 = b2*b2 + b3*b3;
+  double Bmag2  = b1*b1 + Btmag2;
+  double cf = gpr - Bmag2;
+  cf = gpr + Bmag2 + sqrt(cf*cf + 4.0*gpr*Btmag2);
+  cf = sqrt(0.5*cf/v[RHO]);
+  *cmax = v[VXn] + cf;
+  *cmin = v[VXn] - cf;
+}
+
+/* Src/HD/hd.hpp:139-150 */
+static void HD_MaxSignalSpeed(int dir, const double *v, double a2, double *cmin, double *cmax) {
+  double a = sqrt(a2);
+  *cmax = v[VX1+dir] + a;
+  *cmin = v[VX1+dir] - a;
+}
+
+/* ------------------------------------------------------------------ */
+/* CT store (Src/MHD/CT/ct_store.hpp)                                  */
+/* ------------------------------------------------------------------ */
+
+/* Src/MHD/CT/ct_store.hpp:154-177 */
+static void CT_Store_UCTHll(orc_t *o, int dir, const double *vl, const double *vr,
+                            double Sl, double Sr, long e) {
+  int VXt = VX1 + (dir+1)%3, VXb = VX1 + (dir+2)%3;
+  int DIRt = (dir+1)%3, DIRb = (dir+2)%3;
+  double aR_1 = MAX(0.0, Sr);
+  double aL_1 = MIN(0.0, Sl);
+  double scrh = 1.0/(aR_1 - aL_1);
+  o->e[DIRb][dir][e] =  (aR_1*vl[VXt] - aL_1*vr[VXt])*scrh;
+  o->e[DIRt][dir][e] = -(aR_1*vl[VXb] - aL_1*vr[VXb])*scrh;
+  o->aL[dir][e] =  aR_1*scrh;
+  o->aR[dir][e] = -aL_1*scrh;
+  o->dR[dir][e] = -aL_1*aR_1*scrh;
+  o->dL[dir][e] = -aL_1*aR_1*scrh;
+}
+
+/* Src/MHD/CT/ct_store.hpp:252-355 (EOS IDEAL) */
+static void CT_Store_UCTHlld(orc_t *o, int dir, const double *ul, const double *ur,
+                             const double *vl, const double *vr, double Sl, double Sr,
+                             double Bn, long e) {
+  int VXn = VX1 + dir, VXt = VX1 + (dir+1)%3, VXb = VX1 + (dir+2)%3;
+  int MXn = MX1 + dir;
+  int DIRt = (dir+1)%3, DIRb = (dir+2)%3;
+  int switch_to_hll = 0;
+  double scrh;
+  double aR_1 = MAX(0.0, Sr);
+  double aL_1 = MIN(0.0, Sl);
+  double dul = Sl - vl[VXn];
+  double dur = Sr - vr[VXn];
+  double pL = vl[7] + 0.5*(vl[BX1]*vl[BX1] + vl[BX2]*vl[BX2] + vl[BX3]*vl[BX3]);
+  double pR = vr[7] + 0.5*(vr[BX1]*vr[BX1] + vr[BX2]*vr[BX2] + vr[BX3]*vr[BX3]);
+  scrh  = 1.0/(dur*ur[RHO] - dul*ul[RHO]);
+  double Sc = (dur*ur[MXn] - dul*ul[MXn] - pR + pL)*scrh;
+  double usl_RHO = ul[RHO]*dul/(Sl - Sc);
+  double usr_RHO = ur[RHO]*dur/(Sr - Sc);
+  if (usl_RHO < 0.0 || usr_RHO < 0.0) switch_to_hll = 1;
+  double sqrL = sqrt(usl_RHO);
+  double sqrR = sqrt(usr_RHO);
+  double Sal = Sc - fabs(Bn)/sqrL;
+  double Sar = Sc + fabs(Bn)/sqrR;
+  double chiL  = (vl[VXn] - Sc)*(Sl - Sc)/(Sal + Sl - 2.0*Sc);
+  double chiR  = (vr[VXn] - Sc)*(Sr - Sc)/(Sar + Sr - 2.0*Sc);
+  double nuL  = (Sal + Sl)/(fabs(Sal) + fabs(Sl));
+  double nuR  = (Sar + Sr)/(fabs(Sar) + fabs(Sr));
+  double nuLR = (Sal + Sar)/(fabs(Sal) + fabs(Sar));
+  if (fabs(Sar - Sal) > 1.e-9*fabs(Sr-Sl)) {
+    o->dL[dir][e] = 0.5*(chiL*nuL - chiL*nuLR) + 0.5*(fabs(Sal) - nuLR*Sal);
+    o->dR[dir][e] = 0.5*(chiR*nuR - chiR*nuLR) + 0.5*(fabs(Sar) - nuLR*Sar);
+    o->aL[dir][e] = 0.5*(1.0 + nuLR);
+    o->aR[dir][e] = 0.5*(1.0 - nuLR);
+  } else {
+    o->dL[dir][e] = 0.5*chiL*nuL + 0.5*fabs(Sal);
+    o->dR[dir][e] = 0.5*chiR*nuR + 0.5*fabs(Sar);
+    o->aL[dir][e] = 0.5;
+    o->aR[dir][e] = 0.5;
+  }
+  scrh = 1.0/(aR_1 - aL_1);
+  if (switch_to_hll) {
+    o->aL[dir][e] =  aR_1*scrh;
+    o->aR[dir][e] = -aL_1*scrh;
+    o->dR[dir][e] = -aL_1*aR_1*scrh;
+    o->dL[dir][e] = -aL_1*aR_1*scrh;
+  }
+  o->e[DIRb][dir][e] =  (aR_1*vl[VXt] - aL_1*vr[VXt])*scrh;
+  o->e[DIRt][dir][e] = -(aR_1*vl[VXb] - aL_1*vr[VXb])*scrh;
+}
+
+/* ------------------------------------------------------------------ */
+/* Riemann solvers                                                     */
+/* ------------------------------------------------------------------ */
+
+/* Src/MHD/hlld.cpp:61-514 (ideal EOS, no background field, no GLM).
+   Returns cmax; writes flux[NVAR]. */
+static double MHD_HLLD(orc_t *o, int dir, double *vl, double *vr, double *flux, long e,
+                       double Bn_face) {
+  const double gamma = o->c.gamma;
+  int VXn = VX1 + dir, VXt = VX1 + (dir+1)%3, VXb = VX1 + (dir+2)%3;
+  int MXn = MX1 + dir, MXt = MX1 + (dir+1)%3, MXb = MX1 + (dir+2)%3;
+  int BXn = BX1 + dir, BXt = BX1 + (dir+1)%3, BXb = BX1 + (dir+2)%3;
+  int nv, switch_to_hll = 0;
+  double ul[8], ur[8], fl[8], fr[8], usl[8], usr[8], Uhll[8];
+  double Sl, Sr, ptl, ptr, sqrL, sqrR, cmax;
+
+  MHD_PrimToCons(vl, ul, gamma);
+  MHD_PrimToCons(vr, ur, gamma);
+  double a2L = gamma*vl[7]/vl[RHO];       /* Src/eos.hpp:96 */
+  double a2R = gamma*vr[7]/vr[RHO];
+  {
+    double sl_min, sl_max, sr_min, sr_max;  /* Src/MHD/mhd.hpp:295-308 */
+    MHD_MaxSignalSpeed(dir, vl, a2L, &sl_min, &sl_max);
+    MHD_MaxSignalSpeed(dir, vr, a2R, &sr_min, &sr_max);
+    Sl = MIN(sl_min, sr_min);
+    Sr = MAX(sl_max, sr_max);
+  }
+  cmax = MAX(fabs(Sl), fabs(Sr));
+  MHD_Flux(dir, vl, ul, fl, &ptl);
+  MHD_Flux(dir, vr, ur, fr, &ptr);
+
+  double dul, dur, Bx, Bx1, sBx, pts, SM;
+  {
+    double scrh = 1.0/(Sr - Sl);
+    Bx1 = Bx = (Sr*vr[BXn] - Sl*vl[BXn])*scrh;
+    sBx = (Bx > 0.0 ? 1.0 : -1.0);
+    dul = Sl - vl[VXn];
+    dur = Sr - vr[VXn];
+    scrh = 1.0/(dur*ur[RHO] - dul*ul[RHO]);
+    SM = (dur*ur[MXn] - dul*ul[MXn] - ptr + ptl)*scrh;
+    pts = dur*ur[RHO]*ptl - dul*ul[RHO]*ptr + vl[RHO]*vr[RHO]*dur*dul*(vr[VXn] - vl[VXn]);
+    pts *= scrh;
+  }
+  usl[RHO] = ul[RHO]*dul/(Sl - SM);
+  usr[RHO] = ur[RHO]*dur/(Sr - SM);
+  if (usl[RHO] < 0.0 || usr[RHO] < 0.0) switch_to_hll = 1;
+  sqrL = sqrt(usl[RHO]);
+  sqrR = sqrt(usr[RHO]);
+  double S1L = SM - fabs(Bx)/sqrL;
+  double S1R = SM + fabs(Bx)/sqrR;
+
+  if (Sl >= 0.0) {
+    for (nv = 0; nv < 8; nv++) flux[nv] = fl[nv];
+  } else if (Sr <= 0.0) {
+    for (nv = 0; nv < 8; nv++) flux[nv] = fr[nv];
+  } else {
+    if (!switch_to_hll) {
+      int switch_to_hllc = 0;
+      if ((S1L - Sl) <  1.e-4*(SM - Sl)) switch_to_hllc = 1;
+      if ((S1R - Sr) > -1.e-4*(Sr - SM)) switch_to_hllc = 1;
+      double scrhL, scrhR;
+      if (!switch_to_hllc) {
+        scrhL = (ul[RHO]*dul*dul - Bx*Bx)/(ul[RHO]*dul*(Sl - SM) - Bx*Bx);
+        scrhR = (ur[RHO]*dur*dur - Bx*Bx)/(ur[RHO]*dur*(Sr - SM) - Bx*Bx);
+        usl[BXn] = Bx1;
+        usl[BXt] = ul[BXt]*scrhL;
+        usl[BXb] = ul[BXb]*scrhL;
+        usr[BXn] = Bx1;
+        usr[BXt] = ur[BXt]*scrhR;
+        usr[BXb] = ur[BXb]*scrhR;
+      } else {
+        double scrh = 1.0/(Sr - Sl);
+        for (nv = 0; nv < 8; nv++) {
+          Uhll[nv]  = Sr*ur[nv] - Sl*ul[nv] + fl[nv] - fr[nv];
+          Uhll[nv] *= scrh;
+        }
+        usl[BXn] = usr[BXn] = Bx1;
+        usl[BXt] = usr[BXt] = Uhll[BXt];
+        usl[BXb] = usr[BXb] = Uhll[BXb];
+        S1L = S1R = SM;
+      }
+      scrhL = Bx/(ul[RHO]*dul);
+      scrhR = Bx/(ur[RHO]*dur);
+      double vsL = vl[VXt] - scrhL*(usl[BXt] - ul[BXt]);
+      double vsR = vr[VXt] - scrhR*(usr[BXt] - ur[BXt]);
+      double wsL = vl[VXb] - scrhL*(usl[BXb] - ul[BXb]);
+      double wsR = vr[VXb] - scrhR*(usr[BXb] - ur[BXb]);
+      usl[MXn] = usl[RHO]*SM;
+      usr[MXn] = usr[RHO]*SM;
+      usl[MXt] = usl[RHO]*vsL;
+      usr[MXt] = usr[RHO]*vsR;
+      usl[MXb] = usl[RHO]*wsL;
+      usr[MXb] = usr[RHO]*wsR;
+      scrhL  = vl[VXn]*Bx1 + vl[VXt]*ul[BXt] + vl[VXb]*ul[BXb];
+      scrhL -= SM*Bx1 + vsL*usl[BXt] + wsL*usl[BXb];
+      usl[7]  = dul*ul[7] - ptl*vl[VXn] + pts*SM + Bx*scrhL;
+      usl[7] /= Sl - SM;
+      scrhR  = vr[VXn]*Bx1 + vr[VXt]*ur[BXt] + vr[VXb]*ur[BXb];
+      scrhR -= SM*Bx1 + vsR*usr[BXt] + wsR*usr[BXb];
+      usr[7]  = dur*ur[7] - ptr*vr[VXn] + pts*SM + Bx*scrhR;
+      usr[7] /= Sr - SM;
+
+      if (S1L >= 0.0) {
+        for (nv = 0; nv < 8; nv++) flux[nv] = fl[nv] + Sl*(usl[nv] - ul[nv]);
+      } else if (S1R <= 0.0) {
+        for (nv = 0; nv < 8; nv++) flux[nv] = fr[nv] + Sr*(usr[nv] - ur[nv]);
+      } else {
+        double ussl[8], ussr[8];
+        ussl[RHO] = usl[RHO];
+        ussr[RHO] = usr[RHO];
+        double vss = sqrL*vsL + sqrR*vsR + (usr[BXt] - usl[BXt])*sBx;
+        vss /= sqrL + sqrR;
+        double wss = sqrL*wsL + sqrR*wsR + (usr[BXb] - usl[BXb])*sBx;
+        wss /= sqrL + sqrR;
+        ussl[MXn] = ussl[RHO]*SM;
+        ussr[MXn] = ussr[RHO]*SM;
+        ussl[MXt] = ussl[RHO]*vss;
+        ussr[MXt] = ussr[RHO]*vss;
+        ussl[MXb] = ussl[RHO]*wss;
+        ussr[MXb] = ussr[RHO]*wss;
+        ussl[BXn] = ussr[BXn] = Bx1;
+        ussl[BXt]  = sqrL*usr[BXt] + sqrR*usl[BXt] + sqrL*sqrR*(vsR - vsL)*sBx;
+        ussl[BXt] /= sqrL + sqrR;
+        ussr[BXt]  = ussl[BXt];
+        ussl[BXb]  = sqrL*usr[BXb] + sqrR*usl[BXb] + sqrL*sqrR*(wsR - wsL)*sBx;
+        ussl[BXb] /= sqrL + sqrR;
+        ussr[BXb]  = ussl[BXb];
+        scrhL  = SM*Bx1 + vsL*usl [BXt] + wsL*usl [BXb];
+        scrhL -= SM*Bx1 + vss*ussl[BXt] + wss*ussl[BXb];
+        scrhR  = SM*Bx1 + vsR*usr [BXt] + wsR*usr [BXb];
+        scrhR -= SM*Bx1 + vss*ussr[BXt] + wss*ussr[BXb];
+        ussl[7] = usl[7] - sqrL*scrhL*sBx;
+        ussr[7] = usr[7] + sqrR*scrhR*sBx;
+        if (SM >= 0.0) {
+          for (nv = 0; nv < 8; nv++)
+            flux[nv] = fl[nv] + S1L*(ussl[nv] - usl[nv]) + Sl*(usl[nv] - ul[nv]);
+        } else {
+          for (nv = 0; nv < 8; nv++)
+            flux[nv] = fr[nv] + S1R*(ussr[nv] - usr[nv]) + Sr*(usr[nv] - ur[nv]);
+        }
+      }
+    } else {
+      double scrh = 1.0/(Sr - Sl);
+      for (nv = 0; nv < 8; nv++) {
+        flux[nv]  = Sl*Sr*(ur[nv] - ul[nv]) + Sr*fl[nv] - Sl*fr[nv];
+        flux[nv] *= scrh;
+      }
+    }
+  }
+  for (nv = 0; nv < 8; nv++) if (isnan(flux[nv])) o->err |= ERR_NAN | ERR_QUIT;
+
+  if (o->c.ct == ORC_UCT_HLLD) CT_Store_UCTHlld(o, dir, ul, ur, vl, vr, Sl, Sr, Bn_face, e);
+  else                         CT_Store_UCTHll(o, dir, vl, vr, Sl, Sr, e);
+  return cmax;
+}
+
+/* Src/MHD/hll.cpp:50-220 (MHD) */
+static double MHD_HLL(orc_t *o, int dir, double *vl, double *vr, double *flux, long e) {
+  const double gamma = o->c.gamma;
+  int nv;
+  double ul[8], ur[8], fl[8], fr[8], Sl, Sr, pl, pr;
+  MHD_PrimToCons(vl, ul, gamma);
+  MHD_PrimToCons(vr, ur, gamma);
+  double a2L = gamma*vl[7]/vl[RHO];
+  double a2R = gamma*vr[7]/vr[RHO];
+  {
+    double sl_min, sl_max, sr_min, sr_max;
+    MHD_MaxSignalSpeed(dir, vl, a2L, &sl_min, &sl_max);
+    MHD_MaxSignalSpeed(dir, vr, a2R, &sr_min, &sr_max);
+    Sl = MIN(sl_min, sr_min);
+    Sr = MAX(sl_max, sr_max);
+  }
+  double bL = MIN(Sl, 0.0);
+  double bR = MAX(0.0, Sr);
+  double cmax = MAX(fabs(Sl), fabs(Sr));
+  MHD_Flux(dir, vl, ul, fl, &pl);
+  MHD_Flux(dir, vr, ur, fr, &pr);
+  double scrh = 1.0/(bR - bL);
+  for (nv = 0; nv < 8; nv++) {
+    flux[nv]  = bL*bR*(ur[nv] - ul[nv]) + bR*fl[nv] - bL*fr[nv];
+    flux[nv] *= scrh;
+  }
+  for (nv = 0; nv < 8; nv++) if (isnan(flux[nv])) o->err |= ERR_NAN | ERR_QUIT;
+  CT_Store_UCTHll(o, dir, vl, vr, Sl, Sr, e);
+  return cmax;
+}
+
+/* Src/HD/hllc.cpp:54-260 (ideal EOS) */
+static double HD_HLLC(orc_t *o, int dir, double *vl, double *vr, double *flux) {
+  const double gamma = o->c.gamma;
+  int VXn = VX1 + dir, VXt = VX1 + (dir+1)%3, VXb = VX1 + (dir+2)%3;
+  int MXn = MX1 + dir, MXt = MX1 + (dir+1)%3, MXb = MX1 + (dir+2)%3;
+  int nv;
+  double ul[5], ur[5], fL[5], fR[5], usl[5], usr[5], Sl, Sr, pl, pr;
+  HD_PrimToCons(vl, ul, gamma);
+  HD_PrimToCons(vr, ur, gamma);
+  double a2L = gamma*vl[4]/vl[RHO];
+  double a2R = gamma*vr[4]/vr[RHO];
+  HD_Flux(dir, vl, ul, fL, &pl);
+  HD_Flux(dir, vr, ur, fR, &pr);
+  {
+    double sl_min, sl_max, sr_min, sr_max;
+    HD_MaxSignalSpeed(dir, vl, a2L, &sl_min, &sl_max);
+    HD_MaxSignalSpeed(dir, vr, a2R, &sr_min, &sr_max);
+    Sl = MIN(sl_min, sr_min);
+    Sr = MAX(sl_max, sr_max);
+  }
+  double cmax = MAX(fabs(Sl), fabs(Sr));
+  if (Sl > 0.0) {
+    for (nv = 0; nv < 5; nv++) flux[nv] = fL[nv];
+  } else if (Sr < 0.0) {
+    for (nv = 0; nv < 5; nv++) flux[nv] = fR[nv];
+  } else {
+    double vs;
+    {
+      double qL = vl[4] + ul[MXn]*(vl[VXn] - Sl);
+      double qR = vr[4] + ur[MXn]*(vr[VXn] - Sr);
+      double wL = vl[RHO]*(vl[VXn] - Sl);
+      double wR = vr[RHO]*(vr[VXn] - Sr);
+      vs = (qR - qL)/(wR - wL);
+    }
+    {
+      double vxr = vr[VXn];
+      double vxl = vl[VXn];
+      usl[RHO] = ul[RHO]*(Sl - vxl)/(Sl - vs);
+      usr[RHO] = ur[RHO]*(Sr - vxr)/(Sr - vs);
+      usl[MXn] = usl[RHO]*vs;      usr[MXn] = usr[RHO]*vs;
+      usl[MXt] = usl[RHO]*vl[VXt]; usr[MXt] = usr[RHO]*vr[VXt];
+      usl[MXb] = usl[RHO]*vl[VXb]; usr[MXb] = usr[RHO]*vr[VXb];
+      usl[4] = ul[4]/vl[RHO] + (vs - vxl)*(vs + vl[4]/(vl[RHO]*(Sl - vxl)));
+      usr[4] = ur[4]/vr[RHO] + (vs - vxr)*(vs + vr[4]/(vr[RHO]*(Sr - vxr)));
+    }
+    usl[4] *= usl[RHO];
+    usr[4] *= usr[RHO];
+    if (vs >= 0.0) {
+      for (nv = 0; nv < 5; nv++) flux[nv] = fL[nv] + Sl*(usl[nv] - ul[nv]);
+    } else {
+      for (nv = 0; nv < 5; nv++) flux[nv] = fR[nv] + Sr*(usr[nv] - ur[nv]);
+    }
+  }
+  for (nv = 0; nv < 5; nv++) if (isnan(flux[nv])) o->err |= ERR_NAN | ERR_QUIT;
+  return cmax;
+}
+
+/* Src/HD/hll.cpp:95-175 (HD HLL: explicit supersonic branches) */
+static double HD_HLL(orc_t *o, int dir, double *vl, double *vr, double *flux) {
+  const double gamma = o->c.gamma;
+  int nv;
+  double ul[5], ur[5], fL[5], fR[5], Sl, Sr, pl, pr;
+  HD_PrimToCons(vl, ul, gamma);
+  HD_PrimToCons(vr, ur, gamma);
+  double a2L = gamma*vl[4]/vl[RHO];
+  double a2R = gamma*vr[4]/vr[RHO];
+  {
+    double sl_min, sl_max, sr_min, sr_max;
+    HD_MaxSignalSpeed(dir, vl, a2L, &sl_min, &sl_max);
+    HD_MaxSignalSpeed(dir, vr, a2R, &sr_min, &sr_max);
+    Sl = MIN(sl_min, sr_min);
+    Sr = MAX(sl_max, sr_max);
+  }
+  double cmax = MAX(fabs(Sl), fabs(Sr));
+  HD_Flux(dir, vl, ul, fL, &pl);
+  HD_Flux(dir, vr, ur, fR, &pr);
+  if (Sl > 0.0) {
+    for (nv = 0; nv < 5; nv++) flux[nv] = fL[nv];
+  } else if (Sr < 0.0) {
+    for (nv = 0; nv < 5; nv++) flux[nv] = fR[nv];
+  } else {
+    double scrh = 1.0/(Sr - Sl);
+    for (nv = 0; nv < 5; nv++) {
+      flux[nv]  = Sl*Sr*(ur[nv] - ul[nv]) + Sr*fL[nv] - Sl*fR[nv];
+      flux[nv] *= scrh;
+    }
+  }
+  for (nv = 0; nv < 5; nv++) if (isnan(flux[nv])) o->err |= ERR_NAN | ERR_QUIT;
+  return cmax;
+}
+
+/* ------------------------------------------------------------------ */
+/* reconstruction                                                      */
+/* ------------------------------------------------------------------ */
+
+/* Src/States/plm_coeffs.hpp:88-100 (uniform Cartesian grid) and
+   Src/macros.hpp:200 (minmod) */
+static double Limit(int lim, double dvp, double dvm) {
+  double dv;
+  if (lim == ORC_LIM_MC) {
+    if (dvp*dvm > 0.0) {
+      double qc = 0.5*(dvm + dvp), scrh = 2.0*ABS_MIN(dvp, dvm);
+      dv = ABS_MIN(qc, scrh);
+    } else dv = 0.0;
+  } else if (lim == ORC_LIM_VL) {
+    dv = (dvp*dvm > 0.0 ? 2.0*dvp*dvm/(dvp + dvm) : 0.0);
+  } else if (lim == ORC_LIM_MINMOD) {
+    dv = (dvp*dvm > 0.0 ? ABS_MIN(dvp, dvm) : 0.0);
+  } else {
+    dv = 0.0;
+  }
+  return dv;
+}
+
+/* ------------------------------------------------------------------ */
+/* boundary: Src/boundary.cpp:67-322 + PeriodicBoundary 502-675         */
+/* ------------------------------------------------------------------ */
+static void AverageStaggered(orc_t *o, int ib, int ie, int jb, int je, int kb, int ke,
+                             int write_vc) {
+  /* Src/MHD/CT/ct_field_average.cpp:175-200, 378-410 (Cartesian) */
+  int i, j, k, d;
+  for (k = kb; k <= ke; k++)
+  for (j = jb; j <= je; j++)
+  for (i = ib; i <= ie; i++) {
+    for (d = 0; d < o->c.ndim; d++) {
+      int di = (d == 0), dj = (d == 1), dk = (d == 2);
+      double bf = 0.5*(o->Vs[d][SI(o,d,i,j,k)] + o->Vs[d][SI(o,d,i+di,j+dj,k+dk)]);
+      *VC(o, o->Uc, BX1+d, i, j, k) = bf;
+      if (write_vc) *VC(o, o->Vc, BX1+d, i, j, k) = bf;
+    }
+  }
+}
+
+static void Boundary(orc_t *o) {
+  int side, nv, i, j, k;
+  int isMHD = (o->c.physics != ORC_HD);
+  for (side = 0; side < 2*o->c.ndim; side++) {
+    int d = side/2, beg = (side%2 == 0);
+    int lo[3] = {0, 0, 0}, hi[3] = {o->nt[0]-1, o->nt[1]-1, o->nt[2]-1};
+    int shift = beg ? o->c.n[d] : -o->c.n[d];
+    if (beg) { lo[d] = 0; hi[d] = o->beg[d]-1; }
+    else     { lo[d] = o->end[d]+1; hi[d] = o->nt[d]-1; }
+    for (nv = 0; nv < o->nvar; nv++)
+      for (k = lo[2]; k <= hi[2]; k++)
+      for (j = lo[1]; j <= hi[1]; j++)
+      for (i = lo[0]; i <= hi[0]; i++) {
+        int s[3] = {i, j, k}; s[d] += shift;
+        *VC(o, o->Vc, nv, i, j, k) = *VC(o, o->Vc, nv, s[0], s[1], s[2]);
+      }
+    if (isMHD) {
+      int c;
+      for (c = 0; c < o->c.ndim; c++) {
+        /* BOX_LOOP on the own-direction beg side, BOXI/J/K_LOOP elsewhere */
+        int ext = (c == d && beg) ? 0 : 1;
+        int h[3] = {hi[0], hi[1], hi[2]};
+        h[c] += ext;
+        for (k = lo[2]; k <= h[2]; k++)
+        for (j = lo[1]; j <= h[1]; j++)
+        for (i = lo[0]; i <= h[0]; i++) {
+          int s[3] = {i, j, k}; s[d] += shift;
+          o->Vs[c][SI(o,c,i,j,k)] = o->Vs[c][SI(o,c,s[0],s[1],s[2])];
+        }
+      }
+      /* Src/boundary.cpp:285-307: ghost cell B from faces, copied to Vc */
+      AverageStaggered(o, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], 1);
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* sweeps: Src/update_stage.cpp:57-384                                 */
+/* ------------------------------------------------------------------ */
+static void Sweep(orc_t *o, int dir, double dt) {
+  const int nvar = o->nvar, ndim = o->c.ndim;
+  const int isMHD = (o->c.physics != ORC_HD);
+  int ntr = isMHD ? o->ng : 0;    /* Src/update_stage.cpp:80-90 */
+  int t1d = (dir == 0 ? 1 : 0), t2d = (dir == 2 ? 1 : 2);
+  int tlo1 = o->beg[t1d], thi1 = o->end[t1d], tlo2 = o->beg[t2d], thi2 = o->end[t2d];
+  if (t1d < ndim) { tlo1 -= ntr; thi1 += ntr; }
+  if (t2d < ndim) { tlo2 -= ntr; thi2 += ntr; }
+  int nd = o->nt[dir], ib = o->beg[dir], ie = o->end[dir];
+  double dtdx = dt/o->c.dx[dir];
+  int t1, t2, i, nv;
+  double *v = o->pv, *vL = o->pvL, *vR = o->pvR, *flux = o->pflux, *cmax = o->pcmax, *Bn = o->pBn;
+
+  for (t2 = tlo2; t2 <= thi2; t2++)
+  for (t1 = tlo1; t1 <= thi1; t1++) {
+    int ti, tj, tk;
+    /* DataToSweep: Src/data2sweep.cpp:48-222 */
+    for (i = 0; i < nd; i++) {
+      TrueIdx(dir, i, t1, t2, &ti, &tj, &tk);
+      for (nv = 0; nv < nvar; nv++) v[i*nvar + nv] = *VC(o, o->Vc, nv, ti, tj, tk);
+      if (isMHD) Bn[i] = o->Vs[dir][SI(o, dir, ti, tj, tk)];
+    }
+    /* Reconstruct: Src/States/plm_states.cpp:99-141 */
+    for (nv = 0; nv < nvar; nv++)
+      for (i = ib-1; i <= ie+1; i++) {
+        double dvp = v[(i+1)*nvar + nv] - v[i*nvar + nv];
+        double dvm = v[i*nvar + nv] - v[(i-1)*nvar + nv];
+        double dv = Limit(o->c.limiter, dvp, dvm);
+        vL[(i+1)*nvar + nv] = v[i*nvar + nv] + 0.5*dv;
+        vR[i*nvar + nv]     = v[i*nvar + nv] - 0.5*dv;
+      }
+    /* CT normal-field overwrite: Src/States/plm_states.cpp:184-189 */
+    if (isMHD) {
+      for (i = ib-1; i <= ie+1; i++) {
+        vL[(i+1)*nvar + BX1 + dir] = Bn[i+1];
+        vR[i*nvar + BX1 + dir] = Bn[i];
+      }
+    }
+    /* Riemann solver at interfaces i-1/2, i in [ib, ie+1] */
+    for (i = ib; i <= ie+1; i++) {
+      TrueIdx(dir, i, t1, t2, &ti, &tj, &tk);
+      long e = EI(o, ti, tj, tk);
+      double *vl = vL + i*nvar, *vr = vR + i*nvar, *f = flux + i*nvar;
+      if (o->c.physics == ORC_MHD) {
+        if (o->c.solver == ORC_HLLD) cmax[i] = MHD_HLLD(o, dir, vl, vr, f, e, Bn[i]);
+        else                         cmax[i] = MHD_HLL(o, dir, vl, vr, f, e);
+      } else if (o->c.physics == ORC_HD) {
+        if (o->c.solver == ORC_HLLC) cmax[i] = HD_HLLC(o, dir, vl, vr, f);
+        else                         cmax[i] = HD_HLL(o, dir, vl, vr, f);
+      } else {
+        cmax[i] = orc_rmhd_riemann(o, dir, vl, vr, f, e);
+      }
+    }
+    /* RightHandSide over the interior box only: Src/MHD/rhs.cpp:383-386, 523 */
+    if (t1 < o->beg[t1d] || t1 > o->end[t1d] || t2 < o->beg[t2d] || t2 > o->end[t2d]) continue;
+    for (i = ib; i <= ie; i++) {
+      TrueIdx(dir, i, t1, t2, &ti, &tj, &tk);
+      for (nv = 0; nv < nvar; nv++) {
+        double rhs = -dtdx*(flux[(i+1)*nvar + nv] - flux[i*nvar + nv]);
+        double *r = VC(o, o->Rc, nv, ti, tj, tk);
+        if (dir == 0) *r = rhs; else *r += rhs;    /* Src/update_stage.cpp:173-184 */
+      }
+      double cdt = 0.5*(cmax[i] + cmax[i+1])/o->c.dx[dir];
+      long c = CI(o, ti, tj, tk);
+      if (dir == 0) o->Cdt[c] = cdt; else o->Cdt[c] += cdt;
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* EMF: Src/MHD/CT/ct_emf_average.cpp:535-995 with ArrayReconstruct    */
+/* (Src/array_reconstruct.cpp:45-206)                                  */
+/* ------------------------------------------------------------------ */
+
+/* Reconstruct Q along `dir` on the pencil at transverse (t1,t2).  Q is either a
+   staggered field (stag >= 0, component index) or an EMF face array. */
+static void ArrayRec(orc_t *o, int dir, int t1, int t2, int stag, const double *Qe,
+                     int lim, double *qL, double *qR) {
+  int nd = o->nt[dir], i, ti, tj, tk;
+  double *q = o->pq;
+  for (i = 0; i < nd; i++) {
+    TrueIdx(dir, i, t1, t2, &ti, &tj, &tk);
+    q[i] = (stag >= 0) ? o->Vs[stag][SI(o, stag, ti, tj, tk)] : Qe[EI(o, ti, tj, tk)];
+  }
+  for (i = 1; i < nd-1; i++) {
+    double dqp = q[i+1] - q[i];
+    double dqm = q[i] - q[i-1];
+    double dq = Limit(lim, dqp, dqm);
+    qL[i+1] = q[i] + 0.5*dq;
+    qR[i]   = q[i] - 0.5*dq;
+  }
+}
+
+static void ComputeEMF(orc_t *o) {
+  const int ndim = o->c.ndim;
+  int recV = o->c.limiter, recB = ORC_LIM_MC;
+  int ib = o->beg[0], ie = o->end[0] + 1;
+  int jb = o->beg[1], je = o->end[1] + 1;
+  int kb = o->beg[2], ke = o->end[2] + (ndim == 3);
+  int i, j, k;
+  double *bL = o->pqL, *bR = o->pqR, *vL = o->pvL, *vR = o->pvR;   /* scratch */
+  double *qL2 = o->pflux, *qR2 = o->pcmax;
+  (void)vL; (void)vR;
+
+  /* X1a: By and -vx along x -> Ez at (i-1/2, j-1/2, k) */
+  for (k = kb; k <= ke; k++)
+  for (j = jb; j <= je; j++) {
+    ArrayRec(o, 0, j, k, 1, NULL, recB, bL, bR);
+    ArrayRec(o, 0, j, k, -1, o->e[2][1], recV, qL2, qR2);
+    for (i = ib; i <= ie; i++) {
+      double aL = 0.5*(o->aL[0][EI(o,i,j-1,k)] + o->aL[0][EI(o,i,j,k)]);
+      double aR = 0.5*(o->aR[0][EI(o,i,j-1,k)] + o->aR[0][EI(o,i,j,k)]);
+      double dL = 0.5*(o->dL[0][EI(o,i,j-1,k)] + o->dL[0][EI(o,i,j,k)]);
+      double dR = 0.5*(o->dR[0][EI(o,i,j-1,k)] + o->dR[0][EI(o,i,j,k)]);
+      double phi = dR*bR[i] - dL*bL[i];
+      o->Ee[2][EI(o,i,j,k)] = (aL*qL2[i]*bL[i] + aR*qR2[i]*bR[i]) + phi;
+    }
+  }
+  if (ndim == 3) {
+    /* X1b: Bz and vx along x -> Ey at (i-1/2, j, k-1/2) */
+    for (k = kb; k <= ke; k++)
+    for (j = jb; j <= je; j++) {
+      ArrayRec(o, 0, j, k, 2, NULL, recB, bL, bR);
+      ArrayRec(o, 0, j, k, -1, o->e[1][2], recV, qL2, qR2);
+      for (i = ib; i <= ie; i++) {
+        double aL = 0.5*(o->aL[0][EI(o,i,j,k-1)] + o->aL[0][EI(o,i,j,k)]);
+        double aR = 0.5*(o->aR[0][EI(o,i,j,k-1)] + o->aR[0][EI(o,i,j,k)]);
+        double dL = 0.5*(o->dL[0][EI(o,i,j,k-1)] + o->dL[0][EI(o,i,j,k)]);
+        double dR = 0.5*(o->dR[0][EI(o,i,j,k-1)] + o->dR[0][EI(o,i,j,k)]);
+        double phi = dR*bR[i] - dL*bL[i];
+        o->Ee[1][EI(o,i,j,k)] = (aL*qL2[i]*bL[i] + aR*qR2[i]*bR[i]) - phi;
+      }
+    }
+    /* X2a: Bz and -vy along y -> Ex at (i, j-1/2, k-1/2) */
+    for (k = kb; k <= ke; k++)
+    for (i = ib; i <= ie; i++) {
+      ArrayRec(o, 1, i, k, 2, NULL, recB, bL, bR);
+      ArrayRec(o, 1, i, k, -1, o->e[0][2], recV, qL2, qR2);
+      for (j = jb; j <= je; j++) {
+        double aL = 0.5*(o->aL[1][EI(o,i,j,k-1)] + o->aL[1][EI(o,i,j,k)]);
+        double aR = 0.5*(o->aR[1][EI(o,i,j,k-1)] + o->aR[1][EI(o,i,j,k)]);
+        double dL = 0.5*(o->dL[1][EI(o,i,j,k-1)] + o->dL[1][EI(o,i,j,k)]);
+        double dR = 0.5*(o->dR[1][EI(o,i,j,k-1)] + o->dR[1][EI(o,i,j,k)]);
+        double phi = dR*bR[j] - dL*bL[j];
+        o->Ee[0][EI(o,i,j,k)] = (aL*qL2[j]*bL[j] + aR*qR2[j]*bR[j]) + phi;
+      }
+    }
+  }
+  /* X2b: Bx and vy along y -> complete Ez */
+  for (k = kb; k <= ke; k++)
+  for (i = ib; i <= ie; i++) {
+    ArrayRec(o, 1, i, k, 0, NULL, recB, bL, bR);
+    ArrayRec(o, 1, i, k, -1, o->e[2][0], recV, qL2, qR2);
+    for (j = jb; j <= je; j++) {
+      double aL = 0.5*(o->aL[1][EI(o,i-1,j,k)] + o->aL[1][EI(o,i,j,k)]);
+      double aR = 0.5*(o->aR[1][EI(o,i-1,j,k)] + o->aR[1][EI(o,i,j,k)]);
+      double dL = 0.5*(o->dL[1][EI(o,i-1,j,k)] + o->dL[1][EI(o,i,j,k)]);
+      double dR = 0.5*(o->dR[1][EI(o,i-1,j,k)] + o->dR[1][EI(o,i,j,k)]);
+      double phi = dR*bR[j] - dL*bL[j];
+      o->Ee[2][EI(o,i,j,k)] += (aL*qL2[j]*bL[j] + aR*qR2[j]*bR[j]) - phi;
+    }
+  }
+  if (ndim == 3) {
+    /* X3a: Bx and -vz along z -> complete Ey */
+    for (j = jb; j <= je; j++)
+    for (i = ib; i <= ie; i++) {
+      ArrayRec(o, 2, i, j, 0, NULL, recB, bL, bR);
+      ArrayRec(o, 2, i, j, -1, o->e[1][0], recV, qL2, qR2);
+      for (k = kb; k <= ke; k++) {
+        double aL = 0.5*(o->aL[2][EI(o,i-1,j,k)] + o->aL[2][EI(o,i,j,k)]);
+        double aR = 0.5*(o->aR[2][EI(o,i-1,j,k)] + o->aR[2][EI(o,i,j,k)]);
+        double dL = 0.5*(o->dL[2][EI(o,i-1,j,k)] + o->dL[2][EI(o,i,j,k)]);
+        double dR = 0.5*(o->dR[2][EI(o,i-1,j,k)] + o->dR[2][EI(o,i,j,k)]);
+        double phi = dR*bR[k] - dL*bL[k];
+        o->Ee[1][EI(o,i,j,k)] += (aL*qL2[k]*bL[k] + aR*qR2[k]*bR[k]) + phi;
+      }
+    }
+    /* X3b: By and vz along z -> complete Ex */
+    for (j = jb; j <= je; j++)
+    for (i = ib; i <= ie; i++) {
+      ArrayRec(o, 2, i, j, 1, NULL, recB, bL, bR);
+      ArrayRec(o, 2, i, j, -1, o->e[0][1], recV, qL2, qR2);
+      for (k = kb; k <= ke; k++) {
+        double aL = 0.5*(o->aL[2][EI(o,i,j-1,k)] + o->aL[2][EI(o,i,j,k)]);
+        double aR = 0.5*(o->aR[2][EI(o,i,j-1,k)] + o->aR[2][EI(o,i,j,k)]);
+        double dL = 0.5*(o->dL[2][EI(o,i,j-1,k)] + o->dL[2][EI(o,i,j,k)]);
+        double dR = 0.5*(o->dR[2][EI(o,i,j-1,k)] + o->dR[2][EI(o,i,j,k)]);
+        double phi = dR*bR[k] - dL*bL[k];
+        o->Ee[0][EI(o,i,j,k)] += (aL*qL2[k]*bL[k] + aR*qR2[k]*bR[k]) - phi;
+      }
+    }
+  }
+}
+
+/* Src/MHD/CT/ct_update.cpp:181-423 (Cartesian) -> Rs = -curl(E) dt */
+static void CTUpdate(orc_t *o, double dt) {
+  const int ndim = o->c.ndim;
+  int i, j, k;
+  int ib = o->beg[0], ie = o->end[0], jb = o->beg[1], je = o->end[1], kb = o->beg[2], ke = o->end[2];
+  double dtdx1 = dt/o->c.dx[0], dtdx2 = dt/o->c.dx[1], dtdx3 = dt/o->c.dx[2];
+  /* Bx1 faces */
+  for (k = kb; k <= ke; k++)
+  for (j = jb; j <= je; j++)
+  for (i = ib; i <= ie+1; i++) {
+    double curlE = 0.0 + dtdx2*(o->Ee[2][EI(o,i,j+1,k)] - o->Ee[2][EI(o,i,j,k)]);
+    if (ndim == 3) curlE = curlE - dtdx3*(o->Ee[1][EI(o,i,j,k+1)] - o->Ee[1][EI(o,i,j,k)]);
+    o->Rs[0][SI(o,0,i,j,k)] = -curlE;
+  }
+  /* Bx2 faces */
+  for (k = kb; k <= ke; k++)
+  for (j = jb; j <= je+1; j++)
+  for (i = ib; i <= ie; i++) {
+    double curlE = -dtdx1*(o->Ee[2][EI(o,i+1,j,k)] - o->Ee[2][EI(o,i,j,k)]);
+    if (ndim == 3) curlE = curlE + dtdx3*(o->Ee[0][EI(o,i,j,k+1)] - o->Ee[0][EI(o,i,j,k)]);
+    o->Rs[1][SI(o,1,i,j,k)] = -curlE;
+  }
+  if (ndim == 3) {
+    for (k = kb; k <= ke+1; k++)
+    for (j = jb; j <= je; j++)
+    for (i = ib; i <= ie; i++) {
+      double curlE = dtdx1*(o->Ee[1][EI(o,i+1,j,k)] - o->Ee[1][EI(o,i,j,k)])
+                   - dtdx2*(o->Ee[0][EI(o,i,j+1,k)] - o->Ee[0][EI(o,i,j,k)]);
+      o->Rs[2][SI(o,2,i,j,k)] = -curlE;
+    }
+  }
+}
+
+/* Src/update_stage.cpp:57-438 */
+static double UpdateStage(orc_t *o, double dt, int stage) {
+  int d;
+  for (d = 0; d < o->c.ndim; d++) Sweep(o, d, dt);
+  if (o->c.physics != ORC_HD) {
+    ComputeEMF(o);
+    CTUpdate(o, dt);
+  }
+  double inv = -1.0;
+  if (stage == 1) {
+    int i, j, k;
+    for (k = o->beg[2]; k <= o->end[2]; k++)
+    for (j = o->beg[1]; j <= o->end[1]; j++)
+    for (i = o->beg[0]; i <= o->end[0]; i++) inv = MAX(inv, o->Cdt[CI(o,i,j,k)]);
+    inv = inv/(double)o->c.ndim;   /* update_stage.cpp:422-435 */
+  }
+  return inv;
+}
+
+/* Src/mappers3D.cpp:76-194 over the interior box */
+static void ConsToPrim3D(orc_t *o) {
+  int i, j, k, nv;
+  double u[8], v[8];
+  for (k = o->beg[2]; k <= o->end[2]; k++)
+  for (j = o->beg[1]; j <= o->end[1]; j++)
+  for (i = o->beg[0]; i <= o->end[0]; i++) {
+    uint32_t err = 0;
+    for (nv = 0; nv < o->nvar; nv++) {
+      u[nv] = *VC(o, o->Uc, nv, i, j, k);
+      if (isnan(u[nv])) err |= ERR_NAN | ERR_QUIT;
+    }
+    uint32_t le;
+    if (o->c.physics == ORC_MHD) le = MHD_ConsToPrim(u, v, o->c.gamma, 1.e-12, 1.e-12);
+    else if (o->c.physics == ORC_HD) le = HD_ConsToPrim(u, v, o->c.gamma, 1.e-12, 1.e-12);
+    else le = orc_rmhd_cons_to_prim(o, u, v, i, j, k);
+    err |= le;
+    if (le & ERR_CONS2PRIM_FAIL) err |= ERR_QUIT;
+    if (le) for (nv = 0; nv < o->nvar; nv++) *VC(o, o->Uc, nv, i, j, k) = u[nv];
+    for (nv = 0; nv < o->nvar; nv++) *VC(o, o->Vc, nv, i, j, k) = v[nv];
+    o->err |= err;
+  }
+}
+
+/* Src/rk_step.cpp:88-593 (RK2 branch) */
+double orc_step(void *h, double dt, uint32_t *err_out) {
+  orc_t *o = (orc_t *)h;
+  const int ndim = o->c.ndim, nvar = o->nvar;
+  const int isMHD = (o->c.physics != ORC_HD);
+  int i, j, k, nv, d;
+  o->err = 0;
+
+  /* stage 1 */
+  Boundary(o);
+  double invDt = UpdateStage(o, dt, 1);
+  for (nv = 0; nv < nvar; nv++)
+    for (k = o->beg[2]; k <= o->end[2]; k++)
+    for (j = o->beg[1]; j <= o->end[1]; j++)
+    for (i = o->beg[0]; i <= o->end[0]; i++) {
+      double *u = VC(o, o->Uc, nv, i, j, k), *u0 = VC(o, o->U0, nv, i, j, k);
+      *u0 = *u;
+      *u = *u0 + 1.0*(*VC(o, o->Rc, nv, i, j, k));
+    }
+  if (isMHD) {
+    for (k = o->beg[2]; k <= o->end[2] + (ndim == 3); k++)
+    for (j = o->beg[1]; j <= o->end[1] + 1; j++)
+    for (i = o->beg[0]; i <= o->end[0] + 1; i++)
+      for (d = 0; d < ndim; d++) {
+        long s = SI(o, d, i, j, k);
+        o->Bs0[d][s] = o->Vs[d][s];
+        o->Vs[d][s] = o->Bs0[d][s] + 1.0*o->Rs[d][s];
+      }
+    AverageStaggered(o, o->beg[0], o->end[0], o->beg[1], o->end[1], o->beg[2], o->end[2], 0);
+  }
+  ConsToPrim3D(o);
+
+  /* stage 2 */
+  Boundary(o);
+  UpdateStage(o, dt, 2);
+  for (nv = 0; nv < nvar; nv++)
+    for (k = o->beg[2]; k <= o->end[2]; k++)
+    for (j = o->beg[1]; j <= o->end[1]; j++)
+    for (i = o->beg[0]; i <= o->end[0]; i++) {
+      double *u = VC(o, o->Uc, nv, i, j, k);
+      *u = 0.5*(*VC(o, o->U0, nv, i, j, k)) + 0.5*(*u) + 0.5*(*VC(o, o->Rc, nv, i, j, k));
+    }
+  if (isMHD) {
+    for (k = o->beg[2]; k <= o->end[2] + (ndim == 3); k++)
+    for (j = o->beg[1]; j <= o->end[1] + 1; j++)
+    for (i = o->beg[0]; i <= o->end[0] + 1; i++)
+      for (d = 0; d < ndim; d++) {
+        long s = SI(o, d, i, j, k);
+        o->Vs[d][s] = 0.5*o->Bs0[d][s] + 0.5*o->Vs[d][s] + 0.5*o->Rs[d][s];
+      }
+    AverageStaggered(o, o->beg[0], o->end[0], o->beg[1], o->end[1], o->beg[2], o->end[2], 0);
+  }
+  ConsToPrim3D(o);
+  if (err_out) *err_out = o->err;
+  return invDt;
+}
+
+/* Src/next_time_step.cpp:20-130 (no MPI, no parabolic terms) */
+double orc_next_dt(double invDt_hyp, double cfl, double cfl_max_var, double dt) {
+  double dt_new = cfl/invDt_hyp;
+  dt_new = MIN(dt_new, cfl_max_var*dt);
+  return dt_new;
+}
+
+/* ------------------------------------------------------------------ */
+/* state I/O (interior, SoA [nv][k][j][i])                             */
+/* ------------------------------------------------------------------ */
+void orc_set_state(void *h, const double *V, const double *U, const double *Bs) {
+  orc_t *o = (orc_t *)h;
+  int i, j, k, nv, d;
+  long c = 0;
+  for (nv = 0; nv < o->nvar; nv++)
+    for (k = o->beg[2]; k <= o->end[2]; k++)
+    for (j = o->beg[1]; j <= o->end[1]; j++)
+    for (i = o->beg[0]; i <= o->end[0]; i++, c++) {
+      *VC(o, o->Vc, nv, i, j, k) = V[c];
+      *VC(o, o->Uc, nv, i, j, k) = U[c];
+    }
+  if (o->c.physics != ORC_HD) {
+    long n = (long)o->c.n[0]*o->c.n[1]*o->c.n[2];
+    for (d = 0; d < o->c.ndim; d++) {
+      c = 0;
+      for (k = o->beg[2]; k <= o->end[2]; k++)
+      for (j = o->beg[1]; j <= o->end[1]; j++)
+      for (i = o->beg[0]; i <= o->end[0]; i++, c++)
+        o->Vs[d][SI(o, d, i, j, k)] = Bs[d*n + c];
+      /* the right boundary face equals the left one (periodic) */
+    }
+    for (d = 0; d < o->c.ndim; d++) {
+      int di = (d == 0), dj = (d == 1), dk = (d == 2);
+      for (k = o->beg[2]; k <= o->end[2]; k++)
+      for (j = o->beg[1]; j <= o->end[1]; j++)
+      for (i = o->beg[0]; i <= o->end[0]; i++) {
+        if ((di && i == o->beg[0]) || (dj && j == o->beg[1]) || (dk && k == o->beg[2]))
+          o->Vs[d][SI(o, d, i + di*o->c.n[0], j + dj*o->c.n[1], k + dk*o->c.n[2])] =
+            o->Vs[d][SI(o, d, i, j, k)];
+      }
+    }
+  }
+}
+
+void orc_get_state(void *h, double *V, double *U, double *Bs) {
+  orc_t *o = (orc_t *)h;
+  int i, j, k, nv, d;
+  long c = 0;
+  for (nv = 0; nv < o->nvar; nv++)
+    for (k = o->beg[2]; k <= o->end[2]; k++)
+    for (j = o->beg[1]; j <= o->end[1]; j++)
+    for (i = o->beg[0]; i <= o->end[0]; i++, c++) {
+      if (V) V[c] = *VC(o, o->Vc, nv, i, j, k);
+      if (U) U[c] = *VC(o, o->Uc, nv, i, j, k);
+    }
+  if (Bs && o->c.physics != ORC_HD) {
+    long n = (long)o->c.n[0]*o->c.n[1]*o->c.n[2];
+    for (d = 0; d < o->c.ndim; d++) {
+      c = 0;
+      for (k = o->beg[2]; k <= o->end[2]; k++)
+      for (j = o->beg[1]; j <= o->end[1]; j++)
+      for (i = o->beg[0]; i <= o->end[0]; i++, c++)
+        Bs[d*n + c] = o->Vs[d][SI(o, d, i, j, k)];
+    }
+  }
+}
+
+/* Start-up conversion, Src/startup.cpp:542-566: U = PrimToCons(V) per cell */
+void orc_prim_to_cons(int physics, double gamma, long ncell, const double *V, double *U) {
+  int nvar = (physics == ORC_HD) ? 5 : 8, nv;
+  long c;
+  double v[8], u[8];
+  for (c = 0; c < ncell; c++) {
+    for (nv = 0; nv < nvar; nv++) v[nv] = V[nv*ncell + c];
+    if (physics == ORC_MHD) MHD_PrimToCons(v, u, gamma);
+    else if (physics == ORC_HD) HD_PrimToCons(v, u, gamma);
+    else orc_rmhd_prim_to_cons(v, u, gamma);
+    for (nv = 0; nv < nvar; nv++) U[nv*ncell + c] = u[nv];
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* construction                                                        */
+/* ------------------------------------------------------------------ */
+void *orc_create(const orc_cfg *cfg) {
+  orc_t *o = (orc_t *)calloc(1, sizeof(orc_t));
+  int d, e;
+  o->c = *cfg;
+  o->nvar = (cfg->physics == ORC_HD) ? 5 : 8;
+  o->ng = 2;   /* PLM: Src/get_nghost.cpp */
+  o->ncell = 1;
+  for (d = 0; d < 3; d++) {
+    if (d < cfg->ndim) { o->nt[d] = cfg->n[d] + 2*o->ng; o->beg[d] = o->ng; }
+    else { o->nt[d] = 1; o->beg[d] = 0; o->c.n[d] = 1; }
+    o->end[d] = o->beg[d] + o->c.n[d] - 1;
+    o->ncell *= o->nt[d];
+    o->ne[d] = o->nt[d] + 1;
+  }
+  o->Vc = calloc((size_t)o->nvar*o->ncell, sizeof(double));
+  o->Uc = calloc((size_t)o->nvar*o->ncell, sizeof(double));
+  o->U0 = calloc((size_t)o->nvar*o->ncell, sizeof(double));
+  o->Rc = calloc((size_t)o->nvar*o->ncell, sizeof(double));
+  o->Cdt = calloc((size_t)o->ncell, sizeof(double));
+  if (cfg->physics != ORC_HD) {
+    long ne = (long)o->ne[0]*o->ne[1]*o->ne[2];
+    for (d = 0; d < 3; d++) {
+      long ns = 1;
+      for (e = 0; e < 3; e++) { o->ns[d][e] = o->nt[e] + (e == d && d < cfg->ndim); ns *= o->ns[d][e]; }
+      if (d < cfg->ndim) {
+        o->Vs[d] = calloc(ns, sizeof(double));
+        o->Bs0[d] = calloc(ns, sizeof(double));
+        o->Rs[d] = calloc(ns, sizeof(double));
+      }
+      o->aL[d] = calloc(ne, sizeof(double));
+      o->aR[d] = calloc(ne, sizeof(double));
+      o->dL[d] = calloc(ne, sizeof(double));
+      o->dR[d] = calloc(ne, sizeof(double));
+      o->Ee[d] = calloc(ne, sizeof(double));
+      for (e = 0; e < 3; e++) o->e[d][e] = calloc(ne, sizeof(double));
+    }
+  }
+  o->pmax = 0;
+  for (d = 0; d < 3; d++) if (o->nt[d] + 2 > o->pmax) o->pmax = o->nt[d] + 2;
+  o->pv = calloc((size_t)o->pmax*8, sizeof(double));
+  o->pvL = calloc((size_t)o->pmax*8, sizeof(double));
+  o->pvR = calloc((size_t)o->pmax*8, sizeof(double));
+  o->pflux = calloc((size_t)o->pmax*8, sizeof(double));
+  o->pcmax = calloc((size_t)o->pmax*8, sizeof(double));
+  o->pBn = calloc((size_t)o->pmax, sizeof(double));
+  o->pq = calloc((size_t)o->pmax, sizeof(double));
+  o->pqL = calloc((size_t)o->pmax, sizeof(double));
+  o->pqR = calloc((size_t)o->pmax, sizeof(double));
+  orc_rmhd_init(o);
+  return o;
+}
+
+void orc_destroy(void *h) {
+  orc_t *o = (orc_t *)h;
+  int d, e;
+  if (!o) return;
+  free(o->Vc); free(o->Uc); free(o->U0); free(o->Rc); free(o->Cdt);
+  for (d = 0; d < 3; d++) {
+    free(o->Vs[d]); free(o->Bs0[d]); free(o->Rs[d]);
+    free(o->aL[d]); free(o->aR[d]); free(o->dL[d]); free(o->dR[d]); free(o->Ee[d]);
+    for (e = 0; e < 3; e++) free(o->e[d][e]);
+  }
+  free(o->pv); free(o->pvL); free(o->pvR); free(o->pflux); free(o->pcmax);
+  free(o->pBn); free(o->pq); free(o->pqL); free(o->pqR);
+  free(o);
+}
+
+/* Convenience: run nsteps with the reference dt rule; dt_hist gets the dt
+   of every step taken plus the next one (nsteps+1 entries). */
+uint32_t orc_run(void *h, int nsteps, double first_dt, double *dt_hist) {
+  orc_t *o = (orc_t *)h;
+  double dt = first_dt;
+  uint32_t err_all = 0, err;
+  int n;
+  for (n = 0; n < nsteps; n++) {
+    if (dt_hist) dt_hist[n] = dt;
+    double inv = orc_step(h, dt, &err);
+    err_all |= err;
+    dt = orc_next_dt(inv, o->c.cfl, o->c.cfl_max_var, dt);
+  }
+  if (dt_hist) dt_hist[nsteps] = dt;
+  return err_all;
+}
+
+#include "gp_oracle_rmhd.inc"

@@ -1,0 +1,31 @@
+/*
+ * gp_oracle.h -- C interface of the CPU restatement of the gPLUTO Godunov
+ * step (test infrastructure only; see gp_oracle.c).
+ */
+#ifndef GP_ORACLE_H
+#define GP_ORACLE_H
+#include <stdint.h>
+
+enum { ORC_HD = 0, ORC_MHD = 1, ORC_RMHD = 2 };
+enum { ORC_LIM_FLAT = 0, ORC_LIM_MINMOD = 1, ORC_LIM_VL = 2, ORC_LIM_MC = 3 };
+enum { ORC_HLL = 0, ORC_HLLC = 1, ORC_HLLD = 2 };
+enum { ORC_UCT_HLL = 0, ORC_UCT_HLLD = 1 };
+
+typedef struct {
+  int physics, ndim;
+  int n[3];
+  int limiter, solver, ct;
+  double gamma;
+  double dx[3];
+  double cfl, cfl_max_var;
+} orc_cfg;
+
+void    *orc_create(const orc_cfg *cfg);
+void     orc_destroy(void *h);
+void     orc_set_state(void *h, const double *V, const double *U, const double *Bs);
+void     orc_get_state(void *h, double *V, double *U, double *Bs);
+double   orc_step(void *h, double dt, uint32_t *err);
+double   orc_next_dt(double invDt_hyp, double cfl, double cfl_max_var, double dt);
+uint32_t orc_run(void *h, int nsteps, double first_dt, double *dt_hist);
+void     orc_prim_to_cons(int physics, double gamma, long ncell, const double *V, double *U);
+#endif

@@ -1,0 +1,91 @@
+"""Generate the golden parity fixtures from the reference gPLUTO serial build.
+
+Run in a container that has the reference tree (default /root/reference):
+
+    python tests/golden/make_golden.py [name ...]
+
+For each case this builds the reference binary (oracle/ref/build_ref.py,
+sources compiled in place), writes a seeded initial condition made by
+gpluto_dev_b200/ics.py, runs N steps with FTZ/DAZ off, and stores the
+initial primitive state, the face fields and the reference's final
+Vc/Uc/Vs plus its dt history as ``<name>.npz`` next to this script.
+The fixtures are small so that they can be committed; the GPU box never
+needs the reference tree.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle", "ref"))
+
+from gpluto_dev_b200 import ics  # noqa: E402
+import build_ref as br  # noqa: E402
+
+# name: (generator, kwargs, RefConfig kwargs, nsteps)
+CASES = {
+    "mhd2d_mc_hlld_ucthlld": (ics.mhd2d_turbulence, dict(n=(32, 32), seed=3),
+                              dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",
+                                   ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4), 20),
+    "mhd2d_mc_hlld_ucthlld_long": (ics.mhd2d_turbulence, dict(n=(40, 40), seed=11),
+                                   dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",
+                                        ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4), 100),
+    "mhd2d_vl_hll_ucthll": (ics.mhd2d_turbulence, dict(n=(32, 24), seed=5),
+                            dict(physics="MHD", ndim=2, limiter="VANLEER_LIM", solver="hll",
+                                 ct_emf="UCT_HLL", cfl=0.4, first_dt=1e-4), 20),
+    "mhd2d_mc_hlld_ucthll": (ics.mhd2d_turbulence, dict(n=(24, 32), seed=6),
+                             dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",
+                                  ct_emf="UCT_HLL", cfl=0.4, first_dt=1e-4), 20),
+    "mhd3d_mc_hlld_ucthlld": (ics.mhd3d_turbulence, dict(n=(12, 10, 8), seed=7),
+                              dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                   ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4), 10),
+    "mhd3d_blast_mc_hlld": (ics.mhd3d_blast, dict(n=(16, 16, 16), seed=2, radius=0.2),
+                            dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                 ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4), 12),
+    "hd2d_mc_hllc": (ics.hd_turbulence, dict(n=(32, 32), seed=8),
+                     dict(physics="HD", ndim=2, limiter="MC_LIM", solver="hllc",
+                          cfl=0.4, first_dt=1e-4), 20),
+    "hd3d_vl_hll": (ics.hd_turbulence, dict(n=(12, 12, 10), seed=9),
+                    dict(physics="HD", ndim=3, limiter="VANLEER_LIM", solver="hll",
+                         cfl=0.4, first_dt=1e-4), 10),
+}
+
+
+def ref_cfg_name(rc: dict) -> str:
+    return "{physics}{ndim}d_{limiter}_{solver}_{ct}".format(
+        ct=rc.get("ct_emf", "none"), **rc).lower()
+
+
+def make(name: str) -> str:
+    gen, kw, rc, nsteps = CASES[name]
+    st = gen(**kw)
+    cfg = br.RefConfig(name=ref_cfg_name(rc), n=st.shape, **rc)
+    # the grid size is a run-time ini parameter: one binary per scheme,
+    # re-using objects; the ini is rewritten per case
+    binary = br.build(cfg)
+    with tempfile.TemporaryDirectory() as tmp:
+        icp = os.path.join(tmp, "ic.bin")
+        dmp = os.path.join(tmp, "out.dump")
+        ics.write_ic(icp, st)
+        d = br.run_ref(binary, icp, nsteps, dmp)
+    out = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(
+        out, physics=st.physics, ndim=st.ndim, shape=np.array(st.shape), gamma=st.gamma,
+        V0=st.V, Bs0=np.array(st.Bs) if st.Bs else np.zeros(0),
+        V=d.V, U=d.U, Bs=np.array(d.Bs) if d.Bs else np.zeros(0), dt=d.dt, nsteps=nsteps,
+        limiter=rc["limiter"], solver=rc["solver"], ct=rc.get("ct_emf", "none"),
+        cfl=rc["cfl"], cfl_max_var=1.1, first_dt=rc["first_dt"])
+    return out
+
+
+if __name__ == "__main__":
+    names = sys.argv[1:] or list(CASES)
+    for nm in names:
+        p = make(nm)
+        print(f"{nm}: {os.path.getsize(p)/1024:.0f} KiB")

@@ -1,0 +1,41 @@
+"""Helpers to load the committed golden fixtures (reference outputs)."""
+from __future__ import annotations
+
+import glob
+import os
+
+import numpy as np
+
+from gpluto_dev_b200 import ics
+
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+LIMITER = {"MC_LIM": "mc", "VANLEER_LIM": "vl", "MINMOD_LIM": "minmod"}
+CT = {"UCT_HLLD": "uct_hlld", "UCT_HLL": "uct_hll", "none": "uct_hll"}
+
+
+def names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+
+
+class Golden:
+    def __init__(self, name: str):
+        z = np.load(os.path.join(GOLDEN_DIR, name + ".npz"))
+        self.name = name
+        self.physics = int(z["physics"])
+        self.ndim = int(z["ndim"])
+        self.shape = tuple(int(x) for x in z["shape"])
+        self.gamma = float(z["gamma"])
+        Bs0 = list(z["Bs0"]) if self.physics != ics.PHYS_HD else []
+        self.ic = ics.PrimState(self.physics, self.ndim, self.shape, self.gamma,
+                                z["V0"].copy(), [b.copy() for b in Bs0])
+        self.V, self.U = z["V"], z["U"]
+        self.Bs = list(z["Bs"]) if self.physics != ics.PHYS_HD else []
+        self.dt = z["dt"]
+        self.nsteps = int(z["nsteps"])
+        self.limiter = LIMITER[str(z["limiter"])]
+        self.solver = str(z["solver"])
+        self.ct = CT[str(z["ct"])]
+        self.cfl = float(z["cfl"])
+        self.cfl_max_var = float(z["cfl_max_var"])
+        self.first_dt = float(z["first_dt"])
