@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""Throughput of the B200 Godunov step on the 3-D 256^3 ideal-MHD blast.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one full RK2 step of the grid): 3-D ideal MHD, 256^3
+periodic on [0,1]^3, PLM with the MC limiter, HLLD, UCT_HLLD constrained
+transport, RK2, CFL 0.4, gamma 5/3; seeded blast initial condition (rho=1,
+p=0.1, p=10 inside r<0.1, uniform B at beta 0.1 along a seeded direction,
+divergence-free random velocity at rms 0.1).  Plain FP64 form; the mixed
+FP32-flux form is timed beside it.  Inputs are far larger than L2 (the
+state alone is ~2.5 GB), so no L2 flush is needed between steps.
+
+Multi-GPU: replicas only (one independent grid per rank, no data-path
+collective); value = zone updates of all ranks / max-over-ranks time.
+
+``--impl reference`` times the reference gPLUTO serial build (compiled from
+the reference sources into oracle/_ref by __graft_entry__.build()) on all
+host cores, one independent process per core, each step a bounded sample:
+one RK2 step of a 64^3 grid of the same scheme per process.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mzone-updates/s"
+WORKLOAD = "3d_ideal_mhd_blast_256^3"
+SCHEME = dict(limiter="mc", riemann="hlld", ct_emf="uct_hlld", cfl=0.4, cfl_max_var=1.1)
+FIRST_DT = 1e-4
+N = 256
+# algorithmic bytes per zone-update of the RK2 step (state read/written once
+# per stage: 5 x 8 B x (NVAR + n_face)) for 3-D ideal MHD
+ALG_BYTES_ZONE = 440
+# compulsory bytes per cell of each kernel of the FP64 3-D MHD step (arrays
+# it must read and write once, 8 B each), indexed by (kernel, stage)
+KERNEL_BYTES = {
+    ("sweep_x", 1): 168, ("sweep_x", 2): 168,
+    ("sweep_y", 1): 216, ("sweep_y", 2): 216,
+    ("sweep_z", 1): 248, ("sweep_z", 2): 288,
+    ("emf", 1): 192, ("emf", 2): 192,
+    ("finish", 1): 224, ("finish", 2): 248,
+}
+REF_SAMPLE_N = 64
+REF_BINARY = os.path.join(ROOT, "oracle", "_ref", "mhd3d_mc_lim_hlld_uct_hlld", "pluto")
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+# clocks sampled during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# reference (CPU) timing: the reference serial build, one process per core
+# --------------------------------------------------------------------------
+def _ref_available() -> bool:
+    return os.path.exists(REF_BINARY)
+
+
+def run_reference_sample(nproc: int, nsteps_timed: int, nwarm: int, n=REF_SAMPLE_N):
+    """Run `nproc` concurrent reference processes on n^3 blast grids.
+
+    Returns (Mzone-updates/s aggregate, mean s/step, cores, kind, sample text)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle", "ref"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from gpluto_dev_b200 import ics
+    total = nwarm + nsteps_timed
+    if _ref_available():
+        import build_ref as br
+        cfg = br.RefConfig(name="bench", physics="MHD", ndim=3, n=(n, n, n), limiter="MC_LIM",
+                           solver="hlld", ct_emf="UCT_HLLD", cfl=0.4, first_dt=FIRST_DT)
+        with tempfile.TemporaryDirectory() as tmp:
+            procs = []
+            for r in range(nproc):
+                d = os.path.join(tmp, f"p{r}")
+                os.makedirs(d)
+                open(os.path.join(d, "pluto.ini"), "w").write(cfg.ini())
+                icp = os.path.join(d, "ic.bin")
+                ics.write_ic(icp, ics.mhd3d_blast(n=(n, n, n), seed=1 + r))
+                env = dict(os.environ, GPLUTO_FTZ_DAZ="0", GP_IC_FILE=icp,
+                           GP_DUMP_STEP=str(total + 1), GP_DUMP_FILE=os.path.join(d, "out.dump"))
+                procs.append((d, subprocess.Popen([REF_BINARY, "-no-write", "-maxsteps",
+                                                   str(total + 1)], cwd=d, env=env,
+                                                  stdout=subprocess.DEVNULL,
+                                                  stderr=subprocess.DEVNULL)))
+            per = []
+            for d, p in procs:
+                p.wait()
+                dm = br.read_dump(os.path.join(d, "out.dump"))
+                w = dm.wall
+                per.append((w[nwarm + nsteps_timed] - w[nwarm]) / nsteps_timed)
+        kind = "reference"
+    else:  # C restatement of the reference (oracle port), one process per core
+        import oracle as orc
+        from concurrent.futures import ProcessPoolExecutor
+        import multiprocessing as mp
+        with ProcessPoolExecutor(nproc, mp_context=mp.get_context("spawn")) as ex:
+            per = list(ex.map(_oracle_worker, [(n, total, nwarm, r) for r in range(nproc)]))
+        kind = "port"
+    zones = n ** 3
+    value = sum(zones / t for t in per) / 1e6
+    sample = (f"{nproc} concurrent single-thread processes, each one {n}^3 grid of the same "
+              f"scheme, {nsteps_timed} timed RK2 steps after {nwarm} warm-up")
+    return value, statistics.mean(per), nproc, kind, sample
+
+
+def _oracle_worker(args):
+    n, total, nwarm, r = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    from gpluto_dev_b200 import ics
+    o = orc.Oracle(ics.mhd3d_blast(n=(n, n, n), seed=1 + r), limiter="mc", solver="hlld",
+                   ct="uct_hlld")
+    dt = FIRST_DT
+    for _ in range(nwarm):
+        inv, _ = o.step(dt)
+        dt = orc.lib().orc_next_dt(inv, 0.4, 1.1, dt)
+    t0 = time.perf_counter()
+    for _ in range(total - nwarm):
+        inv, _ = o.step(dt)
+        dt = orc.lib().orc_next_dt(inv, 0.4, 1.1, dt)
+    return (time.perf_counter() - t0) / (total - nwarm)
+
+
+def config_block():
+    return {"workload": WORKLOAD, "grid": [N, N, N], "physics": "ideal MHD",
+            "scheme": "PLM-MC + HLLD + UCT_HLLD + RK2, CFL 0.4, gamma 5/3",
+            "boundary": "periodic", "ic": "seeded blast (seed 1 + rank)",
+            "l2": "inputs larger than L2 (state ~2.5 GB), no flush"}
+
+
+def impl_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    ncores = os.cpu_count() or 1
+    nproc = max(1, min(ncores, 64))
+    value, sps, cores, kind, sample = run_reference_sample(nproc, args.steps, args.warmup)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_block(),
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+def impl_ours(args):
+    import torch
+    from gpluto_dev_b200 import api, ics
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    n = args.n
+    st = ics.mhd3d_blast(n=(n, n, n), seed=1 + rank)
+    ncell = n ** 3
+
+    def solver(precision):
+        sch = api.Scheme(physics=api.MHD, precision=precision, gamma=st.gamma, **SCHEME)
+        return api.Solver.from_state(st, sch)
+
+    # ---- plain FP64 form: timed region ---------------------------------
+    s64 = solver(api.FP64)
+    dt = FIRST_DT
+    dt, _, _ = s64.run(args.warmup, dt, history=False)
+    clock = ClockSampler(local)
+    torch.cuda.synchronize()
+    barrier()
+    clock.start()
+    time.sleep(0.25)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    dt_after, _, out = s64.run(args.steps, dt, history=False)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clock.stop()
+    barrier()
+    t_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    ms_step = t_ms / args.steps
+    value = world * ncell * args.steps / (t_ms * 1e-3) / 1e6
+    launches = args.steps * s64.launches_per_step
+
+    # ---- per-kernel timing (CUDA events around every launch) -----------
+    prof, _ = s64.profile(3, dt_after)
+    peak, peak_kind = peaks()
+    per_kernel = []
+    for name, stage, ms in prof:
+        b = KERNEL_BYTES.get((name, stage), 0) * ncell
+        per_kernel.append({"kernel": name, "stage": stage, "ms": ms,
+                           "gbs": b / (ms * 1e-3) / 1e9 if ms > 0 else None})
+    top = max(per_kernel, key=lambda k: k["ms"])
+    top_bytes = KERNEL_BYTES[(top["kernel"], top["stage"])] * ncell
+    achieved = top_bytes / (top["ms"] * 1e-3) / 1e9
+    step_gbs = ALG_BYTES_ZONE * ncell / (ms_step * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        tj = json.load(open(tpath))
+        traffic = tj.get(f"{top['kernel']}_stage{top['stage']}")
+    roofline = {"bound": "hbm", "kernel": f"{top['kernel']} (stage {top['stage']})",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "traffic": traffic,
+                "alg_bytes_per_launch": top_bytes, "launch_ms": top["ms"],
+                "step": {"alg_bytes_per_zone_update": ALG_BYTES_ZONE, "achieved": step_gbs,
+                         "frac": step_gbs / peak}}
+
+    # ---- mixed FP32-flux form ------------------------------------------
+    mixed = None
+    if not args.no_mixed:
+        del s64
+        torch.cuda.empty_cache()
+        smx = solver(api.MIXED)
+        d2, _, _ = smx.run(args.warmup, FIRST_DT, history=False)
+        torch.cuda.synchronize()
+        barrier()
+        e0.record()
+        smx.run(args.steps, d2, history=False)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        tm = e0.elapsed_time(e1)
+        if dist is not None:
+            tt = torch.tensor([tm], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            tm = float(tt.item())
+        mixed = {"value": world * ncell * args.steps / (tm * 1e-3) / 1e6,
+                 "ms_per_step": tm / args.steps}
+        mixed["speedup_vs_fp64"] = mixed["value"] / value
+        del smx
+        torch.cuda.empty_cache()
+
+    # ---- end to end through the C ABI with host buffers ------------------
+    # Per step: host (pinned) -> device upload of the full reference-layout
+    # state (Uc, Vc, Vs with ghost zones, as Data holds it), one AdvanceStep,
+    # device -> host download of the same arrays.
+    se = solver(api.FP64)
+    cshape, fshapes = se.reference_shapes()
+    hU = torch.empty(cshape, dtype=torch.float64, pin_memory=True)
+    hV = torch.empty(cshape, dtype=torch.float64, pin_memory=True)
+    hB = [torch.empty(f, dtype=torch.float64, pin_memory=True) for f in fshapes]
+    L = api.lib()
+
+    def dl():
+        api._check(L.gp_download_state(se._h, api.LAYOUT_REFERENCE, api._dp(hU), api._dp(hV),
+                                       api._dp(hB[0]), api._dp(hB[1]), api._dp(hB[2])))
+
+    dl()
+    k_e2e = max(1, min(args.steps, 10))
+    de = FIRST_DT
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(k_e2e):
+        api._check(L.gp_upload_state(se._h, api.LAYOUT_REFERENCE, api._dp(hU), api._dp(hV),
+                                     api._dp(hB[0]), api._dp(hB[1]), api._dp(hB[2])))
+        o = se.AdvanceStep(de)
+        de = api.NextTimeStep(o.invDt_hyp, 0.4, 1.1, de)
+        dl()
+    torch.cuda.synchronize()
+    te = time.perf_counter() - t0
+    if dist is not None:
+        tt = torch.tensor([te], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+    nbytes = (hU.numel() + hV.numel() + sum(b.numel() for b in hB)) * 8
+    e2e = {"value": world * ncell * k_e2e / te / 1e6, "unit": METRIC,
+           "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": k_e2e,
+           "path": "gp_upload_state(reference layout, pinned host) + gp_advance_step + "
+                   "gp_download_state(reference layout) per step"}
+    del se
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        nproc = max(1, min(os.cpu_count() or 1, 16))
+        v, sps, cores, kind, sample = run_reference_sample(nproc, 2, 1)
+        cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample}
+
+    if dist is not None:
+        barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded 3-D MHD blast initial conditions)",
+            "config": dict(config_block(), parallelism=f"replicas x{world}"),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clocks,
+            "forms": {"fp64": {"value": value, "ms_per_step": ms_step}, "mixed": mixed},
+            "kernels": per_kernel, "err_bits": out.err_bits}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N)
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return impl_reference(args)
+    return impl_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

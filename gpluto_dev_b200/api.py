@@ -1,0 +1,259 @@
+"""Python host side of the B200 Godunov step (ctypes over include/gpluto_b200.h).
+
+Mirrors the reference's step interface: :meth:`Solver.AdvanceStep` is
+``AdvanceStep(Data*, Grid*, timeStep*)`` (Src/rk_step.cpp:88) for one step
+of size dt, :func:`NextTimeStep` is ``NextTimeStep`` (Src/next_time_step.cpp:
+20-130), and :meth:`Solver.run` is the main loop of Src/main.cpp:320-485 with
+``-maxsteps`` (dt sequence kept on the device).
+
+There is no CPU path.  Constructing a :class:`Solver` without the built
+library or without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+
+import numpy as np
+
+from . import ics
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libgpluto_b200.so")
+
+GP_OK, GP_ERR_QUIT, GP_ERR_NO_DEVICE = 0, -5, -6
+HD, MHD, RMHD = 0, 1, 2
+LIMITERS = {"flat": 0, "minmod": 1, "vl": 2, "vanleer": 2, "mc": 3}
+SOLVERS = {"hll": 0, "hllc": 1, "hlld": 2}
+CT_AVG = {"uct_hll": 0, "uct_hlld": 1}
+FP64, MIXED = 0, 1
+LAYOUT_INTERIOR, LAYOUT_REFERENCE = 0, 1
+ERR_QUIT = 1 << 15
+
+
+class GpGridDesc(ctypes.Structure):
+    _fields_ = [("ndim", ctypes.c_int), ("nint", ctypes.c_int * 3), ("nghost", ctypes.c_int),
+                ("xbeg", ctypes.c_double * 3), ("xend", ctypes.c_double * 3),
+                ("dx", ctypes.POINTER(ctypes.c_double) * 3),
+                ("lbound", ctypes.c_int * 3), ("rbound", ctypes.c_int * 3)]
+
+
+class GpScheme(ctypes.Structure):
+    _fields_ = [("physics", ctypes.c_int), ("limiter", ctypes.c_int), ("riemann", ctypes.c_int),
+                ("ct_emf", ctypes.c_int), ("rk_stages", ctypes.c_int), ("precision", ctypes.c_int),
+                ("gamma", ctypes.c_double), ("cfl", ctypes.c_double),
+                ("cfl_max_var", ctypes.c_double), ("small_rho", ctypes.c_double),
+                ("small_prs", ctypes.c_double)]
+
+
+class GpStepOut(ctypes.Structure):
+    _fields_ = [("err_bits", ctypes.c_uint32), ("invDt_hyp", ctypes.c_double),
+                ("dt_next", ctypes.c_double)]
+
+
+class GPError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"gpluto_b200 error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load the in-tree shared library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} missing: run `python -m gpluto_dev_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        P, D = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+        L.gp_create.argtypes = [ctypes.POINTER(GpGridDesc), ctypes.POINTER(GpScheme), P,
+                                ctypes.POINTER(P)]
+        L.gp_destroy.argtypes = [P]
+        L.gp_upload_state.argtypes = [P, ctypes.c_int, D, D, D, D, D]
+        L.gp_download_state.argtypes = [P, ctypes.c_int, D, D, D, D, D]
+        L.gp_advance_step.argtypes = [P, ctypes.c_double, ctypes.POINTER(GpStepOut)]
+        L.gp_advance_steps.argtypes = [P, ctypes.c_int, D, D, ctypes.POINTER(GpStepOut)]
+        L.gp_next_time_step.restype = ctypes.c_double
+        L.gp_next_time_step.argtypes = [ctypes.c_double] * 4
+        L.gp_device_state.argtypes = [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(P * 3)]
+        L.gp_launches_per_step.argtypes = [P]
+        L.gp_profile_steps.argtypes = [P, ctypes.c_int, D, ctypes.POINTER(ctypes.c_float),
+                                       ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.gp_kernel_name.restype = ctypes.c_char_p
+        L.gp_kernel_name.argtypes = [P, ctypes.c_int]
+        L.gp_last_error.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != GP_OK:
+        raise GPError(rc, lib().gp_last_error().decode())
+
+
+def _dp(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    # torch tensor (host, possibly pinned)
+    return ctypes.cast(a.data_ptr(), ctypes.POINTER(ctypes.c_double))
+
+
+def NextTimeStep(invDt_hyp: float, cfl: float, cfl_max_var: float, dt: float) -> float:
+    """Src/next_time_step.cpp:80,125: min(cfl/invDt_hyp, cfl_max_var*dt)."""
+    return lib().gp_next_time_step(invDt_hyp, cfl, cfl_max_var, dt)
+
+
+@dataclasses.dataclass
+class Scheme:
+    physics: int = MHD
+    limiter: str = "mc"
+    riemann: str = "hlld"
+    ct_emf: str = "uct_hlld"
+    precision: int = FP64
+    gamma: float = 5.0 / 3.0
+    cfl: float = 0.4
+    cfl_max_var: float = 1.1
+    small_rho: float = 1e-12
+    small_prs: float = 1e-12
+
+    def to_c(self) -> GpScheme:
+        s = GpScheme()
+        s.physics = self.physics
+        s.limiter = LIMITERS[self.limiter]
+        s.riemann = SOLVERS[self.riemann]
+        s.ct_emf = CT_AVG[self.ct_emf]
+        s.rk_stages = 2
+        s.precision = self.precision
+        s.gamma, s.cfl, s.cfl_max_var = self.gamma, self.cfl, self.cfl_max_var
+        s.small_rho, s.small_prs = self.small_rho, self.small_prs
+        return s
+
+
+@dataclasses.dataclass
+class StepOut:
+    err_bits: int
+    invDt_hyp: float
+    dt_next: float
+
+
+class Solver:
+    """Device-resident state of one grid and its Godunov step."""
+
+    def __init__(self, ndim: int, shape, scheme: Scheme, xbeg=(0.0, 0.0, 0.0),
+                 xend=(1.0, 1.0, 1.0), nghost: int = 2, stream=None):
+        g = GpGridDesc()
+        g.ndim = ndim
+        nx, ny, nz = (tuple(shape) + (1, 1, 1))[:3]
+        g.nint[0], g.nint[1], g.nint[2] = nx, ny, (nz if ndim == 3 else 1)
+        g.nghost = nghost
+        for d in range(3):
+            g.xbeg[d], g.xend[d] = xbeg[d], xend[d]
+            g.lbound[d] = g.rbound[d] = 0
+        self.ndim, self.shape = ndim, (nx, ny, nz if ndim == 3 else 1)
+        self.scheme = scheme
+        self.nvar = 5 if scheme.physics == HD else 8
+        self.nghost = nghost
+        self._gdesc, self._sdesc = g, scheme.to_c()
+        h = ctypes.c_void_p()
+        sp = ctypes.c_void_p(stream) if stream is not None else None
+        _check(lib().gp_create(ctypes.byref(g), ctypes.byref(self._sdesc), sp, ctypes.byref(h)))
+        self._h = h
+
+    # -- construction helpers -------------------------------------------
+    @classmethod
+    def from_state(cls, st: "ics.PrimState", scheme: Scheme | None = None, **kw) -> "Solver":
+        scheme = scheme or Scheme(physics=st.physics, gamma=st.gamma)
+        scheme.gamma = st.gamma
+        s = cls(st.ndim, st.shape, scheme, st.xbeg, st.xend, **kw)
+        s.upload(st.V, None, st.Bs)
+        return s
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    # -- state transfer ---------------------------------------------------
+    def upload(self, V, U=None, Bs=None, layout=LAYOUT_INTERIOR):
+        """Host -> device (Uc=None: start-up PrimToCons on the device)."""
+        bs = list(Bs or []) + [None] * 3
+        _check(lib().gp_upload_state(self._h, layout, _dp(U), _dp(V), _dp(bs[0]), _dp(bs[1]),
+                                     _dp(bs[2])))
+
+    def download(self, layout=LAYOUT_INTERIOR):
+        """Device -> host: (V, U, Bs) in the interior layout."""
+        nx, ny, nz = self.shape
+        if layout != LAYOUT_INTERIOR:
+            raise ValueError("use download_reference for the ghosted layout")
+        V = np.empty((self.nvar, nz, ny, nx))
+        U = np.empty_like(V)
+        Bs = [np.empty((nz, ny, nx)) for _ in range(self.ndim)] if self.scheme.physics != HD else []
+        bs = Bs + [None] * 3
+        _check(lib().gp_download_state(self._h, layout, _dp(U), _dp(V), _dp(bs[0]), _dp(bs[1]),
+                                       _dp(bs[2])))
+        return V, U, Bs
+
+    def reference_shapes(self):
+        """Shapes of Data::Uc/Vc and Data::Vs[d] including ghost zones."""
+        g = self.nghost
+        n = list(self.shape)
+        tot = [n[d] + (2 * g if d < self.ndim else 0) for d in range(3)]
+        cell = (self.nvar, tot[2], tot[1], tot[0])
+        faces = []
+        for d in range(self.ndim):
+            t = list(tot)
+            t[d] += 1
+            faces.append((t[2], t[1], t[0]))
+        return cell, faces
+
+    # -- stepping ----------------------------------------------------------
+    def AdvanceStep(self, dt: float) -> StepOut:
+        """One RK2 step (Src/rk_step.cpp:88-593); raises on ERR_QUIT."""
+        out = GpStepOut()
+        _check(lib().gp_advance_step(self._h, dt, ctypes.byref(out)))
+        return StepOut(out.err_bits, out.invDt_hyp, out.dt_next)
+
+    def run(self, nsteps: int, dt: float, history: bool = True):
+        """``nsteps`` steps with the device-side dt sequence.
+
+        Returns (dt_after, dt_hist, StepOut)."""
+        d = ctypes.c_double(dt)
+        hist = np.zeros(max(nsteps, 1)) if history else None
+        out = GpStepOut()
+        _check(lib().gp_advance_steps(self._h, nsteps, ctypes.byref(d), _dp(hist),
+                                      ctypes.byref(out)))
+        return d.value, (hist[:nsteps] if history else None), StepOut(out.err_bits,
+                                                                       out.invDt_hyp,
+                                                                       out.dt_next)
+
+    def profile(self, nsteps: int, dt: float):
+        """Mean per-launch kernel times (ms) over ``nsteps`` instrumented steps.
+
+        Returns (list of (name, stage, ms), dt_after)."""
+        buf = (ctypes.c_float * 64)()
+        nk = ctypes.c_int(0)
+        d = ctypes.c_double(dt)
+        _check(lib().gp_profile_steps(self._h, nsteps, ctypes.byref(d), buf, 64, ctypes.byref(nk)))
+        per = nk.value // 2
+        res = [(lib().gp_kernel_name(self._h, q).decode(), 1 + q // per, float(buf[q]))
+               for q in range(nk.value)]
+        return res, d.value
+
+    def device_pointers(self):
+        u, v = ctypes.c_void_p(), ctypes.c_void_p()
+        bs = (ctypes.c_void_p * 3)()
+        _check(lib().gp_device_state(self._h, ctypes.byref(u), ctypes.byref(v), ctypes.byref(bs)))
+        return u.value, v.value, [bs[i] for i in range(3)]
+
+    @property
+    def launches_per_step(self) -> int:
+        return lib().gp_launches_per_step(self._h)

@@ -1,0 +1,68 @@
+"""Build the sm_100a shared library of the Godunov step (in-tree).
+
+    python -m gpluto_dev_b200.build
+
+Produces gpluto_dev_b200/_build/libgpluto_b200.so from csrc/ with nvcc:
+gp_launch.cu twice (FP64 form with -fmad=false so the plain form keeps the
+reference's rounding sequence; mixed form with contraction), gp_api.cu for
+the C ABI.  Objects are rebuilt only when a source is newer.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "_build")
+LIB = os.path.join(OUT, "libgpluto_b200.so")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+BASE = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+
+UNITS = [
+    ("gp_launch_fp64.o", "gp_launch.cu", ["-DGP_MIXED=0", "-fmad=false"]),
+    ("gp_launch_mixed.o", "gp_launch.cu", ["-DGP_MIXED=1", "-fmad=true"]),
+    ("gp_api.o", "gp_api.cu", ["-fmad=false"]),
+]
+
+
+def nvcc() -> str:
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def _deps() -> list:
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [
+        os.path.join(os.path.dirname(HERE), "include", "gpluto_b200.h")]
+
+
+def build(verbose: bool = False, jobs: int = 3) -> str:
+    os.makedirs(OUT, exist_ok=True)
+    newest = max(os.path.getmtime(p) for p in _deps())
+    procs = []
+    objs = []
+    for obj, src, flags in UNITS:
+        o = os.path.join(OUT, obj)
+        objs.append(o)
+        if os.path.exists(o) and os.path.getmtime(o) >= newest:
+            continue
+        cmd = [nvcc(), *ARCH, *BASE, *flags, "-c", os.path.join(CSRC, src), "-o", o]
+        if verbose:
+            print(" ".join(cmd))
+        procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+    for cmd, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + out.decode()[-6000:])
+    if (not os.path.exists(LIB)) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

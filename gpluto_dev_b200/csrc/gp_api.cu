@@ -1,0 +1,543 @@
+// gp_api.cu -- C ABI (include/gpluto_b200.h) over the sm_100a stage kernels.
+//
+// Owns the device state of one grid, orders the RK2 stages exactly like
+// AdvanceStep (Src/rk_step.cpp:88-593) and keeps the dt sequence on the
+// device so that many steps run without a host round trip
+// (NextTimeStep, Src/next_time_step.cpp:20-130, evaluated by a one-thread
+// kernel after each step).  There is no CPU fallback: every entry point that
+// computes fails with GP_ERR_NO_DEVICE when no CUDA device is present.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "../../include/gpluto_b200.h"
+#include "gp_launch.h"
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CUDA_TRY(call)                                                              \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess)                                                          \
+      return fail(GP_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                  __FILE__, __LINE__);                                              \
+  } while (0)
+
+// Per-step scalars living in device memory.
+struct StepScalars {
+  double dt;                 // dt of the step about to run
+  double dtdx[3];            // dt/dx_d for that step
+  double invdt;              // stage-1 invDt_hyp of the last step
+  double dt_next;            // NextTimeStep of the last step
+  unsigned long long invdt_bits;  // running max of C_dt (stage 1)
+  uint32_t err;              // OR of error bits since the last reset
+  uint32_t pad;
+};
+
+// NextTimeStep + bookkeeping; one thread.  Src/update_stage.cpp:422-435
+// (invDt_hyp = max(C_dt)/dim) and Src/next_time_step.cpp:80,125.
+__global__ void dt_update_kernel(StepScalars* sc, double ndim, double cfl, double cfl_max_var,
+                                 double dx0, double dx1, double dx2, double* hist, int slot) {
+  double mx = __longlong_as_double((long long)sc->invdt_bits);
+  double inv = mx / ndim;
+  double dt = sc->dt;
+  if (hist) hist[slot] = dt;
+  double dtn = cfl / inv;
+  dtn = (dtn <= cfl_max_var * dt) ? dtn : cfl_max_var * dt;
+  sc->invdt = inv;
+  sc->dt_next = dtn;
+  sc->dt = dtn;
+  sc->dtdx[0] = dtn / dx0;
+  sc->dtdx[1] = dtn / dx1;
+  sc->dtdx[2] = dtn / dx2;
+  sc->invdt_bits = 0ull;
+}
+
+// interior <-> reference (ghosted) layout for one 3-D array
+__global__ void gather_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                              int nvar, int sx, int sy, int sz, int ox, int oy, int oz,
+                              int nx, int ny, int nz) {
+  long long n = (long long)nx * ny * nz;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * nvar) return;
+  int nv = (int)(t / n);
+  long long c = t - (long long)nv * n;
+  int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+  long long s = (long long)(i + ox) + (long long)sx * ((j + oy) + (long long)sy * (k + oz));
+  dst[t] = src[(long long)nv * sx * sy * sz + s];
+}
+
+// fill a ghosted array from the interior with periodic wrap (what Boundary()
+// produces for periodic sides); `stag` adds the extra face along that dir.
+__global__ void scatter_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                               int nvar, int sx, int sy, int sz, int ox, int oy, int oz,
+                               int nx, int ny, int nz) {
+  long long ns = (long long)sx * sy * sz;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns * nvar) return;
+  int nv = (int)(t / ns);
+  long long s = t - (long long)nv * ns;
+  int i = (int)(s % sx), j = (int)((s / sx) % sy), k = (int)(s / ((long long)sx * sy));
+  int ii = ((i - ox) % nx + nx) % nx, jj = ((j - oy) % ny + ny) % ny, kk = ((k - oz) % nz + nz) % nz;
+  dst[t] = src[(long long)nv * nx * ny * nz + ii + (long long)nx * (jj + (long long)ny * kk)];
+}
+
+bool uniform(const double* dx, int n) {
+  if (!dx) return true;
+  for (int i = 1; i < n; i++)
+    if (dx[i] != dx[0]) return false;
+  return true;
+}
+
+}  // namespace
+
+struct gp_handle {
+  gp_grid_desc grid;
+  gp_scheme scheme;
+  int nx, ny, nz, ndim, nvar, ng;
+  long long n;
+  double dx[3];
+  cudaStream_t stream;
+  bool mixed;
+  gp::SchemeKey key;
+  int seg;
+  // device state
+  double* U[2];
+  double* V;
+  double* dU;
+  double* Cdt;
+  double* Bs[3][3];   // [rotation buffer][component]
+  int bcur;           // buffer holding B^n
+  void* ct[3][6];
+  double* Ee[3];
+  StepScalars* sc;
+  StepScalars* sc_host;  // pinned mirror
+  double* hist;
+  int hist_cap;
+  double* stage_buf;     // device staging for reference-layout transfers
+  size_t stage_bytes;
+  int launches_per_step;
+};
+
+namespace {
+
+void free_all(gp_handle* h) {
+  cudaFree(h->U[0]);
+  cudaFree(h->U[1]);
+  cudaFree(h->V);
+  cudaFree(h->dU);
+  cudaFree(h->Cdt);
+  for (int b = 0; b < 3; b++)
+    for (int d = 0; d < 3; d++) cudaFree(h->Bs[b][d]);
+  for (int d = 0; d < 3; d++) {
+    for (int r = 0; r < 6; r++) cudaFree(h->ct[d][r]);
+    cudaFree(h->Ee[d]);
+  }
+  cudaFree(h->sc);
+  cudaFreeHost(h->sc_host);
+  cudaFree(h->hist);
+  cudaFree(h->stage_buf);
+}
+
+int enqueue_step(gp_handle* h, double* hist, int slot, cudaEvent_t* ev = nullptr) {
+  const int b0 = h->bcur, b1 = (h->bcur + 1) % 3, b2 = (h->bcur + 2) % 3;
+  const bool mhd = h->scheme.physics != GP_HD;
+  gp::StageDesc d;
+  std::memset(&d, 0, sizeof(d));
+  d.dU = h->dU;
+  d.Cdt = h->Cdt;
+  for (int q = 0; q < 3; q++) {
+    d.dx[q] = h->dx[q];
+    d.Ee[q] = h->Ee[q];
+    for (int r = 0; r < 6; r++) d.ct[q][r] = h->ct[q][r];
+  }
+  d.dtdx = h->sc->dtdx;
+  d.gamma = h->scheme.gamma;
+  d.small_rho = h->scheme.small_rho;
+  d.small_prs = h->scheme.small_prs;
+  d.invdt_bits = &h->sc->invdt_bits;
+  d.err = &h->sc->err;
+  const int per_stage = gp::stage_launch_count(h->key);
+  auto launch = [&](const gp::StageDesc& sd) {
+    gp::GridDims g{h->nx, h->ny, h->nz, h->n};
+    cudaEvent_t* e = ev ? ev + (sd.stage - 1) * 2 * per_stage : nullptr;
+    return h->mixed ? gp::launch_stage_mixed(sd, g, h->key, h->seg, h->stream, e)
+                    : gp::launch_stage_fp64(sd, g, h->key, h->seg, h->stream, e);
+  };
+  // stage 1: (U^n, B^n) -> (U1, B1)
+  d.stage = 1;
+  d.V = h->V;
+  d.Vout = h->V;
+  d.U0 = h->U[0];
+  d.Uc = h->U[0];
+  d.Uout = h->U[1];
+  for (int q = 0; q < 3; q++) {
+    d.Bs[q] = mhd ? h->Bs[b0][q] : nullptr;
+    d.Bs0[q] = d.Bs[q];
+    d.Bsout[q] = mhd ? h->Bs[b1][q] : nullptr;
+  }
+  if (launch(d) != 0) return fail(GP_ERR_UNSUPPORTED, "scheme not compiled");
+  // stage 2: (U^n, U1, B^n, B1) -> (U^{n+1} in place of U^n, B^{n+1})
+  d.stage = 2;
+  d.Uc = h->U[1];
+  d.Uout = h->U[0];
+  for (int q = 0; q < 3; q++) {
+    d.Bs[q] = mhd ? h->Bs[b1][q] : nullptr;
+    d.Bs0[q] = mhd ? h->Bs[b0][q] : nullptr;
+    d.Bsout[q] = mhd ? h->Bs[b2][q] : nullptr;
+  }
+  if (launch(d) != 0) return fail(GP_ERR_UNSUPPORTED, "scheme not compiled");
+  dt_update_kernel<<<1, 1, 0, h->stream>>>(h->sc, (double)h->ndim, h->scheme.cfl,
+                                          h->scheme.cfl_max_var, h->dx[0], h->dx[1], h->dx[2],
+                                          hist, slot);
+  CUDA_TRY(cudaGetLastError());
+  h->bcur = b2;
+  return GP_OK;
+}
+
+int set_dt(gp_handle* h, double dt) {
+  h->sc_host->dt = dt;
+  for (int q = 0; q < 3; q++) h->sc_host->dtdx[q] = dt / h->dx[q];
+  h->sc_host->invdt = 0.0;
+  h->sc_host->dt_next = 0.0;
+  h->sc_host->invdt_bits = 0ull;
+  h->sc_host->err = 0u;
+  CUDA_TRY(cudaMemcpyAsync(h->sc, h->sc_host, sizeof(StepScalars), cudaMemcpyHostToDevice,
+                           h->stream));
+  return GP_OK;
+}
+
+int check_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+    return fail(GP_ERR_NO_DEVICE, "no CUDA device: the Godunov step has no CPU path");
+  return GP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gp_last_error(void) { return g_err; }
+
+double gp_next_time_step(double invDt_hyp, double cfl, double cfl_max_var, double dt) {
+  double dt_new = cfl / invDt_hyp;
+  return (dt_new <= cfl_max_var * dt) ? dt_new : cfl_max_var * dt;
+}
+
+int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
+              gp_handle** out) {
+  if (!grid || !scheme || !out) return fail(GP_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (grid->ndim != 2 && grid->ndim != 3) return fail(GP_ERR_UNSUPPORTED, "ndim must be 2 or 3");
+  if (scheme->physics != GP_MHD && scheme->physics != GP_HD)
+    return fail(GP_ERR_UNSUPPORTED, "physics %d not built", scheme->physics);
+  if (scheme->rk_stages != 2) return fail(GP_ERR_UNSUPPORTED, "only RK2 is built");
+  if (scheme->precision != GP_FP64 && scheme->precision != GP_MIXED)
+    return fail(GP_ERR_INVALID, "bad precision");
+  for (int d = 0; d < 3; d++) {
+    if (d < grid->ndim) {
+      if (grid->nint[d] < 2) return fail(GP_ERR_INVALID, "nint[%d] < 2", d);
+      if (grid->lbound[d] != GP_BC_PERIODIC || grid->rbound[d] != GP_BC_PERIODIC)
+        return fail(GP_ERR_UNSUPPORTED, "only periodic boundaries are built");
+      if (!uniform(grid->dx[d], grid->nint[d] + 2 * grid->nghost))
+        return fail(GP_ERR_UNSUPPORTED, "non-uniform grid along %d", d);
+    }
+  }
+  if (scheme->physics == GP_MHD && scheme->riemann == GP_RS_HLLC)
+    return fail(GP_ERR_UNSUPPORTED, "MHD HLLC not built");
+  if (scheme->physics == GP_HD && scheme->riemann == GP_RS_HLLD)
+    return fail(GP_ERR_UNSUPPORTED, "HD has no HLLD solver");
+  if (scheme->limiter < GP_LIM_MINMOD || scheme->limiter > GP_LIM_MC)
+    return fail(GP_ERR_UNSUPPORTED, "limiter %d not built", scheme->limiter);
+  int rc = check_device();
+  if (rc) return rc;
+  gp_handle* h = new (std::nothrow) gp_handle;
+  if (!h) return fail(GP_ERR_NOMEM, "host allocation");
+  std::memset(h, 0, sizeof(*h));
+  h->grid = *grid;
+  h->scheme = *scheme;
+  h->ndim = grid->ndim;
+  h->nx = grid->nint[0];
+  h->ny = grid->nint[1];
+  h->nz = grid->ndim == 3 ? grid->nint[2] : 1;
+  h->n = (long long)h->nx * h->ny * h->nz;
+  h->nvar = scheme->physics == GP_HD ? 5 : 8;
+  h->ng = grid->nghost;
+  for (int d = 0; d < 3; d++) {
+    int nn = (d == 0 ? h->nx : d == 1 ? h->ny : h->nz);
+    h->dx[d] = (grid->dx[d] && d < grid->ndim) ? grid->dx[d][0]
+                                               : (grid->xend[d] - grid->xbeg[d]) / nn;
+    if (!(h->dx[d] > 0.0)) h->dx[d] = 1.0;
+  }
+  h->stream = (cudaStream_t)stream;
+  h->mixed = scheme->precision == GP_MIXED;
+  h->key = gp::SchemeKey{scheme->physics, grid->ndim, scheme->riemann, scheme->ct_emf,
+                         scheme->limiter};
+  // pencil segment for the marching sweeps: enough threads to fill 148 SMs
+  {
+    long long cols = (long long)h->nx * (h->ndim == 3 ? h->nz : 1);
+    int nd = h->ny;
+    int seg = 64;
+    while (seg > 4 && cols * ((nd + seg - 1) / seg) < 148LL * 1024) seg /= 2;
+    h->seg = seg;
+  }
+  const size_t cell = sizeof(double) * h->n;
+  const size_t ctb = (h->mixed ? sizeof(float) : sizeof(double)) * h->n;
+  bool ok = true;
+  auto alloc = [&](void** p, size_t b) {
+    if (ok && cudaMalloc(p, b) != cudaSuccess) ok = false;
+  };
+  alloc((void**)&h->U[0], cell * h->nvar);
+  alloc((void**)&h->U[1], cell * h->nvar);
+  alloc((void**)&h->V, cell * h->nvar);
+  alloc((void**)&h->dU, cell * h->nvar);
+  alloc((void**)&h->Cdt, cell);
+  if (scheme->physics != GP_HD) {
+    for (int b = 0; b < 3; b++)
+      for (int d = 0; d < h->ndim; d++) alloc((void**)&h->Bs[b][d], cell);
+    for (int d = 0; d < h->ndim; d++)
+      for (int r = 0; r < 6; r++) alloc(&h->ct[d][r], ctb);
+    for (int d = 0; d < 3; d++)
+      if (h->ndim == 3 || d == 2) alloc((void**)&h->Ee[d], cell);
+  }
+  alloc((void**)&h->sc, sizeof(StepScalars));
+  if (ok && cudaMallocHost((void**)&h->sc_host, sizeof(StepScalars)) != cudaSuccess) ok = false;
+  if (!ok) {
+    cudaGetLastError();
+    long long ncell = h->n;
+    free_all(h);
+    delete h;
+    return fail(GP_ERR_NOMEM, "device allocation failed for %lld cells", ncell);
+  }
+  cudaMemsetAsync(h->sc, 0, sizeof(StepScalars), h->stream);
+  cudaMemsetAsync(h->dU, 0, cell * h->nvar, h->stream);
+  h->bcur = 0;
+  h->launches_per_step = 2 * gp::stage_launch_count(h->key) + 1;
+  *out = h;
+  return GP_OK;
+}
+
+int gp_destroy(gp_handle* h) {
+  if (!h) return GP_OK;
+  cudaStreamSynchronize(h->stream);
+  free_all(h);
+  delete h;
+  return GP_OK;
+}
+
+static int ensure_stage(gp_handle* h, size_t bytes) {
+  if (h->stage_bytes >= bytes) return GP_OK;
+  cudaFree(h->stage_buf);
+  h->stage_buf = nullptr;
+  h->stage_bytes = 0;
+  CUDA_TRY(cudaMalloc((void**)&h->stage_buf, bytes));
+  h->stage_bytes = bytes;
+  return GP_OK;
+}
+
+// reference-layout extents of a cell array (s*) and its interior offset (o*)
+static void ref_dims(const gp_handle* h, int stag, int* s, int* o) {
+  int n[3] = {h->nx, h->ny, h->nz};
+  for (int d = 0; d < 3; d++) {
+    bool act = d < h->ndim;
+    s[d] = n[d] + (act ? 2 * h->ng : 0) + (stag == d ? 1 : 0);
+    o[d] = act ? h->ng : 0;
+  }
+}
+
+static int upload_one(gp_handle* h, int layout, const double* src, double* dst, int nvar,
+                      int stag) {
+  const size_t nb = sizeof(double) * h->n * nvar;
+  if (layout == GP_LAYOUT_INTERIOR) {
+    CUDA_TRY(cudaMemcpyAsync(dst, src, nb, cudaMemcpyHostToDevice, h->stream));
+    return GP_OK;
+  }
+  int s[3], o[3];
+  ref_dims(h, stag, s, o);
+  size_t tot = sizeof(double) * (size_t)s[0] * s[1] * s[2] * nvar;
+  int rc = ensure_stage(h, tot);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(h->stage_buf, src, tot, cudaMemcpyHostToDevice, h->stream));
+  long long work = h->n * nvar;
+  gather_kernel<<<(unsigned)((work + 255) / 256), 256, 0, h->stream>>>(
+      h->stage_buf, dst, nvar, s[0], s[1], s[2], o[0], o[1], o[2], h->nx, h->ny, h->nz);
+  CUDA_TRY(cudaGetLastError());
+  return GP_OK;
+}
+
+static int download_one(gp_handle* h, int layout, const double* src, double* dst, int nvar,
+                        int stag) {
+  const size_t nb = sizeof(double) * h->n * nvar;
+  if (layout == GP_LAYOUT_INTERIOR) {
+    CUDA_TRY(cudaMemcpyAsync(dst, src, nb, cudaMemcpyDeviceToHost, h->stream));
+    return GP_OK;
+  }
+  int s[3], o[3];
+  ref_dims(h, stag, s, o);
+  long long tot = (long long)s[0] * s[1] * s[2] * nvar;
+  int rc = ensure_stage(h, sizeof(double) * tot);
+  if (rc) return rc;
+  scatter_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, h->stream>>>(
+      src, h->stage_buf, nvar, s[0], s[1], s[2], o[0], o[1], o[2], h->nx, h->ny, h->nz);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(dst, h->stage_buf, sizeof(double) * tot, cudaMemcpyDeviceToHost,
+                           h->stream));
+  return GP_OK;
+}
+
+int gp_upload_state(gp_handle* h, int layout, const double* Uc, const double* Vc,
+                    const double* Vs0, const double* Vs1, const double* Vs2) {
+  if (!h || !Vc) return fail(GP_ERR_INVALID, "null handle or Vc");
+  if (layout != GP_LAYOUT_INTERIOR && layout != GP_LAYOUT_REFERENCE)
+    return fail(GP_ERR_INVALID, "bad layout");
+  int rc = upload_one(h, layout, Vc, h->V, h->nvar, -1);
+  if (rc) return rc;
+  if (Uc) {
+    rc = upload_one(h, layout, Uc, h->U[0], h->nvar, -1);
+  } else {
+    rc = gp::launch_prim2cons(h->scheme.physics, h->V, h->U[0], h->n, h->scheme.gamma,
+                              h->stream);
+    if (rc) return fail(GP_ERR_UNSUPPORTED, "prim2cons not built for this physics");
+  }
+  if (rc) return rc;
+  if (h->scheme.physics != GP_HD) {
+    const double* vs[3] = {Vs0, Vs1, Vs2};
+    for (int d = 0; d < h->ndim; d++) {
+      if (!vs[d]) return fail(GP_ERR_INVALID, "missing Vs%d", d);
+      rc = upload_one(h, layout, vs[d], h->Bs[h->bcur][d], 1, d);
+      if (rc) return rc;
+    }
+  }
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return GP_OK;
+}
+
+int gp_download_state(gp_handle* h, int layout, double* Uc, double* Vc, double* Vs0,
+                      double* Vs1, double* Vs2) {
+  if (!h) return fail(GP_ERR_INVALID, "null handle");
+  int rc;
+  if (Uc && (rc = download_one(h, layout, h->U[0], Uc, h->nvar, -1))) return rc;
+  if (Vc && (rc = download_one(h, layout, h->V, Vc, h->nvar, -1))) return rc;
+  if (h->scheme.physics != GP_HD) {
+    double* vs[3] = {Vs0, Vs1, Vs2};
+    for (int d = 0; d < h->ndim; d++)
+      if (vs[d] && (rc = download_one(h, layout, h->Bs[h->bcur][d], vs[d], 1, d))) return rc;
+  }
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return GP_OK;
+}
+
+int gp_advance_step(gp_handle* h, double dt, gp_step_out* out) {
+  if (!h) return fail(GP_ERR_INVALID, "null handle");
+  if (!(dt > 0.0)) return fail(GP_ERR_INVALID, "dt must be > 0");
+  int rc = set_dt(h, dt);
+  if (rc) return rc;
+  rc = enqueue_step(h, nullptr, 0);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(StepScalars), cudaMemcpyDeviceToHost,
+                           h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (out) {
+    out->err_bits = h->sc_host->err;
+    out->invDt_hyp = h->sc_host->invdt;
+    out->dt_next = h->sc_host->dt_next;
+  }
+  if (h->sc_host->err & (1u << 15)) return fail(GP_ERR_QUIT, "ERR_QUIT raised (bits 0x%x)", h->sc_host->err);
+  return GP_OK;
+}
+
+int gp_advance_steps(gp_handle* h, int nsteps, double* dt, double* dt_hist, gp_step_out* out) {
+  if (!h || !dt) return fail(GP_ERR_INVALID, "null argument");
+  if (nsteps < 0) return fail(GP_ERR_INVALID, "nsteps < 0");
+  if (!(*dt > 0.0)) return fail(GP_ERR_INVALID, "dt must be > 0");
+  int rc = set_dt(h, *dt);
+  if (rc) return rc;
+  if (dt_hist && h->hist_cap < nsteps) {
+    cudaFree(h->hist);
+    h->hist = nullptr;
+    h->hist_cap = 0;
+    CUDA_TRY(cudaMalloc((void**)&h->hist, sizeof(double) * nsteps));
+    h->hist_cap = nsteps;
+  }
+  for (int s = 0; s < nsteps; s++) {
+    rc = enqueue_step(h, dt_hist ? h->hist : nullptr, s);
+    if (rc) return rc;
+  }
+  CUDA_TRY(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(StepScalars), cudaMemcpyDeviceToHost,
+                           h->stream));
+  if (dt_hist && nsteps > 0)
+    CUDA_TRY(cudaMemcpyAsync(dt_hist, h->hist, sizeof(double) * nsteps, cudaMemcpyDeviceToHost,
+                             h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  *dt = h->sc_host->dt;
+  if (out) {
+    out->err_bits = h->sc_host->err;
+    out->invDt_hyp = h->sc_host->invdt;
+    out->dt_next = h->sc_host->dt_next;
+  }
+  if (h->sc_host->err & (1u << 15)) return fail(GP_ERR_QUIT, "ERR_QUIT raised (bits 0x%x)", h->sc_host->err);
+  return GP_OK;
+}
+
+int gp_device_state(gp_handle* h, double** Uc, double** Vc, double** Vs) {
+  if (!h) return fail(GP_ERR_INVALID, "null handle");
+  if (Uc) *Uc = h->U[0];
+  if (Vc) *Vc = h->V;
+  if (Vs)
+    for (int d = 0; d < 3; d++) Vs[d] = h->Bs[h->bcur][d];
+  return GP_OK;
+}
+
+int gp_launches_per_step(const gp_handle* h) { return h ? h->launches_per_step : 0; }
+
+int gp_profile_steps(gp_handle* h, int nsteps, double* dt, float* kernel_ms, int cap,
+                     int* nkernels) {
+  if (!h || !dt || !kernel_ms || !nkernels) return fail(GP_ERR_INVALID, "null argument");
+  const int nk = 2 * gp::stage_launch_count(h->key);
+  *nkernels = nk;
+  if (cap < nk) return fail(GP_ERR_INVALID, "kernel_ms needs %d entries", nk);
+  for (int q = 0; q < nk; q++) kernel_ms[q] = 0.f;
+  int rc = set_dt(h, *dt);
+  if (rc) return rc;
+  cudaEvent_t ev[64];
+  for (int q = 0; q < 2 * nk; q++) CUDA_TRY(cudaEventCreate(&ev[q]));
+  for (int s = 0; s < nsteps && rc == GP_OK; s++) {
+    rc = enqueue_step(h, nullptr, 0, ev);
+    if (rc) break;
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) { rc = fail(GP_ERR_CUDA, "%s", cudaGetErrorString(e)); break; }
+    for (int q = 0; q < nk; q++) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[2 * q], ev[2 * q + 1]);
+      kernel_ms[q] += ms;
+    }
+  }
+  for (int q = 0; q < 2 * nk; q++) cudaEventDestroy(ev[q]);
+  if (rc) return rc;
+  for (int q = 0; q < nk; q++) kernel_ms[q] /= (nsteps > 0 ? nsteps : 1);
+  CUDA_TRY(cudaMemcpy(h->sc_host, h->sc, sizeof(StepScalars), cudaMemcpyDeviceToHost));
+  *dt = h->sc_host->dt;
+  return GP_OK;
+}
+
+const char* gp_kernel_name(const gp_handle* h, int idx) {
+  if (!h) return "?";
+  const int per = gp::stage_launch_count(h->key);
+  return gp::stage_kernel_name(h->key, idx % per);
+}
+
+}  // extern "C"

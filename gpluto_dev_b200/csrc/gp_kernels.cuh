@@ -1,0 +1,546 @@
+// gp_kernels.cuh -- fused stage kernels of the Godunov step (sm_100a).
+//
+// Device layout (one grid): interior cells only, structure of arrays,
+// x fastest: cell (i,j,k) of variable nv sits at nv*n + i + nx*(j + ny*k).
+// Face-normal fields Bs[d] hold the LEFT face of each cell (x_d = i_d - 1/2);
+// periodic ghost zones are index wrap-around, never copies (the reference
+// fills ghosts by copy, Src/boundary.cpp:502-675; with periodic data the two
+// give identical operands, so results agree bit for bit).
+//
+// One RK stage (Src/update_stage.cpp:57-438 + Src/rk_step.cpp:357-593):
+//   sweep_x   : warp per x-row; PLM + Riemann per face, flux difference into
+//               dU (=), per-cell inverse dt into Cdt (=), UCT face data.
+//   sweep_m<d>: thread per (x, pencil segment) marching along y or z with a
+//               register window; dU (+=), Cdt (+=); the last direction fuses
+//               the RK combine (writes U_out) and the stage-1 CFL max.
+//   emf       : thread per cell, its three edge EMFs (UCT_HLLD / UCT_HLL
+//               composition, Src/MHD/CT/ct_emf_average.cpp:535-995).
+//   finish    : thread per cell: CT face update of its left faces (and the
+//               right faces recomputed for the cell average), RK combine of
+//               the faces, cell-centred B average, con2prim -> V, U fixups.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gp_phys.cuh"
+
+namespace gp {
+
+struct Grid3 {
+  int nx, ny, nz;
+  long long n;  // nx*ny*nz
+};
+
+template <typename CTT>
+struct StageArgs {
+  const double* V;        // [nvar][n] primitives at stage start
+  const double* Bs[3];    // stage-input face fields (left faces)
+  const double* Bs0[3];   // face fields at t^n (stage 2)
+  double* Bsout[3];       // face fields written by this stage
+  double* dU;             // [nvar][n] rhs accumulator
+  double* Cdt;            // [n] inverse dt accumulator
+  const double* U0;       // U^n
+  const double* Uc;       // stage-input U
+  double* Uout;           // U written by this stage
+  double* Vout;           // primitives written by this stage
+  CTT* ct[3][6];          // UCT face data per direction: eb, et, aL, aR, dL, dR
+  double* Ee[3];          // edge EMFs: Ee[0]=Ex(i,j-1/2,k-1/2), Ee[1]=Ey, Ee[2]=Ez
+  const double* dtdx;     // dt/dx_d (3 values in device memory, set per step)
+  double dx[3];
+  double gamma, small_rho, small_prs;
+  int stage;              // 1 or 2 (RK2)
+  unsigned long long* invdt_bits;  // max over cells of Cdt (stage 1)
+  uint32_t* err;          // OR of error bits
+};
+
+__device__ __forceinline__ int wrapi(int i, int n) {
+  return i < 0 ? i + n : (i >= n ? i - n : i);
+}
+
+template <int NV, typename R>
+__device__ __forceinline__ void load_cell(const double* __restrict__ V, long long n,
+                                          long long c, R* v) {
+#pragma unroll
+  for (int nv = 0; nv < NV; nv++) v[nv] = (R)__ldg(V + nv * n + c);
+}
+
+__device__ __forceinline__ void atomic_max_pos(unsigned long long* addr, double v) {
+  // non-negative doubles order like their bit patterns
+  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+// whether conserved component nv receives a flux difference that survives
+// the stage (the cell-centred field along active directions is overwritten
+// by the face average, Src/MHD/CT/ct_field_average.cpp:378-410)
+template <int PHYS, int NDIM>
+__device__ __forceinline__ constexpr bool rhs_var(int nv) {
+  return !(PHYS != PHYS_HD && nv >= BX1 && nv < BX1 + NDIM);
+}
+
+// Riemann dispatch for one interface.
+template <int PHYS, int RS, int CT, int DIR, typename R>
+__device__ __forceinline__ R riemann(const R* vl, const R* vr, R* flux, R gamma, R Bn,
+                                     CTFace<R>& ct) {
+  if constexpr (PHYS == PHYS_MHD) {
+    if constexpr (RS == RS_HLLD) return mhd_hlld<DIR, CT>(vl, vr, flux, gamma, Bn, ct);
+    else return mhd_hll<DIR>(vl, vr, flux, gamma, ct);
+  } else {
+    if constexpr (RS == RS_HLLC) return hd_hllc<DIR>(vl, vr, flux, gamma);
+    else return hd_hll<DIR>(vl, vr, flux, gamma);
+  }
+}
+
+// Flux difference for one cell, Src/MHD/rhs.cpp:383-386 + 523 (x), 756, 981,
+// accumulated as in Src/update_stage.cpp:173-184/272-284/369-380.  MODE 0:
+// first direction (=), 1: middle (+=), 2: last (combine into U_out, RK2
+// weights of Src/rk_step.cpp:366-374, 509-517).
+template <int PHYS, int NV, int NDIM, int MODE, typename R, typename CTT>
+__device__ __forceinline__ double cell_update(const StageArgs<CTT>& a, long long n,
+                                              long long c, const R* Fl, const R* Fr,
+                                              R cml, R cmr, int dir) {
+  const double dtdx = a.dtdx[dir];
+#pragma unroll
+  for (int nv = 0; nv < NV; nv++) {
+    if (!rhs_var<PHYS, NDIM>(nv)) continue;
+    double rhs = -dtdx * ((double)Fr[nv] - (double)Fl[nv]);
+    double* du = a.dU + nv * n + c;
+    if constexpr (MODE == 0) {
+      *du = rhs;
+    } else if constexpr (MODE == 1) {
+      *du = *du + rhs;
+    } else {
+      double Rc = *du + rhs;
+      double u0 = a.U0[nv * n + c];
+      double out;
+      if (a.stage == 1) out = u0 + Rc;
+      else out = 0.5 * u0 + 0.5 * a.Uc[nv * n + c] + 0.5 * Rc;
+      a.Uout[nv * n + c] = out;
+    }
+  }
+  double cd = 0.5 * ((double)cml + (double)cmr) / a.dx[dir];
+  if constexpr (MODE == 0) {
+    a.Cdt[c] = cd;
+  } else {
+    cd = a.Cdt[c] + cd;
+    if constexpr (MODE == 1) a.Cdt[c] = cd;
+  }
+  return cd;
+}
+
+template <typename R, typename CTT>
+__device__ __forceinline__ void store_ct(const StageArgs<CTT>& a, int dir, long long f,
+                                         const CTFace<R>& ct) {
+  a.ct[dir][0][f] = (CTT)ct.eb;
+  a.ct[dir][1][f] = (CTT)ct.et;
+  a.ct[dir][2][f] = (CTT)ct.aL;
+  a.ct[dir][3][f] = (CTT)ct.aR;
+  a.ct[dir][4][f] = (CTT)ct.dL;
+  a.ct[dir][5][f] = (CTT)ct.dR;
+}
+
+// ---------------------------------------------------------------------
+// x sweep: one warp per x-row, 32 faces per chunk, neighbours by shuffle.
+// Face f (between cells f-1 and f) is computed by lane f%32; the lane then
+// updates cell f-1.  The first face's flux is kept for cell nx-1.
+// ---------------------------------------------------------------------
+template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, typename R, typename CTT>
+__global__ void __launch_bounds__(128) sweep_x_kernel(StageArgs<CTT> a, Grid3 g) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (row >= g.ny * g.nz) return;  // warp-uniform
+  const int nx = g.nx;
+  const long long n = g.n;
+  const long long rb = (long long)row * nx;
+  const R gamma = (R)a.gamma;
+
+  // carried state of cell c0-1 (uniform over lanes)
+  R pV[NV], pVLn[NV], pF[NV], pCm = R(0);
+  {
+    R vm[NV], v0[NV], vp[NV];
+    load_cell<NV>(a.V, n, rb + wrapi(nx - 2, nx), vm);
+    load_cell<NV>(a.V, n, rb + (nx - 1), v0);
+    load_cell<NV>(a.V, n, rb + 0, vp);
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      R dv = limit<LIM>(vp[nv] - v0[nv], v0[nv] - vm[nv]);
+      pV[nv] = v0[nv];
+      pVLn[nv] = v0[nv] + R(0.5) * dv;
+      pF[nv] = R(0);
+    }
+  }
+  R fF[NV], fCm = R(0);  // flux of face 0 (lane 0 of the first chunk)
+  R F[NV], cm = R(0);
+#pragma unroll
+  for (int nv = 0; nv < NV; nv++) { fF[nv] = R(0); F[nv] = R(0); }
+  uint32_t err = 0;
+
+  for (int c0 = 0; c0 < nx; c0 += 32) {
+    const int f = c0 + lane;
+    const bool act = f < nx;
+    const int fc = act ? f : nx - 1;
+    R Vc[NV], Vm1[NV], Vp1[NV], vL[NV], vR[NV], vLn[NV];
+    load_cell<NV>(a.V, n, rb + fc, Vc);
+    const bool selfp1 = (lane == 31) || (f + 1 >= nx);
+    if (selfp1) load_cell<NV>(a.V, n, rb + wrapi(fc + 1, nx), Vp1);
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      R up = __shfl_up_sync(FULL, Vc[nv], 1);
+      R dn = __shfl_down_sync(FULL, Vc[nv], 1);
+      Vm1[nv] = (lane == 0) ? pV[nv] : up;
+      if (!selfp1) Vp1[nv] = dn;
+      R dv = limit<LIM>(Vp1[nv] - Vc[nv], Vc[nv] - Vm1[nv]);
+      vR[nv] = Vc[nv] - R(0.5) * dv;
+      vLn[nv] = Vc[nv] + R(0.5) * dv;
+      R l = __shfl_up_sync(FULL, vLn[nv], 1);
+      vL[nv] = (lane == 0) ? pVLn[nv] : l;
+    }
+    R Bn = R(0);
+    if constexpr (PHYS != PHYS_HD) {
+      Bn = (R)__ldg(a.Bs[0] + rb + fc);  // Src/States/plm_states.cpp:184-189
+      vL[BX1] = Bn;
+      vR[BX1] = Bn;
+    }
+    CTFace<R> ct;
+    cm = riemann<PHYS, RS, CT, 0>(vL, vR, F, gamma, Bn, ct);
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++)
+      if (act && rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) err |= ERR_NAN | ERR_QUIT;
+    if constexpr (PHYS != PHYS_HD) {
+      if (act) store_ct(a, 0, rb + f, ct);
+    }
+    // flux of face f-1 and cell update of cell f-1
+    R Fm1[NV];
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      R t = __shfl_up_sync(FULL, F[nv], 1);
+      Fm1[nv] = (lane == 0) ? pF[nv] : t;
+    }
+    R cmm1;
+    {
+      R t = __shfl_up_sync(FULL, cm, 1);
+      cmm1 = (lane == 0) ? pCm : t;
+    }
+    if (act && f >= 1)
+      cell_update<PHYS, NV, NDIM, 0>(a, n, rb + (f - 1), Fm1, F, cmm1, cm, 0);
+    if (c0 == 0) {
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) fF[nv] = F[nv];
+      fCm = cm;
+    }
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      pV[nv] = __shfl_sync(FULL, Vc[nv], 31);
+      pVLn[nv] = __shfl_sync(FULL, vLn[nv], 31);
+      pF[nv] = __shfl_sync(FULL, F[nv], 31);
+    }
+    pCm = __shfl_sync(FULL, cm, 31);
+  }
+  // cell nx-1 uses F[nx-1] (lane (nx-1)%32 of the last chunk) and F[nx] = F[0]
+  {
+    R F0[NV];
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) F0[nv] = __shfl_sync(FULL, fF[nv], 0);
+    R cm0 = __shfl_sync(FULL, fCm, 0);
+    if (lane == ((nx - 1) & 31))
+      cell_update<PHYS, NV, NDIM, 0>(a, n, rb + (nx - 1), F, F0, cm, cm0, 0);
+  }
+  if (err) atomicOr(a.err, err);
+}
+
+// ---------------------------------------------------------------------
+// y / z sweep: thread per (x, pencil segment), marching along DIR.
+// MODE 1 accumulates into dU/Cdt; MODE 2 (last direction) combines into
+// U_out and reduces the stage-1 CFL maximum.
+// ---------------------------------------------------------------------
+template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, int DIR, int MODE,
+          typename R, typename CTT>
+__global__ void __launch_bounds__(128) sweep_m_kernel(StageArgs<CTT> a, Grid3 g, int S) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nd = (DIR == 1) ? g.ny : g.nz;
+  const int nseg = (nd + S - 1) / S;
+  const int t = blockIdx.y / nseg;       // k for DIR=1, j for DIR=2
+  const int seg = blockIdx.y - t * nseg;
+  const long long n = g.n;
+  const R gamma = (R)a.gamma;
+  double cdmax = 0.0;
+  uint32_t err = 0;
+  if (i < g.nx) {
+    const long long stride = (DIR == 1) ? (long long)g.nx : (long long)g.nx * g.ny;
+    const long long base = (DIR == 1) ? i + (long long)g.nx * g.ny * t
+                                      : i + (long long)g.nx * t;
+    const int m0 = seg * S;
+    const int m1 = min(m0 + S, nd);
+    R Vp[NV], Vc[NV], vLn[NV], Fp[NV], cmp = R(0);
+    {
+      R vmm[NV];
+      load_cell<NV>(a.V, n, base + wrapi(m0 - 2, nd) * stride, vmm);
+      load_cell<NV>(a.V, n, base + wrapi(m0 - 1, nd) * stride, Vp);
+      load_cell<NV>(a.V, n, base + (long long)m0 * stride, Vc);
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) {
+        R dv = limit<LIM>(Vc[nv] - Vp[nv], Vp[nv] - vmm[nv]);
+        vLn[nv] = Vp[nv] + R(0.5) * dv;
+        Fp[nv] = R(0);
+      }
+    }
+    for (int m = m0; m <= m1; m++) {
+      R Vn[NV], vL[NV], vR[NV], F[NV];
+      const int mw = wrapi(m, nd);
+      load_cell<NV>(a.V, n, base + (long long)wrapi(m + 1, nd) * stride, Vn);
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) {
+        R dv = limit<LIM>(Vn[nv] - Vc[nv], Vc[nv] - Vp[nv]);
+        vL[nv] = vLn[nv];
+        vR[nv] = Vc[nv] - R(0.5) * dv;
+        vLn[nv] = Vc[nv] + R(0.5) * dv;
+      }
+      R Bn = R(0);
+      if constexpr (PHYS != PHYS_HD) {
+        Bn = (R)__ldg(a.Bs[DIR] + base + (long long)mw * stride);
+        vL[BX1 + DIR] = Bn;
+        vR[BX1 + DIR] = Bn;
+      }
+      CTFace<R> ct;
+      R cm = riemann<PHYS, RS, CT, DIR>(vL, vR, F, gamma, Bn, ct);
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++)
+        if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) err |= ERR_NAN | ERR_QUIT;
+      if constexpr (PHYS != PHYS_HD) {
+        if (m < m1) store_ct(a, DIR, base + (long long)mw * stride, ct);
+      }
+      if (m > m0) {
+        double cd = cell_update<PHYS, NV, NDIM, MODE>(a, n, base + (long long)(m - 1) * stride,
+                                                      Fp, F, cmp, cm, DIR);
+        if constexpr (MODE == 2) cdmax = GP_MAX(cdmax, cd);
+      }
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) {
+        Vp[nv] = Vc[nv];
+        Vc[nv] = Vn[nv];
+        Fp[nv] = F[nv];
+      }
+      cmp = cm;
+    }
+  }
+  if constexpr (MODE == 2) {
+    if (a.stage == 1) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double other = __shfl_xor_sync(0xffffffffu, cdmax, o);  // all lanes, once
+        cdmax = GP_MAX(cdmax, other);
+      }
+      if ((threadIdx.x & 31) == 0) atomic_max_pos(a.invdt_bits, cdmax);
+    }
+  }
+  if (err) atomicOr(a.err, err);
+}
+
+// ---------------------------------------------------------------------
+// UCT edge EMF (Src/MHD/CT/ct_emf_average.cpp:535-995, reconstruction of
+// Src/array_reconstruct.cpp:45-206: face field with MC, stored velocities
+// with the scheme limiter).
+// b[0..3], q[0..3]: values at the four cells straddling the edge along the
+// reconstruction direction (edge between b[1] and b[2]).
+// ---------------------------------------------------------------------
+template <int LIM, typename R>
+__device__ __forceinline__ void uct_terms(const R* b, const R* q, R aL, R aR, R dL, R dR,
+                                          R& avg, R& phi) {
+  R dbl = limit<LIM_MC>(b[2] - b[1], b[1] - b[0]);
+  R dbr = limit<LIM_MC>(b[3] - b[2], b[2] - b[1]);
+  R dql = limit<LIM>(q[2] - q[1], q[1] - q[0]);
+  R dqr = limit<LIM>(q[3] - q[2], q[2] - q[1]);
+  R bL = b[1] + R(0.5) * dbl, bR = b[2] - R(0.5) * dbr;
+  R vL = q[1] + R(0.5) * dql, vR = q[2] - R(0.5) * dqr;
+  phi = dR * bR - dL * bL;
+  avg = aL * vL * bL + aR * vR * bR;
+}
+
+template <typename R, typename CTT>
+__device__ __forceinline__ void face_coef(const StageArgs<CTT>& a, int d, long long f1,
+                                          long long f2, R& aL, R& aR, R& dL, R& dR) {
+  aL = R(0.5) * ((R)a.ct[d][2][f1] + (R)a.ct[d][2][f2]);
+  aR = R(0.5) * ((R)a.ct[d][3][f1] + (R)a.ct[d][3][f2]);
+  dL = R(0.5) * ((R)a.ct[d][4][f1] + (R)a.ct[d][4][f2]);
+  dR = R(0.5) * ((R)a.ct[d][5][f1] + (R)a.ct[d][5][f2]);
+}
+
+template <int NDIM, int LIM, typename R, typename CTT>
+__global__ void __launch_bounds__(256) emf_kernel(StageArgs<CTT> a, Grid3 g) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = (int)(c % nx);
+  const int j = (int)((c / nx) % ny);
+  const int k = (int)(c / ((long long)nx * ny));
+  auto id = [&](int ii, int jj, int kk) -> long long {
+    return wrapi(ii, nx) + (long long)nx * (wrapi(jj, ny) + (long long)ny * wrapi(kk, nz));
+  };
+  R b[4], q[4], aL, aR, dL, dR, avg, phi;
+  // Ez at (i-1/2, j-1/2, k)
+  {
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      long long e = id(i - 2 + m, j, k);
+      b[m] = (R)a.Bs[1][e];
+      q[m] = (R)a.ct[1][1][e];
+    }
+    face_coef<R>(a, 0, id(i, j - 1, k), c, aL, aR, dL, dR);
+    uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+    R Ez = avg + phi;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      long long e = id(i, j - 2 + m, k);
+      b[m] = (R)a.Bs[0][e];
+      q[m] = (R)a.ct[0][0][e];
+    }
+    face_coef<R>(a, 1, id(i - 1, j, k), c, aL, aR, dL, dR);
+    uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+    Ez += avg - phi;
+    a.Ee[2][c] = (double)Ez;
+  }
+  if constexpr (NDIM == 3) {
+    // Ey at (i-1/2, j, k-1/2)
+    {
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        long long e = id(i - 2 + m, j, k);
+        b[m] = (R)a.Bs[2][e];
+        q[m] = (R)a.ct[2][0][e];
+      }
+      face_coef<R>(a, 0, id(i, j, k - 1), c, aL, aR, dL, dR);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      R Ey = avg - phi;
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        long long e = id(i, j, k - 2 + m);
+        b[m] = (R)a.Bs[0][e];
+        q[m] = (R)a.ct[0][1][e];
+      }
+      face_coef<R>(a, 2, id(i - 1, j, k), c, aL, aR, dL, dR);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      Ey += avg + phi;
+      a.Ee[1][c] = (double)Ey;
+    }
+    // Ex at (i, j-1/2, k-1/2)
+    {
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        long long e = id(i, j - 2 + m, k);
+        b[m] = (R)a.Bs[2][e];
+        q[m] = (R)a.ct[2][1][e];
+      }
+      face_coef<R>(a, 1, id(i, j, k - 1), c, aL, aR, dL, dR);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      R Ex = avg + phi;
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        long long e = id(i, j, k - 2 + m);
+        b[m] = (R)a.Bs[1][e];
+        q[m] = (R)a.ct[1][0][e];
+      }
+      face_coef<R>(a, 2, id(i, j - 1, k), c, aL, aR, dL, dR);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      Ex += avg - phi;
+      a.Ee[0][c] = (double)Ex;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
+// Stage finish: CT update (Src/MHD/CT/ct_update.cpp:181-423), face RK
+// combine (Src/rk_step.cpp:378-385, 536-552), cell-centred average
+// (Src/MHD/CT/ct_field_average.cpp:175-200), con2prim
+// (Src/mappers3D.cpp:104-194) -- all FP64.
+// ---------------------------------------------------------------------
+template <int NDIM, typename CTT>
+__device__ __forceinline__ double face_rs(const StageArgs<CTT>& a, const Grid3& g, int d,
+                                          int i, int j, int k) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  auto id = [&](int ii, int jj, int kk) -> long long {
+    return wrapi(ii, nx) + (long long)nx * (wrapi(jj, ny) + (long long)ny * wrapi(kk, nz));
+  };
+  double curlE;
+  if (d == 0) {
+    curlE = 0.0 + a.dtdx[1] * (a.Ee[2][id(i, j + 1, k)] - a.Ee[2][id(i, j, k)]);
+    if (NDIM == 3) curlE = curlE - a.dtdx[2] * (a.Ee[1][id(i, j, k + 1)] - a.Ee[1][id(i, j, k)]);
+  } else if (d == 1) {
+    curlE = -a.dtdx[0] * (a.Ee[2][id(i + 1, j, k)] - a.Ee[2][id(i, j, k)]);
+    if (NDIM == 3) curlE = curlE + a.dtdx[2] * (a.Ee[0][id(i, j, k + 1)] - a.Ee[0][id(i, j, k)]);
+  } else {
+    curlE = a.dtdx[0] * (a.Ee[1][id(i + 1, j, k)] - a.Ee[1][id(i, j, k)]) -
+            a.dtdx[1] * (a.Ee[0][id(i, j + 1, k)] - a.Ee[0][id(i, j, k)]);
+  }
+  return -curlE;
+}
+
+template <typename CTT>
+__device__ __forceinline__ double face_new(const StageArgs<CTT>& a, int d, long long f,
+                                           double rs) {
+  double bc = a.Bs[d][f];
+  if (a.stage == 1) return bc + rs;
+  return 0.5 * a.Bs0[d][f] + 0.5 * bc + 0.5 * rs;
+}
+
+template <int PHYS, int NV, int NDIM, typename CTT>
+__global__ void __launch_bounds__(256) finish_kernel(StageArgs<CTT> a, Grid3 g) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  const long long n = g.n;
+  double u[8], v[8];
+#pragma unroll
+  for (int nv = 0; nv < NV; nv++) u[nv] = a.Uout[nv * n + c];
+  if constexpr (PHYS != PHYS_HD) {
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int i = (int)(c % nx);
+    const int j = (int)((c / nx) % ny);
+    const int k = (int)(c / ((long long)nx * ny));
+#pragma unroll
+    for (int d = 0; d < NDIM; d++) {
+      const int di = (d == 0), dj = (d == 1), dk = (d == 2);
+      const long long fr = wrapi(i + di, nx) +
+                           (long long)nx * (wrapi(j + dj, ny) + (long long)ny * wrapi(k + dk, nz));
+      double bl = face_new(a, d, c, face_rs<NDIM>(a, g, d, i, j, k));
+      double br = face_new(a, d, fr, face_rs<NDIM>(a, g, d, i + di, j + dj, k + dk));
+      a.Bsout[d][c] = bl;
+      u[BX1 + d] = 0.5 * (bl + br);
+    }
+  }
+  uint32_t err = 0;
+#pragma unroll
+  for (int nv = 0; nv < NV; nv++)
+    if (isnan(u[nv])) err |= ERR_NAN | ERR_QUIT;
+  uint32_t le;
+  if constexpr (PHYS == PHYS_MHD) le = mhd_cons2prim(u, v, a.gamma, a.small_rho, a.small_prs);
+  else le = hd_cons2prim(u, v, a.gamma, a.small_rho, a.small_prs);
+  err |= le;
+  if (le & ERR_CONS2PRIM_FAIL) err |= ERR_QUIT;
+  if constexpr (PHYS != PHYS_HD) {
+#pragma unroll
+    for (int d = 0; d < NDIM; d++) a.Uout[(BX1 + d) * n + c] = u[BX1 + d];
+  }
+  if (le) {
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) a.Uout[nv * n + c] = u[nv];
+  }
+#pragma unroll
+  for (int nv = 0; nv < NV; nv++) a.Vout[nv * n + c] = v[nv];
+  if (err) atomicOr(a.err, err);
+}
+
+// Start-up primitive -> conservative map (Src/startup.cpp:542-566).
+template <int PHYS, int NV>
+__global__ void prim2cons_kernel(const double* __restrict__ V, double* __restrict__ U,
+                                 long long n, double gamma) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  double v[8], u[8];
+#pragma unroll
+  for (int nv = 0; nv < NV; nv++) v[nv] = V[nv * n + c];
+  if constexpr (PHYS == PHYS_MHD) mhd_prim2cons(v, u, gamma - 1.0);
+  else hd_prim2cons(v, u, gamma);
+#pragma unroll
+  for (int nv = 0; nv < NV; nv++) U[nv * n + c] = u[nv];
+}
+
+}  // namespace gp

@@ -1,0 +1,162 @@
+// gp_launch.cu -- template dispatch of the stage kernels.
+//
+// Compiled twice: with GP_MIXED=0 (FP64 everywhere, -fmad=false so that the
+// plain form keeps the reference's rounding sequence) and GP_MIXED=1 (FP32
+// reconstruction/limiter/Riemann/EMF arithmetic, FP64 accumulation, CT
+// update and con2prim).
+#include "gp_kernels.cuh"
+#include "gp_launch.h"
+
+#ifndef GP_MIXED
+#define GP_MIXED 0
+#endif
+
+namespace gp {
+
+#if GP_MIXED
+using RT = float;
+using CTT = float;
+#define GP_LAUNCH_STAGE launch_stage_mixed
+#else
+using RT = double;
+using CTT = double;
+#define GP_LAUNCH_STAGE launch_stage_fp64
+#endif
+
+static StageArgs<CTT> make_args(const StageDesc& d) {
+  StageArgs<CTT> a;
+  a.V = d.V;
+  for (int q = 0; q < 3; q++) {
+    a.Bs[q] = d.Bs[q];
+    a.Bs0[q] = d.Bs0[q];
+    a.Bsout[q] = d.Bsout[q];
+    a.Ee[q] = d.Ee[q];
+    a.dx[q] = d.dx[q];
+    for (int r = 0; r < 6; r++) a.ct[q][r] = static_cast<CTT*>(d.ct[q][r]);
+  }
+  a.dtdx = d.dtdx;
+  a.dU = d.dU;
+  a.Cdt = d.Cdt;
+  a.U0 = d.U0;
+  a.Uc = d.Uc;
+  a.Uout = d.Uout;
+  a.Vout = d.Vout;
+  a.gamma = d.gamma;
+  a.small_rho = d.small_rho;
+  a.small_prs = d.small_prs;
+  a.stage = d.stage;
+  a.invdt_bits = d.invdt_bits;
+  a.err = d.err;
+  return a;
+}
+
+template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM>
+static void run_stage(const StageArgs<CTT>& a, const GridDims& gd, int seg, cudaStream_t s,
+                      cudaEvent_t* ev) {
+  Grid3 g{gd.nx, gd.ny, gd.nz, gd.n};
+  int kidx = 0;
+  auto pre = [&]() { if (ev) cudaEventRecord(ev[2 * kidx], s); };
+  auto post = [&]() { if (ev) cudaEventRecord(ev[2 * kidx + 1], s); kidx++; };
+  {
+    const int rows = gd.ny * gd.nz;
+    const int wpb = 4;
+    dim3 grid((rows + wpb - 1) / wpb);
+    pre();
+    sweep_x_kernel<PHYS, NV, NDIM, RS, CT, LIM, RT, CTT><<<grid, 32 * wpb, 0, s>>>(a, g);
+    post();
+  }
+  {
+    const int nseg = (gd.ny + seg - 1) / seg;
+    dim3 grid((gd.nx + 127) / 128, gd.nz * nseg);
+    pre();
+    if constexpr (NDIM == 2)
+      sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 1, 2, RT, CTT><<<grid, 128, 0, s>>>(a, g, seg);
+    else
+      sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 1, 1, RT, CTT><<<grid, 128, 0, s>>>(a, g, seg);
+    post();
+  }
+  if constexpr (NDIM == 3) {
+    const int nseg = (gd.nz + seg - 1) / seg;
+    dim3 grid((gd.nx + 127) / 128, gd.ny * nseg);
+    pre();
+    sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 2, 2, RT, CTT><<<grid, 128, 0, s>>>(a, g, seg);
+    post();
+  }
+  const unsigned nb = (unsigned)((gd.n + 255) / 256);
+  if constexpr (PHYS != PHYS_HD) {
+    pre();
+    emf_kernel<NDIM, LIM, RT, CTT><<<nb, 256, 0, s>>>(a, g);
+    post();
+  }
+  pre();
+  finish_kernel<PHYS, NV, NDIM, CTT><<<nb, 256, 0, s>>>(a, g);
+  post();
+}
+
+template <int PHYS, int NV, int NDIM, int RS, int CT>
+static int by_lim(const StageArgs<CTT>& a, const GridDims& g, int lim, int seg, cudaStream_t s,
+                  cudaEvent_t* ev) {
+  switch (lim) {
+    case LIM_MC: run_stage<PHYS, NV, NDIM, RS, CT, LIM_MC>(a, g, seg, s, ev); return 0;
+    case LIM_VL: run_stage<PHYS, NV, NDIM, RS, CT, LIM_VL>(a, g, seg, s, ev); return 0;
+    case LIM_MINMOD: run_stage<PHYS, NV, NDIM, RS, CT, LIM_MINMOD>(a, g, seg, s, ev); return 0;
+    default: return -1;
+  }
+}
+
+template <int NDIM>
+static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey& k, int seg,
+                     cudaStream_t s, cudaEvent_t* ev) {
+  if (k.physics == PHYS_MHD) {
+    if (k.riemann == RS_HLLD && k.ct == CT_UCT_HLLD)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_HLLD, CT_UCT_HLLD>(a, g, k.limiter, seg, s, ev);
+    if (k.riemann == RS_HLLD && k.ct == CT_UCT_HLL)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_HLLD, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
+    if (k.riemann == RS_HLL)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_HLL, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
+    return -1;
+  }
+  if (k.physics == PHYS_HD) {
+    if (k.riemann == RS_HLLC) return by_lim<PHYS_HD, 5, NDIM, RS_HLLC, 0>(a, g, k.limiter, seg, s, ev);
+    if (k.riemann == RS_HLL) return by_lim<PHYS_HD, 5, NDIM, RS_HLL, 0>(a, g, k.limiter, seg, s, ev);
+    return -1;
+  }
+  return -1;
+}
+
+int GP_LAUNCH_STAGE(const StageDesc& d, const GridDims& g, const SchemeKey& k, int seg,
+                    cudaStream_t s, cudaEvent_t* ev) {
+  StageArgs<CTT> a = make_args(d);
+  if (k.ndim == 2) return by_scheme<2>(a, g, k, seg, s, ev);
+  if (k.ndim == 3) return by_scheme<3>(a, g, k, seg, s, ev);
+  return -1;
+}
+
+#if !GP_MIXED
+int launch_prim2cons(int physics, const double* V, double* U, long long n, double gamma,
+                     cudaStream_t s) {
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  if (physics == PHYS_MHD) prim2cons_kernel<PHYS_MHD, 8><<<nb, 256, 0, s>>>(V, U, n, gamma);
+  else if (physics == PHYS_HD) prim2cons_kernel<PHYS_HD, 5><<<nb, 256, 0, s>>>(V, U, n, gamma);
+  else return -1;
+  return 0;
+}
+
+int stage_launch_count(const SchemeKey& k) {
+  int c = 1 + (k.ndim == 3 ? 2 : 1) + 1;  // sweeps + finish
+  if (k.physics != PHYS_HD) c += 1;       // emf
+  return c;
+}
+
+const char* stage_kernel_name(const SchemeKey& k, int idx) {
+  static const char* n3m[] = {"sweep_x", "sweep_y", "sweep_z", "emf", "finish"};
+  static const char* n2m[] = {"sweep_x", "sweep_y", "emf", "finish"};
+  static const char* n3h[] = {"sweep_x", "sweep_y", "sweep_z", "finish"};
+  static const char* n2h[] = {"sweep_x", "sweep_y", "finish"};
+  if (idx < 0 || idx >= stage_launch_count(k)) return "?";
+  if (k.physics != PHYS_HD) return k.ndim == 3 ? n3m[idx] : n2m[idx];
+  return k.ndim == 3 ? n3h[idx] : n2h[idx];
+}
+#endif
+
+}  // namespace gp

@@ -1,0 +1,54 @@
+// gp_launch.h -- host-side launch interface between the C-ABI layer and the
+// per-precision kernel translation units (gp_launch.cu compiled twice: FP64
+// with -fmad=false, mixed FP32-flux with contraction allowed).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gp {
+
+struct StageDesc {
+  const double* V;
+  const double* Bs[3];
+  const double* Bs0[3];
+  double* Bsout[3];
+  double* dU;
+  double* Cdt;
+  const double* U0;
+  const double* Uc;
+  double* Uout;
+  double* Vout;
+  void* ct[3][6];      // double (FP64 form) or float (mixed form)
+  double* Ee[3];
+  const double* dtdx;  // device pointer to dt/dx_d
+  double dx[3];
+  double gamma, small_rho, small_prs;
+  int stage;
+  unsigned long long* invdt_bits;
+  uint32_t* err;
+};
+
+struct GridDims {
+  int nx, ny, nz;
+  long long n;
+};
+
+struct SchemeKey {
+  int physics, ndim, riemann, ct, limiter;
+};
+
+// Launch the kernels of one RK stage on `s`.  Returns 0 on success, a
+// negative value if the scheme combination has no compiled kernels.
+// `ev` (may be null) receives an event pair around every kernel launch, in
+// launch order (2*stage_launch_count(k) events).
+int launch_stage_fp64(const StageDesc& d, const GridDims& g, const SchemeKey& k,
+                      int seg, cudaStream_t s, cudaEvent_t* ev);
+int launch_stage_mixed(const StageDesc& d, const GridDims& g, const SchemeKey& k,
+                       int seg, cudaStream_t s, cudaEvent_t* ev);
+int launch_prim2cons(int physics, const double* V, double* U, long long n, double gamma,
+                     cudaStream_t s);
+// Number of kernel launches one stage issues for this scheme, and their names.
+int stage_launch_count(const SchemeKey& k);
+const char* stage_kernel_name(const SchemeKey& k, int idx);
+
+}  // namespace gp

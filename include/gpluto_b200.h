@@ -1,0 +1,152 @@
+/*
+ * gpluto_b200.h -- C ABI of the B200 (sm_100a) Godunov step.
+ *
+ * Drop-in boundary for gPLUTO's time-step path.  The reference calls
+ *     uint32_t AdvanceStep(Data*, Grid*, timeStep*)        (Src/prototypes.hpp:5)
+ * from its main loop (Src/main.cpp:444-447), then turns the stage-1 inverse
+ * time step into the next dt with
+ *     double NextTimeStep(timeStep*, RunConfig*, Runtime*, Grid*)
+ *                                                          (Src/prototypes.hpp:155,
+ *                                                           Src/next_time_step.cpp:20-130).
+ * Below AdvanceStep sit Boundary (Src/boundary.cpp:67), UpdateStage
+ * (Src/update_stage.cpp:57), the Riemann-solver plug-in selected by name in
+ * SetSolver (Src/MHD/set_solver.cpp:13-54, typedef Src/gpluto.hpp:762),
+ * CT_ComputeEMF / CT_Update / CT_AverageStaggeredFields
+ * (Src/MHD/CT/ct.hpp:118-142) and ConsToPrim3D (Src/mappers3D.cpp:76).
+ * This library replaces all of them with fused CUDA kernels; the host driver,
+ * pluto.ini / definitions.hpp configuration and Data/Grid arrays stay on the
+ * caller's side and cross this boundary as plain pointers and sizes.
+ *
+ * Arrays in GP_LAYOUT_REFERENCE follow Data::Vc/Uc (Ary4D, i fastest, variable
+ * index slowest, ghost zones included, Src/Array.hpp:471-494) and Data::Vs[d]
+ * (Ary3D with one extra point along d, Src/initialize.cpp:424-430).  Arrays in
+ * GP_LAYOUT_INTERIOR hold interior cells only ([nv][k][j][i]) and the left
+ * face of each cell for Vs.
+ *
+ * All functions return GP_OK (0) or a negative gp_status.  They are not
+ * thread-safe on a single handle; use one handle per host thread.
+ */
+#ifndef GPLUTO_B200_H
+#define GPLUTO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gp_handle gp_handle;
+
+enum gp_status {
+  GP_OK = 0,
+  GP_ERR_INVALID = -1,      /* bad argument */
+  GP_ERR_UNSUPPORTED = -2,  /* scheme/grid combination not built */
+  GP_ERR_CUDA = -3,         /* CUDA runtime error (see gp_last_error) */
+  GP_ERR_NOMEM = -4,        /* device allocation failed */
+  GP_ERR_QUIT = -5,         /* a kernel raised ERR_QUIT (the reference would QuitPLUTO) */
+  GP_ERR_NO_DEVICE = -6     /* no CUDA device: this library has no CPU path */
+};
+
+/* PHYSICS (definitions.hpp) */
+enum { GP_HD = 0, GP_MHD = 1, GP_RMHD = 2 };
+/* LIMITER (Src/States/plm_coeffs.hpp) */
+enum { GP_LIM_FLAT = 0, GP_LIM_MINMOD = 1, GP_LIM_VANLEER = 2, GP_LIM_MC = 3 };
+/* [Solver] in pluto.ini (Src/MHD/set_solver.cpp:35-47) */
+enum { GP_RS_HLL = 0, GP_RS_HLLC = 1, GP_RS_HLLD = 2 };
+/* CT_EMF_AVERAGE (Src/MHD/CT/ct.hpp:19-27) */
+enum { GP_CT_UCT_HLL = 0, GP_CT_UCT_HLLD = 1 };
+/* [Boundary] types (Src/boundary.cpp) */
+enum { GP_BC_PERIODIC = 0 };
+/* arithmetic form */
+enum { GP_FP64 = 0, GP_MIXED = 1 };
+/* host array layouts */
+enum { GP_LAYOUT_INTERIOR = 0, GP_LAYOUT_REFERENCE = 1 };
+
+/* Mirrors the parts of Grid (Src/structs.hpp:177-257) the step needs. */
+typedef struct gp_grid_desc {
+  int ndim;               /* DIMENSIONS: 2 or 3 */
+  int nint[3];            /* Grid::nint (1 along inactive directions) */
+  int nghost;             /* Grid::nghost, used only by GP_LAYOUT_REFERENCE */
+  double xbeg[3], xend[3];
+  const double *dx[3];    /* optional Grid::dx, ntot entries; must be uniform */
+  int lbound[3], rbound[3];
+} gp_grid_desc;
+
+/* Mirrors the compile-time scheme (definitions.hpp) and RunConfig/Runtime
+   values (Src/structs.hpp:397-447). */
+typedef struct gp_scheme {
+  int physics;            /* GP_HD, GP_MHD, GP_RMHD */
+  int limiter;            /* GP_LIM_* */
+  int riemann;            /* GP_RS_* */
+  int ct_emf;             /* GP_CT_* (MHD/RMHD) */
+  int rk_stages;          /* TIME_STEPPING: 2 (RK2) */
+  int precision;          /* GP_FP64 or GP_MIXED */
+  double gamma;           /* RunConfig::gamma */
+  double cfl;             /* Runtime::cfl */
+  double cfl_max_var;     /* Runtime::cfl_max_var */
+  double small_rho;       /* RunConfig::small_rho (1e-12 default) */
+  double small_prs;       /* RunConfig::small_prs (1e-12 default) */
+} gp_scheme;
+
+/* Per-step result: what the host needs for NextTimeStep and error handling. */
+typedef struct gp_step_out {
+  uint32_t err_bits;      /* OR of the ERR_* bits of Src/gpluto.hpp:247-265 */
+  double invDt_hyp;       /* timeStep::invDt_hyp of stage 1 */
+  double dt_next;         /* NextTimeStep() of this step */
+} gp_step_out;
+
+/* Allocate the device state for one grid.  `stream` is a cudaStream_t (NULL:
+   the legacy default stream).  Replaces Initialize's allocations
+   (Src/initialize.cpp:396-443) and SetSolver (Src/MHD/set_solver.cpp:13). */
+int gp_create(const gp_grid_desc *grid, const gp_scheme *scheme, void *stream,
+              gp_handle **out);
+int gp_destroy(gp_handle *h);
+
+/* Host -> device state.  Uc may be NULL: it is then computed from Vc with the
+   start-up PrimToCons map (Src/startup.cpp:542-566).  Vs1/Vs2 are NULL for HD
+   and along inactive directions. */
+int gp_upload_state(gp_handle *h, int layout, const double *Uc, const double *Vc,
+                    const double *Vs0, const double *Vs1, const double *Vs2);
+/* Device -> host state (any pointer may be NULL). */
+int gp_download_state(gp_handle *h, int layout, double *Uc, double *Vc,
+                      double *Vs0, double *Vs1, double *Vs2);
+
+/* One RK step of size dt (AdvanceStep, Src/rk_step.cpp:88-593).  Blocks until
+   the step finishes; fills `out` (may be NULL).  Returns GP_ERR_QUIT when a
+   kernel raised ERR_QUIT. */
+int gp_advance_step(gp_handle *h, double dt, gp_step_out *out);
+
+/* `nsteps` RK steps with the dt sequence kept on the device (each next dt by
+   NextTimeStep from the stage-1 reduction), no host round trip between
+   steps.  On entry *dt is the first step's dt; on return the dt of the step
+   after the last.  dt_hist (nsteps entries, may be NULL) receives the dt of
+   every step taken.  out->err_bits is the OR over all steps. */
+int gp_advance_steps(gp_handle *h, int nsteps, double *dt, double *dt_hist, gp_step_out *out);
+
+/* NextTimeStep (Src/next_time_step.cpp:80,125) for the host driver. */
+double gp_next_time_step(double invDt_hyp, double cfl, double cfl_max_var, double dt);
+
+/* Device pointers of the current state (interior layout), for callers that
+   keep data on the GPU.  Valid until the next step. */
+int gp_device_state(gp_handle *h, double **Uc, double **Vc, double **Vs);
+
+/* Kernel launches issued per RK step (for launch accounting). */
+int gp_launches_per_step(const gp_handle *h);
+
+/* Instrumented variant of gp_advance_steps for profiling: every kernel of a
+   step is bracketed by CUDA events on the handle's stream; kernel_ms[q]
+   (cap >= 2*kernels per stage) receives the mean duration of launch q of a
+   step, in launch order; *nkernels the number of launches per step (the
+   dt update kernel excluded).  Not part of the reference interface. */
+int gp_profile_steps(gp_handle *h, int nsteps, double *dt, float *kernel_ms, int cap,
+                     int *nkernels);
+/* Name of launch q of a step (as ordered by gp_profile_steps). */
+const char *gp_kernel_name(const gp_handle *h, int q);
+
+/* Text of the last error on this thread. */
+const char *gp_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPLUTO_B200_H */

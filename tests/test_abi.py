@@ -1,0 +1,64 @@
+"""The C-ABI library: symbols, loading and failure behaviour (no GPU needed)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from gpluto_dev_b200 import api
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    syms = set()
+    inc = os.path.join(ROOT, "include")
+    for f in os.listdir(inc):
+        if f.endswith(".h"):
+            txt = open(os.path.join(inc, f)).read()
+            txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+            syms |= set(re.findall(r"\b(gp_[a-z_0-9]+)\s*\(", txt))
+    return sorted(syms)
+
+
+def test_header_declares_entry_points():
+    s = declared_symbols()
+    for must in ("gp_create", "gp_destroy", "gp_upload_state", "gp_download_state",
+                 "gp_advance_step", "gp_advance_steps", "gp_next_time_step"):
+        assert must in s
+
+
+def test_library_exports_every_declared_symbol():
+    L = api.lib()
+    for name in declared_symbols():
+        assert hasattr(L, name), f"{name} not exported"
+        assert ctypes.cast(getattr(L, name), ctypes.c_void_p).value
+
+
+def test_next_time_step_formula():
+    # Src/next_time_step.cpp:80,125
+    assert api.NextTimeStep(10.0, 0.4, 1.1, 1.0) == 0.04
+    assert api.NextTimeStep(1e-3, 0.4, 1.1, 1e-4) == 1.1 * 1e-4
+
+
+def test_create_rejects_bad_configs_before_touching_the_device():
+    L = api.lib()
+    g = api.GpGridDesc()
+    g.ndim = 1
+    s = api.Scheme().to_c()
+    h = ctypes.c_void_p()
+    assert L.gp_create(ctypes.byref(g), ctypes.byref(s), None, ctypes.byref(h)) == -2
+    g.ndim = 2
+    g.nint[0] = g.nint[1] = 16
+    g.nint[2] = 1
+    s.rk_stages = 3
+    assert L.gp_create(ctypes.byref(g), ctypes.byref(s), None, ctypes.byref(h)) == -2
+
+
+def test_no_cpu_fallback_without_device():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    with pytest.raises(api.GPError) as ei:
+        api.Solver(2, (16, 16), api.Scheme())
+    assert ei.value.code == api.GP_ERR_NO_DEVICE

@@ -1,0 +1,160 @@
+"""Parity of the sm_100a Godunov step with the reference and the oracle.
+
+The FP64 form must reproduce the reference serial build bit for bit (the
+kernels keep the reference's operation order and are compiled with
+-fmad=false); where a bound is written below it is the acceptance bound of
+the plain form (relative L-infinity <= 1e-11 per variable).
+"""
+import numpy as np
+import pytest
+
+import golden_util as gu
+import oracle as orc
+from gpluto_dev_b200 import api, ics
+
+pytestmark = pytest.mark.gpu
+
+RTOL_FP64 = 1e-11
+
+
+def rel_linf(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def make_solver(st, limiter, solver, ct, cfl=0.4, cfl_max_var=1.1, precision=api.FP64):
+    sch = api.Scheme(physics=st.physics, limiter=limiter, riemann=solver, ct_emf=ct,
+                     precision=precision, gamma=st.gamma, cfl=cfl, cfl_max_var=cfl_max_var)
+    return api.Solver.from_state(st, sch)
+
+
+@pytest.mark.parametrize("name", gu.names())
+def test_gpu_matches_reference_fixture_bitwise(name):
+    g = gu.Golden(name)
+    s = make_solver(g.ic, g.limiter, g.solver, g.ct, g.cfl, g.cfl_max_var)
+    dt_after, hist, out = s.run(g.nsteps, g.first_dt)
+    V, U, Bs = s.download()
+    assert out.err_bits & api.ERR_QUIT == 0
+    np.testing.assert_array_equal(hist, g.dt[:-1])
+    assert dt_after == g.dt[-1]
+    np.testing.assert_array_equal(V, g.V)
+    np.testing.assert_array_equal(U, g.U)
+    for a, b in zip(Bs, g.Bs):
+        np.testing.assert_array_equal(a, b)
+
+
+CASES = [
+    # (generator, kwargs, limiter, solver, ct, nsteps)
+    (ics.mhd2d_turbulence, dict(n=(64, 48), seed=21), "mc", "hlld", "uct_hlld", 30),
+    (ics.mhd2d_turbulence, dict(n=(33, 17), seed=22), "vl", "hlld", "uct_hll", 20),
+    (ics.mhd3d_turbulence, dict(n=(20, 18, 16), seed=23), "mc", "hlld", "uct_hlld", 10),
+    (ics.mhd3d_blast, dict(n=(24, 24, 24), seed=24, radius=0.2), "mc", "hlld", "uct_hlld", 10),
+    (ics.mhd3d_turbulence, dict(n=(16, 20, 12), seed=25), "minmod", "hll", "uct_hll", 8),
+    (ics.hd_turbulence, dict(n=(40, 36), seed=26), "mc", "hllc", "uct_hll", 20),
+    (ics.hd_turbulence, dict(n=(16, 12, 20), seed=27), "vl", "hll", "uct_hll", 10),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_gpu_matches_oracle_bitwise(case):
+    gen, kw, lim, rs, ct, nsteps = CASES[case]
+    st = gen(**kw)
+    o = orc.Oracle(st, limiter=lim, solver=rs, ct=ct)
+    ohist, oerr = o.run(nsteps, 1e-4)
+    Vo, Uo, Bo = o.state()
+    s = make_solver(st, lim, rs, ct)
+    dt_after, hist, out = s.run(nsteps, 1e-4)
+    V, U, Bs = s.download()
+    assert out.err_bits == oerr
+    np.testing.assert_array_equal(hist, ohist[:-1])
+    np.testing.assert_array_equal(V, Vo)
+    np.testing.assert_array_equal(U, Uo)
+    for a, b in zip(Bs, Bo):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_host_dt_path_equals_device_dt_path():
+    st = ics.mhd2d_turbulence(n=(48, 40), seed=31)
+    a = make_solver(st, "mc", "hlld", "uct_hlld")
+    b = make_solver(st, "mc", "hlld", "uct_hlld")
+    dt = 1e-4
+    for _ in range(6):
+        out = a.AdvanceStep(dt)
+        dt = api.NextTimeStep(out.invDt_hyp, 0.4, 1.1, dt)
+    dt_b, _, _ = b.run(6, 1e-4)
+    assert dt == dt_b
+    Va, Ua, Ba = a.download()
+    Vb, Ub, Bb = b.download()
+    np.testing.assert_array_equal(Ua, Ub)
+    np.testing.assert_array_equal(Ba[0], Bb[0])
+
+
+def test_deterministic_rerun():
+    st = ics.mhd3d_blast(n=(32, 32, 32), seed=5)
+    r = []
+    for _ in range(2):
+        s = make_solver(st, "mc", "hlld", "uct_hlld")
+        s.run(5, 1e-4)
+        r.append(s.download())
+    for x, y in zip(r[0][:2], r[1][:2]):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_reference_layout_round_trip():
+    st = ics.mhd3d_turbulence(n=(12, 10, 8), seed=41)
+    s = make_solver(st, "mc", "hlld", "uct_hlld")
+    V0, U0, B0 = s.download()
+    cshape, fshapes = s.reference_shapes()
+    g = s.nghost
+    Vr, Ur = np.zeros(cshape), np.zeros(cshape)
+    Br = [np.zeros(f) for f in fshapes]
+    api.lib().gp_download_state(s._h, api.LAYOUT_REFERENCE, api._dp(Ur), api._dp(Vr),
+                                api._dp(Br[0]), api._dp(Br[1]), api._dp(Br[2]))
+    nx, ny, nz = st.shape
+    np.testing.assert_array_equal(Vr[:, g:g + nz, g:g + ny, g:g + nx], V0)
+    # periodic ghosts: left ghost = right interior
+    np.testing.assert_array_equal(Vr[:, g:g + nz, g:g + ny, 0], V0[:, :, :, nx - 2])
+    t = make_solver(st, "mc", "hlld", "uct_hlld")
+    t.upload(Vr, Ur, Br, layout=api.LAYOUT_REFERENCE)
+    V1, U1, B1 = t.download()
+    np.testing.assert_array_equal(V1, V0)
+    np.testing.assert_array_equal(U1, U0)
+    for a, b in zip(B0, B1):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_divb_roundoff_3d_blast():
+    st = ics.mhd3d_blast(n=(48, 48, 48), seed=7)
+    s = make_solver(st, "mc", "hlld", "uct_hlld")
+    s.run(20, 1e-4)
+    _, _, Bs = s.download()
+    nx, ny, nz = st.shape
+    div = ((np.roll(Bs[0], -1, 2) - Bs[0]) * nx + (np.roll(Bs[1], -1, 1) - Bs[1]) * ny
+           + (np.roll(Bs[2], -1, 0) - Bs[2]) * nz)
+    bmax = max(np.abs(b).max() for b in Bs)
+    assert np.abs(div).max() / (bmax * max(nx, ny, nz)) <= 1e-12
+
+
+def test_conservation_periodic():
+    st = ics.mhd3d_turbulence(n=(24, 24, 24), seed=8)
+    s = make_solver(st, "mc", "hlld", "uct_hlld")
+    _, U0, _ = s.download()
+    s.run(10, 1e-4)
+    _, U1, _ = s.download()
+    for nv in (0, 1, 2, 3, 7):   # mass, momentum, total energy
+        tot0, tot1 = U0[nv].sum(), U1[nv].sum()
+        scale = np.abs(U0[nv]).sum()
+        assert abs(tot1 - tot0) <= 1e-12 * scale
+
+
+def test_full_size_2d_100_steps_matches_oracle():
+    """Config-0 size (2-D 256^2 MHD, PLM-MC, HLLD, UCT_HLLD, RK2, CFL 0.4)."""
+    st = ics.mhd2d_turbulence(n=(256, 256), seed=0)
+    o = orc.Oracle(st, limiter="mc", solver="hlld", ct="uct_hlld", cfl=0.4)
+    ohist, _ = o.run(100, 1e-4)
+    Vo, Uo, Bo = o.state()
+    s = make_solver(st, "mc", "hlld", "uct_hlld")
+    s.run(100, 1e-4)
+    V, U, Bs = s.download()
+    for nv in range(8):
+        assert rel_linf(U[nv], Uo[nv]) <= RTOL_FP64
+    assert np.array_equal(U, Uo)
