@@ -192,8 +192,8 @@ def _oracle_worker(args):
     return (time.perf_counter() - t0) / (total - nwarm)
 
 
-def config_block():
-    return {"workload": WORKLOAD, "grid": [N, N, N], "physics": "ideal MHD",
+def config_block(n=N):
+    return {"workload": f"3d_ideal_mhd_blast_{n}^3", "grid": [n, n, n], "physics": "ideal MHD",
             "scheme": "PLM-MC + HLLD + UCT_HLLD + RK2, CFL 0.4, gamma 5/3",
             "boundary": "periodic", "ic": "seeded blast (seed 1 + rank)",
             "l2": "inputs larger than L2 (state ~2.5 GB), no flush"}
@@ -218,6 +218,52 @@ def impl_reference(args):
     print(json.dumps(line), flush=True)
     return 0
 
+
+
+def measure_e2e(make_solver, ncell, world, steps, barrier, dist):
+    """End to end through the C ABI with host buffers.
+
+    Per step: host (pinned) -> device upload of the full reference-layout
+    state (Uc, Vc, Vs with ghost zones, as Data holds it), one AdvanceStep,
+    device -> host download of the same arrays."""
+    import torch
+    from gpluto_dev_b200 import api
+    se = make_solver(api.FP64)
+    cshape, fshapes = se.reference_shapes()
+    hU = torch.empty(cshape, dtype=torch.float64, pin_memory=True)
+    hV = torch.empty(cshape, dtype=torch.float64, pin_memory=True)
+    hB = [torch.empty(f, dtype=torch.float64, pin_memory=True) for f in fshapes]
+    hB += [None] * (3 - len(hB))
+    L = api.lib()
+
+    def dl():
+        api._check(L.gp_download_state(se._h, api.LAYOUT_REFERENCE, api._dp(hU), api._dp(hV),
+                                       api._dp(hB[0]), api._dp(hB[1]), api._dp(hB[2])))
+
+    dl()
+    k = max(1, min(steps, 10))
+    de = FIRST_DT
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(k):
+        api._check(L.gp_upload_state(se._h, api.LAYOUT_REFERENCE, api._dp(hU), api._dp(hV),
+                                     api._dp(hB[0]), api._dp(hB[1]), api._dp(hB[2])))
+        o = se.AdvanceStep(de)
+        de = api.NextTimeStep(o.invDt_hyp, 0.4, 1.1, de)
+        dl()
+    torch.cuda.synchronize()
+    te = time.perf_counter() - t0
+    if dist is not None:
+        tt = torch.tensor([te], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+    nbytes = (hU.numel() + hV.numel() + sum(b.numel() for b in hB if b is not None)) * 8
+    se.close()
+    return {"value": world * ncell * k / te / 1e6, "unit": METRIC,
+            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": k,
+            "path": "gp_upload_state(reference layout, pinned host) + gp_advance_step + "
+                    "gp_download_state(reference layout) per step"}
 
 # --------------------------------------------------------------------------
 # our arm
@@ -328,41 +374,7 @@ def impl_ours(args):
     # Per step: host (pinned) -> device upload of the full reference-layout
     # state (Uc, Vc, Vs with ghost zones, as Data holds it), one AdvanceStep,
     # device -> host download of the same arrays.
-    se = solver(api.FP64)
-    cshape, fshapes = se.reference_shapes()
-    hU = torch.empty(cshape, dtype=torch.float64, pin_memory=True)
-    hV = torch.empty(cshape, dtype=torch.float64, pin_memory=True)
-    hB = [torch.empty(f, dtype=torch.float64, pin_memory=True) for f in fshapes]
-    L = api.lib()
-
-    def dl():
-        api._check(L.gp_download_state(se._h, api.LAYOUT_REFERENCE, api._dp(hU), api._dp(hV),
-                                       api._dp(hB[0]), api._dp(hB[1]), api._dp(hB[2])))
-
-    dl()
-    k_e2e = max(1, min(args.steps, 10))
-    de = FIRST_DT
-    torch.cuda.synchronize()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(k_e2e):
-        api._check(L.gp_upload_state(se._h, api.LAYOUT_REFERENCE, api._dp(hU), api._dp(hV),
-                                     api._dp(hB[0]), api._dp(hB[1]), api._dp(hB[2])))
-        o = se.AdvanceStep(de)
-        de = api.NextTimeStep(o.invDt_hyp, 0.4, 1.1, de)
-        dl()
-    torch.cuda.synchronize()
-    te = time.perf_counter() - t0
-    if dist is not None:
-        tt = torch.tensor([te], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        te = float(tt.item())
-    nbytes = (hU.numel() + hV.numel() + sum(b.numel() for b in hB)) * 8
-    e2e = {"value": world * ncell * k_e2e / te / 1e6, "unit": METRIC,
-           "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": k_e2e,
-           "path": "gp_upload_state(reference layout, pinned host) + gp_advance_step + "
-                   "gp_download_state(reference layout) per step"}
-    del se
+    e2e = None if args.no_e2e else measure_e2e(solver, ncell, world, args.steps, barrier, dist)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -379,7 +391,7 @@ def impl_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded 3-D MHD blast initial conditions)",
-            "config": dict(config_block(), parallelism=f"replicas x{world}"),
+            "config": dict(config_block(args.n), parallelism=f"replicas x{world}"),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clocks,
             "forms": {"fp64": {"value": value, "ms_per_step": ms_step}, "mixed": mixed},
@@ -397,6 +409,7 @@ def main():
     ap.add_argument("--n", type=int, default=N)
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

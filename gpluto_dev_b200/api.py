@@ -20,7 +20,8 @@ import numpy as np
 from . import ics
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_build", "libgpluto_b200.so")
+LIB_PATH = os.environ.get("GPLUTO_B200_LIB") or os.path.join(_HERE, "_build",
+                                                             "libgpluto_b200.so")
 
 GP_OK, GP_ERR_QUIT, GP_ERR_NO_DEVICE = 0, -5, -6
 HD, MHD, RMHD = 0, 1, 2

@@ -304,8 +304,8 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   alloc((void**)&h->U[0], cell * h->nvar);
   alloc((void**)&h->U[1], cell * h->nvar);
   alloc((void**)&h->V, cell * h->nvar);
-  alloc((void**)&h->dU, cell * h->nvar);
-  alloc((void**)&h->Cdt, cell);
+  alloc((void**)&h->dU, cell * h->nvar * 3);
+  alloc((void**)&h->Cdt, cell * 3);
   if (scheme->physics != GP_HD) {
     for (int b = 0; b < 3; b++)
       for (int d = 0; d < h->ndim; d++) alloc((void**)&h->Bs[b][d], cell);
@@ -324,7 +324,8 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
     return fail(GP_ERR_NOMEM, "device allocation failed for %lld cells", ncell);
   }
   cudaMemsetAsync(h->sc, 0, sizeof(StepScalars), h->stream);
-  cudaMemsetAsync(h->dU, 0, cell * h->nvar, h->stream);
+  cudaMemsetAsync(h->dU, 0, cell * h->nvar * 3, h->stream);
+  cudaMemsetAsync(h->Cdt, 0, cell * 3, h->stream);
   h->bcur = 0;
   h->launches_per_step = 2 * gp::stage_launch_count(h->key) + 1;
   *out = h;

@@ -37,8 +37,8 @@ struct StageArgs {
   const double* Bs[3];    // stage-input face fields (left faces)
   const double* Bs0[3];   // face fields at t^n (stage 2)
   double* Bsout[3];       // face fields written by this stage
-  double* dU;             // [nvar][n] rhs accumulator
-  double* Cdt;            // [n] inverse dt accumulator
+  double* dU;             // [3][nvar][n] flux difference of each direction
+  double* Cdt;            // [3][n] inverse dt of each direction
   const double* U0;       // U^n
   const double* Uc;       // stage-input U
   double* Uout;           // U written by this stage
@@ -69,6 +69,28 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long* addr, double 
   atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
 
+// Asynchronous global->shared copies (cp.async, per thread, 8 bytes): the
+// sweeps stage the next stencil cell while the current face is solved, so the
+// prefetch costs no registers.  Each thread reads back only what it staged.
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait1() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait0() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+#ifndef GP_SWEEP_MINB
+#define GP_SWEEP_MINB 3
+#endif
+constexpr int SWEEP_THREADS = 128;
+
 // whether conserved component nv receives a flux difference that survives
 // the stage (the cell-centred field along active directions is overwritten
 // by the face average, Src/MHD/CT/ct_field_average.cpp:378-410)
@@ -90,41 +112,22 @@ __device__ __forceinline__ R riemann(const R* vl, const R* vr, R* flux, R gamma,
   }
 }
 
-// Flux difference for one cell, Src/MHD/rhs.cpp:383-386 + 523 (x), 756, 981,
-// accumulated as in Src/update_stage.cpp:173-184/272-284/369-380.  MODE 0:
-// first direction (=), 1: middle (+=), 2: last (combine into U_out, RK2
-// weights of Src/rk_step.cpp:366-374, 509-517).
-template <int PHYS, int NV, int NDIM, int MODE, typename R, typename CTT>
-__device__ __forceinline__ double cell_update(const StageArgs<CTT>& a, long long n,
-                                              long long c, const R* Fl, const R* Fr,
-                                              R cml, R cmr, int dir) {
+// Flux difference of one cell along `dir` (Src/MHD/rhs.cpp:383-386, 756,
+// 981) and its inverse-dt term (Src/MHD/rhs.cpp:523 and the += at 756, 981),
+// written to the direction's own arrays; the finish kernel sums them in the
+// order x, y, z as Src/update_stage.cpp:173-184/272-284/369-380 does.
+template <int PHYS, int NV, int NDIM, typename R, typename CTT>
+__device__ __forceinline__ void cell_update(const StageArgs<CTT>& a, long long n,
+                                            long long c, const R* Fl, const R* Fr,
+                                            R cml, R cmr, int dir) {
   const double dtdx = a.dtdx[dir];
+  double* du = a.dU + (long long)dir * NV * n;
 #pragma unroll
   for (int nv = 0; nv < NV; nv++) {
     if (!rhs_var<PHYS, NDIM>(nv)) continue;
-    double rhs = -dtdx * ((double)Fr[nv] - (double)Fl[nv]);
-    double* du = a.dU + nv * n + c;
-    if constexpr (MODE == 0) {
-      *du = rhs;
-    } else if constexpr (MODE == 1) {
-      *du = *du + rhs;
-    } else {
-      double Rc = *du + rhs;
-      double u0 = a.U0[nv * n + c];
-      double out;
-      if (a.stage == 1) out = u0 + Rc;
-      else out = 0.5 * u0 + 0.5 * a.Uc[nv * n + c] + 0.5 * Rc;
-      a.Uout[nv * n + c] = out;
-    }
+    du[nv * n + c] = -dtdx * ((double)Fr[nv] - (double)Fl[nv]);
   }
-  double cd = 0.5 * ((double)cml + (double)cmr) / a.dx[dir];
-  if constexpr (MODE == 0) {
-    a.Cdt[c] = cd;
-  } else {
-    cd = a.Cdt[c] + cd;
-    if constexpr (MODE == 1) a.Cdt[c] = cd;
-  }
-  return cd;
+  a.Cdt[(long long)dir * n + c] = 0.5 * ((double)cml + (double)cmr) / a.dx[dir];
 }
 
 template <typename R, typename CTT>
@@ -144,8 +147,12 @@ __device__ __forceinline__ void store_ct(const StageArgs<CTT>& a, int dir, long 
 // updates cell f-1.  The first face's flux is kept for cell nx-1.
 // ---------------------------------------------------------------------
 template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, typename R, typename CTT>
-__global__ void __launch_bounds__(128) sweep_x_kernel(StageArgs<CTT> a, Grid3 g) {
+__global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
+    sweep_x_kernel(StageArgs<CTT> a, Grid3 g) {
   constexpr unsigned FULL = 0xffffffffu;
+  constexpr int SL = 2 * NV + 1;  // staged doubles per lane: V[f], V[f+1], Bs[f]
+  __shared__ double stg[2][SL][SWEEP_THREADS];
+  const int tid = threadIdx.x;
   const int lane = threadIdx.x & 31;
   const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (row >= g.ny * g.nz) return;  // warp-uniform
@@ -175,14 +182,35 @@ __global__ void __launch_bounds__(128) sweep_x_kernel(StageArgs<CTT> a, Grid3 g)
   for (int nv = 0; nv < NV; nv++) { fF[nv] = R(0); F[nv] = R(0); }
   uint32_t err = 0;
 
-  for (int c0 = 0; c0 < nx; c0 += 32) {
+  // stage chunk c0 into buffer b: V[f], V[f+1] (lanes that cannot take it
+  // from the next lane), Bs[f]
+  auto stage_chunk = [&](int c0, int b) {
+    const int f = c0 + lane;
+    const int fc = f < nx ? f : nx - 1;
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][nv][tid], a.V + nv * n + rb + fc);
+    if (lane == 31 || f + 1 >= nx) {
+      const int fp = wrapi(fc + 1, nx);
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][NV + nv][tid], a.V + nv * n + rb + fp);
+    }
+    if constexpr (PHYS != PHYS_HD) cp_async8(&stg[b][2 * NV][tid], a.Bs[0] + rb + fc);
+    cp_async_commit();
+  };
+  stage_chunk(0, 0);
+  int buf = 0;
+  for (int c0 = 0; c0 < nx; c0 += 32, buf ^= 1) {
     const int f = c0 + lane;
     const bool act = f < nx;
-    const int fc = act ? f : nx - 1;
+    stage_chunk(c0 + 32 < nx ? c0 + 32 : c0, buf ^ 1);   // prefetch the next chunk
+    cp_async_wait1();
     R Vc[NV], Vm1[NV], Vp1[NV], vL[NV], vR[NV], vLn[NV];
-    load_cell<NV>(a.V, n, rb + fc, Vc);
     const bool selfp1 = (lane == 31) || (f + 1 >= nx);
-    if (selfp1) load_cell<NV>(a.V, n, rb + wrapi(fc + 1, nx), Vp1);
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      Vc[nv] = (R)stg[buf][nv][tid];
+      if (selfp1) Vp1[nv] = (R)stg[buf][NV + nv][tid];
+    }
 #pragma unroll
     for (int nv = 0; nv < NV; nv++) {
       R up = __shfl_up_sync(FULL, Vc[nv], 1);
@@ -197,7 +225,7 @@ __global__ void __launch_bounds__(128) sweep_x_kernel(StageArgs<CTT> a, Grid3 g)
     }
     R Bn = R(0);
     if constexpr (PHYS != PHYS_HD) {
-      Bn = (R)__ldg(a.Bs[0] + rb + fc);  // Src/States/plm_states.cpp:184-189
+      Bn = (R)stg[buf][2 * NV][tid];  // Src/States/plm_states.cpp:184-189
       vL[BX1] = Bn;
       vR[BX1] = Bn;
     }
@@ -222,7 +250,7 @@ __global__ void __launch_bounds__(128) sweep_x_kernel(StageArgs<CTT> a, Grid3 g)
       cmm1 = (lane == 0) ? pCm : t;
     }
     if (act && f >= 1)
-      cell_update<PHYS, NV, NDIM, 0>(a, n, rb + (f - 1), Fm1, F, cmm1, cm, 0);
+      cell_update<PHYS, NV, NDIM>(a, n, rb + (f - 1), Fm1, F, cmm1, cm, 0);
     if (c0 == 0) {
 #pragma unroll
       for (int nv = 0; nv < NV; nv++) fF[nv] = F[nv];
@@ -236,6 +264,7 @@ __global__ void __launch_bounds__(128) sweep_x_kernel(StageArgs<CTT> a, Grid3 g)
     }
     pCm = __shfl_sync(FULL, cm, 31);
   }
+  cp_async_wait0();
   // cell nx-1 uses F[nx-1] (lane (nx-1)%32 of the last chunk) and F[nx] = F[0]
   {
     R F0[NV];
@@ -243,19 +272,24 @@ __global__ void __launch_bounds__(128) sweep_x_kernel(StageArgs<CTT> a, Grid3 g)
     for (int nv = 0; nv < NV; nv++) F0[nv] = __shfl_sync(FULL, fF[nv], 0);
     R cm0 = __shfl_sync(FULL, fCm, 0);
     if (lane == ((nx - 1) & 31))
-      cell_update<PHYS, NV, NDIM, 0>(a, n, rb + (nx - 1), F, F0, cm, cm0, 0);
+      cell_update<PHYS, NV, NDIM>(a, n, rb + (nx - 1), F, F0, cm, cm0, 0);
   }
   if (err) atomicOr(a.err, err);
 }
 
 // ---------------------------------------------------------------------
-// y / z sweep: thread per (x, pencil segment), marching along DIR.
-// MODE 1 accumulates into dU/Cdt; MODE 2 (last direction) combines into
-// U_out and reduces the stage-1 CFL maximum.
+// y / z sweep: thread per (x, pencil segment), marching along DIR with a
+// register window of three cells; the cell two steps ahead and the next face
+// field are staged into shared memory with cp.async while the current face
+// is solved.  Writes the direction's flux differences, inverse-dt terms and
+// UCT face data (no loads besides the stencil).
 // ---------------------------------------------------------------------
-template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, int DIR, int MODE,
-          typename R, typename CTT>
-__global__ void __launch_bounds__(128) sweep_m_kernel(StageArgs<CTT> a, Grid3 g, int S) {
+template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, int DIR, typename R,
+          typename CTT>
+__global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
+    sweep_m_kernel(StageArgs<CTT> a, Grid3 g, int S) {
+  __shared__ double stg[2][NV + 1][SWEEP_THREADS];
+  const int tid = threadIdx.x;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int nd = (DIR == 1) ? g.ny : g.nz;
   const int nseg = (nd + S - 1) / S;
@@ -263,7 +297,6 @@ __global__ void __launch_bounds__(128) sweep_m_kernel(StageArgs<CTT> a, Grid3 g,
   const int seg = blockIdx.y - t * nseg;
   const long long n = g.n;
   const R gamma = (R)a.gamma;
-  double cdmax = 0.0;
   uint32_t err = 0;
   if (i < g.nx) {
     const long long stride = (DIR == 1) ? (long long)g.nx : (long long)g.nx * g.ny;
@@ -271,6 +304,15 @@ __global__ void __launch_bounds__(128) sweep_m_kernel(StageArgs<CTT> a, Grid3 g,
                                       : i + (long long)g.nx * t;
     const int m0 = seg * S;
     const int m1 = min(m0 + S, nd);
+    auto stage = [&](int mcell, int mface, int b) {
+      const long long cc = base + (long long)wrapi(mcell, nd) * stride;
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][nv][tid], a.V + nv * n + cc);
+      if constexpr (PHYS != PHYS_HD)
+        cp_async8(&stg[b][NV][tid], a.Bs[DIR] + base + (long long)wrapi(mface, nd) * stride);
+      cp_async_commit();
+    };
+    stage(m0 + 1, m0, 0);
     R Vp[NV], Vc[NV], vLn[NV], Fp[NV], cmp = R(0);
     {
       R vmm[NV];
@@ -284,12 +326,14 @@ __global__ void __launch_bounds__(128) sweep_m_kernel(StageArgs<CTT> a, Grid3 g,
         Fp[nv] = R(0);
       }
     }
-    for (int m = m0; m <= m1; m++) {
+    int buf = 0;
+    for (int m = m0; m <= m1; m++, buf ^= 1) {
+      stage(m + 2, m + 1, buf ^ 1);   // prefetch for the next iteration
+      cp_async_wait1();
       R Vn[NV], vL[NV], vR[NV], F[NV];
-      const int mw = wrapi(m, nd);
-      load_cell<NV>(a.V, n, base + (long long)wrapi(m + 1, nd) * stride, Vn);
 #pragma unroll
       for (int nv = 0; nv < NV; nv++) {
+        Vn[nv] = (R)stg[buf][nv][tid];
         R dv = limit<LIM>(Vn[nv] - Vc[nv], Vc[nv] - Vp[nv]);
         vL[nv] = vLn[nv];
         vR[nv] = Vc[nv] - R(0.5) * dv;
@@ -297,7 +341,7 @@ __global__ void __launch_bounds__(128) sweep_m_kernel(StageArgs<CTT> a, Grid3 g,
       }
       R Bn = R(0);
       if constexpr (PHYS != PHYS_HD) {
-        Bn = (R)__ldg(a.Bs[DIR] + base + (long long)mw * stride);
+        Bn = (R)stg[buf][NV][tid];
         vL[BX1 + DIR] = Bn;
         vR[BX1 + DIR] = Bn;
       }
@@ -307,13 +351,11 @@ __global__ void __launch_bounds__(128) sweep_m_kernel(StageArgs<CTT> a, Grid3 g,
       for (int nv = 0; nv < NV; nv++)
         if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) err |= ERR_NAN | ERR_QUIT;
       if constexpr (PHYS != PHYS_HD) {
-        if (m < m1) store_ct(a, DIR, base + (long long)mw * stride, ct);
+        if (m < m1) store_ct(a, DIR, base + (long long)wrapi(m, nd) * stride, ct);
       }
-      if (m > m0) {
-        double cd = cell_update<PHYS, NV, NDIM, MODE>(a, n, base + (long long)(m - 1) * stride,
-                                                      Fp, F, cmp, cm, DIR);
-        if constexpr (MODE == 2) cdmax = GP_MAX(cdmax, cd);
-      }
+      if (m > m0)
+        cell_update<PHYS, NV, NDIM>(a, n, base + (long long)(m - 1) * stride, Fp, F, cmp, cm,
+                                    DIR);
 #pragma unroll
       for (int nv = 0; nv < NV; nv++) {
         Vp[nv] = Vc[nv];
@@ -322,16 +364,7 @@ __global__ void __launch_bounds__(128) sweep_m_kernel(StageArgs<CTT> a, Grid3 g,
       }
       cmp = cm;
     }
-  }
-  if constexpr (MODE == 2) {
-    if (a.stage == 1) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double other = __shfl_xor_sync(0xffffffffu, cdmax, o);  // all lanes, once
-        cdmax = GP_MAX(cdmax, other);
-      }
-      if ((threadIdx.x & 31) == 0) atomic_max_pos(a.invdt_bits, cdmax);
-    }
+    cp_async_wait0();
   }
   if (err) atomicOr(a.err, err);
 }
@@ -485,47 +518,63 @@ __device__ __forceinline__ double face_new(const StageArgs<CTT>& a, int d, long 
 template <int PHYS, int NV, int NDIM, typename CTT>
 __global__ void __launch_bounds__(256) finish_kernel(StageArgs<CTT> a, Grid3 g) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= g.n) return;
   const long long n = g.n;
-  double u[8], v[8];
+  double cdt = 0.0;
+  if (c < n) {
+    double u[8], v[8];
+    // RK combine of the cell-centred variables (Src/rk_step.cpp:366-374,
+    // 509-517) with Rc = (rhs_x + rhs_y) + rhs_z
 #pragma unroll
-  for (int nv = 0; nv < NV; nv++) u[nv] = a.Uout[nv * n + c];
-  if constexpr (PHYS != PHYS_HD) {
-    const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const int i = (int)(c % nx);
-    const int j = (int)((c / nx) % ny);
-    const int k = (int)(c / ((long long)nx * ny));
-#pragma unroll
-    for (int d = 0; d < NDIM; d++) {
-      const int di = (d == 0), dj = (d == 1), dk = (d == 2);
-      const long long fr = wrapi(i + di, nx) +
-                           (long long)nx * (wrapi(j + dj, ny) + (long long)ny * wrapi(k + dk, nz));
-      double bl = face_new(a, d, c, face_rs<NDIM>(a, g, d, i, j, k));
-      double br = face_new(a, d, fr, face_rs<NDIM>(a, g, d, i + di, j + dj, k + dk));
-      a.Bsout[d][c] = bl;
-      u[BX1 + d] = 0.5 * (bl + br);
+    for (int nv = 0; nv < NV; nv++) {
+      if (!rhs_var<PHYS, NDIM>(nv)) continue;
+      double Rc = a.dU[nv * n + c] + a.dU[(NV + nv) * n + c];
+      if (NDIM == 3) Rc = Rc + a.dU[(2 * NV + nv) * n + c];
+      const double u0 = a.U0[nv * n + c];
+      if (a.stage == 1) u[nv] = u0 + Rc;
+      else u[nv] = 0.5 * u0 + 0.5 * a.Uc[nv * n + c] + 0.5 * Rc;
     }
+    cdt = a.Cdt[c] + a.Cdt[n + c];
+    if (NDIM == 3) cdt = cdt + a.Cdt[2 * n + c];
+    if constexpr (PHYS != PHYS_HD) {
+      const int nx = g.nx, ny = g.ny, nz = g.nz;
+      const int i = (int)(c % nx);
+      const int j = (int)((c / nx) % ny);
+      const int k = (int)(c / ((long long)nx * ny));
+#pragma unroll
+      for (int d = 0; d < NDIM; d++) {
+        const int di = (d == 0), dj = (d == 1), dk = (d == 2);
+        const long long fr = wrapi(i + di, nx) +
+                             (long long)nx * (wrapi(j + dj, ny) + (long long)ny * wrapi(k + dk, nz));
+        double bl = face_new(a, d, c, face_rs<NDIM>(a, g, d, i, j, k));
+        double br = face_new(a, d, fr, face_rs<NDIM>(a, g, d, i + di, j + dj, k + dk));
+        a.Bsout[d][c] = bl;
+        u[BX1 + d] = 0.5 * (bl + br);
+      }
+    }
+    uint32_t err = 0;
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++)
+      if (isnan(u[nv])) err |= ERR_NAN | ERR_QUIT;
+    uint32_t le;
+    if constexpr (PHYS == PHYS_MHD) le = mhd_cons2prim(u, v, a.gamma, a.small_rho, a.small_prs);
+    else le = hd_cons2prim(u, v, a.gamma, a.small_rho, a.small_prs);
+    err |= le;
+    if (le & ERR_CONS2PRIM_FAIL) err |= ERR_QUIT;
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      a.Uout[nv * n + c] = u[nv];
+      a.Vout[nv * n + c] = v[nv];
+    }
+    if (err) atomicOr(a.err, err);
   }
-  uint32_t err = 0;
+  if (a.stage == 1) {  // Src/update_stage.cpp:422-435, getMax 446-461
 #pragma unroll
-  for (int nv = 0; nv < NV; nv++)
-    if (isnan(u[nv])) err |= ERR_NAN | ERR_QUIT;
-  uint32_t le;
-  if constexpr (PHYS == PHYS_MHD) le = mhd_cons2prim(u, v, a.gamma, a.small_rho, a.small_prs);
-  else le = hd_cons2prim(u, v, a.gamma, a.small_rho, a.small_prs);
-  err |= le;
-  if (le & ERR_CONS2PRIM_FAIL) err |= ERR_QUIT;
-  if constexpr (PHYS != PHYS_HD) {
-#pragma unroll
-    for (int d = 0; d < NDIM; d++) a.Uout[(BX1 + d) * n + c] = u[BX1 + d];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double other = __shfl_xor_sync(0xffffffffu, cdt, o);
+      cdt = GP_MAX(cdt, other);
+    }
+    if ((threadIdx.x & 31) == 0) atomic_max_pos(a.invdt_bits, cdt);
   }
-  if (le) {
-#pragma unroll
-    for (int nv = 0; nv < NV; nv++) a.Uout[nv * n + c] = u[nv];
-  }
-#pragma unroll
-  for (int nv = 0; nv < NV; nv++) a.Vout[nv * n + c] = v[nv];
-  if (err) atomicOr(a.err, err);
 }
 
 // Start-up primitive -> conservative map (Src/startup.cpp:542-566).

@@ -59,27 +59,24 @@ static void run_stage(const StageArgs<CTT>& a, const GridDims& gd, int seg, cuda
   auto post = [&]() { if (ev) cudaEventRecord(ev[2 * kidx + 1], s); kidx++; };
   {
     const int rows = gd.ny * gd.nz;
-    const int wpb = 4;
+    const int wpb = SWEEP_THREADS / 32;
     dim3 grid((rows + wpb - 1) / wpb);
     pre();
-    sweep_x_kernel<PHYS, NV, NDIM, RS, CT, LIM, RT, CTT><<<grid, 32 * wpb, 0, s>>>(a, g);
+    sweep_x_kernel<PHYS, NV, NDIM, RS, CT, LIM, RT, CTT><<<grid, SWEEP_THREADS, 0, s>>>(a, g);
     post();
   }
   {
     const int nseg = (gd.ny + seg - 1) / seg;
-    dim3 grid((gd.nx + 127) / 128, gd.nz * nseg);
+    dim3 grid((gd.nx + SWEEP_THREADS - 1) / SWEEP_THREADS, gd.nz * nseg);
     pre();
-    if constexpr (NDIM == 2)
-      sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 1, 2, RT, CTT><<<grid, 128, 0, s>>>(a, g, seg);
-    else
-      sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 1, 1, RT, CTT><<<grid, 128, 0, s>>>(a, g, seg);
+    sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 1, RT, CTT><<<grid, SWEEP_THREADS, 0, s>>>(a, g, seg);
     post();
   }
   if constexpr (NDIM == 3) {
     const int nseg = (gd.nz + seg - 1) / seg;
-    dim3 grid((gd.nx + 127) / 128, gd.ny * nseg);
+    dim3 grid((gd.nx + SWEEP_THREADS - 1) / SWEEP_THREADS, gd.ny * nseg);
     pre();
-    sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 2, 2, RT, CTT><<<grid, 128, 0, s>>>(a, g, seg);
+    sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 2, RT, CTT><<<grid, SWEEP_THREADS, 0, s>>>(a, g, seg);
     post();
   }
   const unsigned nb = (unsigned)((gd.n + 255) / 256);
