@@ -686,6 +686,17 @@ static void Sweep(orc_t *o, int dir, double dt) {
         vL[(i+1)*nvar + nv] = v[i*nvar + nv] + 0.5*dv;
         vR[i*nvar + nv]     = v[i*nvar + nv] - 0.5*dv;
       }
+    /* relativistic velocity limiter, Src/vel_limiter.hpp:13-34 (applied in
+       the adjustment loop before the CT overwrite, plm_states.cpp:166) */
+    if (o->c.physics == ORC_RMHD) {
+      for (i = ib-1; i <= ie+1; i++) {
+        double *r = vR + i*nvar, *l = vL + (i+1)*nvar;
+        double v2m = r[VX1]*r[VX1] + r[VX1+1]*r[VX1+1] + r[VX1+2]*r[VX1+2];
+        double v2p = l[VX1]*l[VX1] + l[VX1+1]*l[VX1+1] + l[VX1+2]*l[VX1+2];
+        if (v2m >= 1.0 || v2p >= 1.0)
+          for (nv = 0; nv < nvar; nv++) r[nv] = l[nv] = v[i*nvar + nv];
+      }
+    }
     /* CT normal-field overwrite: Src/States/plm_states.cpp:184-189 */
     if (isMHD) {
       for (i = ib-1; i <= ie+1; i++) {

@@ -48,6 +48,15 @@ CASES = {
     "mhd3d_blast_mc_hlld": (ics.mhd3d_blast, dict(n=(16, 16, 16), seed=2, radius=0.2),
                             dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="hlld",
                                  ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4), 12),
+    "rmhd3d_mc_hlld_ucthll": (ics.rmhd3d_turbulence, dict(n=(10, 12, 8), seed=12),
+                              dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                   ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4), 8),
+    "rmhd2d_mc_hlld_ucthll": (ics.rmhd3d_turbulence, dict(n=(24, 20, 2), seed=13),
+                              dict(physics="RMHD", ndim=2, limiter="MC_LIM", solver="hlld",
+                                   ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4), 16),
+    "rmhd3d_vl_hll_ucthll": (ics.rmhd3d_turbulence, dict(n=(8, 10, 12), seed=14, lorentz_max=5.0),
+                             dict(physics="RMHD", ndim=3, limiter="VANLEER_LIM", solver="hll",
+                                  ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4), 8),
     "hd2d_mc_hllc": (ics.hd_turbulence, dict(n=(32, 32), seed=8),
                      dict(physics="HD", ndim=2, limiter="MC_LIM", solver="hllc",
                           cfl=0.4, first_dt=1e-4), 20),
@@ -62,9 +71,20 @@ def ref_cfg_name(rc: dict) -> str:
         ct=rc.get("ct_emf", "none"), **rc).lower()
 
 
+def _as2d(st):
+    """Take the first z-plane of a 3-D state as a 2-D state (Bz cell-centred)."""
+    V = st.V[:, :1].copy()
+    Bs = [st.Bs[0][:1].copy(), st.Bs[1][:1].copy()]
+    V[ics.BX1] = 0.5 * (Bs[0] + np.roll(Bs[0], -1, axis=2))
+    V[ics.BX2] = 0.5 * (Bs[1] + np.roll(Bs[1], -1, axis=1))
+    return ics.PrimState(st.physics, 2, (st.shape[0], st.shape[1], 1), st.gamma, V, Bs)
+
+
 def make(name: str) -> str:
     gen, kw, rc, nsteps = CASES[name]
     st = gen(**kw)
+    if rc["ndim"] == 2 and st.ndim == 3:
+        st = _as2d(st)
     cfg = br.RefConfig(name=ref_cfg_name(rc), n=st.shape, **rc)
     # the grid size is a run-time ini parameter: one binary per scheme,
     # re-using objects; the ini is rewritten per case
