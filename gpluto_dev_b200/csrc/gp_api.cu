@@ -243,8 +243,11 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   if (!grid || !scheme || !out) return fail(GP_ERR_INVALID, "null argument");
   *out = nullptr;
   if (grid->ndim != 2 && grid->ndim != 3) return fail(GP_ERR_UNSUPPORTED, "ndim must be 2 or 3");
-  if (scheme->physics != GP_MHD && scheme->physics != GP_HD)
+  if (scheme->physics != GP_MHD && scheme->physics != GP_HD && scheme->physics != GP_RMHD)
     return fail(GP_ERR_UNSUPPORTED, "physics %d not built", scheme->physics);
+  if (scheme->physics == GP_RMHD && (scheme->riemann == GP_RS_HLLC || scheme->ct_emf != GP_CT_UCT_HLL))
+    return fail(GP_ERR_UNSUPPORTED, "RMHD is built with HLLD/HLL and UCT_HLL "
+                "(the reference RMHD HLLD stores no UCT_HLLD data, Src/RMHD/hlld.cpp:526-537)");
   if (scheme->rk_stages != 2) return fail(GP_ERR_UNSUPPORTED, "only RK2 is built");
   if (scheme->precision != GP_FP64 && scheme->precision != GP_MIXED)
     return fail(GP_ERR_INVALID, "bad precision");

@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include "gp_phys.cuh"
+#include "gp_rmhd.cuh"
 
 namespace gp {
 
@@ -102,10 +103,28 @@ __device__ __forceinline__ constexpr bool rhs_var(int nv) {
 // Riemann dispatch for one interface.
 template <int PHYS, int RS, int CT, int DIR, typename R>
 __device__ __forceinline__ R riemann(const R* vl, const R* vr, R* flux, R gamma, R Bn,
-                                     CTFace<R>& ct) {
+                                     CTFace<R>& ct, uint32_t& err) {
   if constexpr (PHYS == PHYS_MHD) {
     if constexpr (RS == RS_HLLD) return mhd_hlld<DIR, CT>(vl, vr, flux, gamma, Bn, ct);
     else return mhd_hll<DIR>(vl, vr, flux, gamma, ct);
+  } else if constexpr (PHYS == PHYS_RMHD) {
+    if constexpr (sizeof(R) == sizeof(double)) {
+      return rmhd_riemann<DIR, RS>(vl, vr, flux, gamma, ct, err);
+    } else {
+      // the relativistic HLLD (secant iteration, quartic speeds, nested
+      // con2prim) is not usable in FP32 at Lorentz factors ~10: the mixed
+      // form solves it in FP64 on the FP32 reconstructed states
+      double dl[8], dr[8], df[8];
+#pragma unroll
+      for (int nv = 0; nv < 8; nv++) { dl[nv] = vl[nv]; dr[nv] = vr[nv]; }
+      CTFace<double> cd;
+      double cm = rmhd_riemann<DIR, RS>(dl, dr, df, (double)gamma, cd, err);
+#pragma unroll
+      for (int nv = 0; nv < 8; nv++) flux[nv] = (R)df[nv];
+      ct.eb = (R)cd.eb; ct.et = (R)cd.et; ct.aL = (R)cd.aL;
+      ct.aR = (R)cd.aR; ct.dL = (R)cd.dL; ct.dR = (R)cd.dR;
+      return (R)cm;
+    }
   } else {
     if constexpr (RS == RS_HLLC) return hd_hllc<DIR>(vl, vr, flux, gamma);
     else return hd_hll<DIR>(vl, vr, flux, gamma);
@@ -168,13 +187,16 @@ __global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
     load_cell<NV>(a.V, n, rb + wrapi(nx - 2, nx), vm);
     load_cell<NV>(a.V, n, rb + (nx - 1), v0);
     load_cell<NV>(a.V, n, rb + 0, vp);
+    R pVR[NV];
 #pragma unroll
     for (int nv = 0; nv < NV; nv++) {
       R dv = limit<LIM>(vp[nv] - v0[nv], v0[nv] - vm[nv]);
       pV[nv] = v0[nv];
       pVLn[nv] = v0[nv] + R(0.5) * dv;
+      pVR[nv] = v0[nv] - R(0.5) * dv;
       pF[nv] = R(0);
     }
+    if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(v0, pVR, pVLn);
   }
   R fF[NV], fCm = R(0);  // flux of face 0 (lane 0 of the first chunk)
   R F[NV], cm = R(0);
@@ -220,6 +242,10 @@ __global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
       R dv = limit<LIM>(Vp1[nv] - Vc[nv], Vc[nv] - Vm1[nv]);
       vR[nv] = Vc[nv] - R(0.5) * dv;
       vLn[nv] = Vc[nv] + R(0.5) * dv;
+    }
+    if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(Vc, vR, vLn);
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
       R l = __shfl_up_sync(FULL, vLn[nv], 1);
       vL[nv] = (lane == 0) ? pVLn[nv] : l;
     }
@@ -230,7 +256,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
       vR[BX1] = Bn;
     }
     CTFace<R> ct;
-    cm = riemann<PHYS, RS, CT, 0>(vL, vR, F, gamma, Bn, ct);
+    cm = riemann<PHYS, RS, CT, 0>(vL, vR, F, gamma, Bn, ct, err);
 #pragma unroll
     for (int nv = 0; nv < NV; nv++)
       if (act && rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) err |= ERR_NAN | ERR_QUIT;
@@ -319,12 +345,15 @@ __global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
       load_cell<NV>(a.V, n, base + wrapi(m0 - 2, nd) * stride, vmm);
       load_cell<NV>(a.V, n, base + wrapi(m0 - 1, nd) * stride, Vp);
       load_cell<NV>(a.V, n, base + (long long)m0 * stride, Vc);
+      R vrp[NV];
 #pragma unroll
       for (int nv = 0; nv < NV; nv++) {
         R dv = limit<LIM>(Vc[nv] - Vp[nv], Vp[nv] - vmm[nv]);
         vLn[nv] = Vp[nv] + R(0.5) * dv;
+        vrp[nv] = Vp[nv] - R(0.5) * dv;
         Fp[nv] = R(0);
       }
+      if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(Vp, vrp, vLn);
     }
     int buf = 0;
     for (int m = m0; m <= m1; m++, buf ^= 1) {
@@ -339,6 +368,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
         vR[nv] = Vc[nv] - R(0.5) * dv;
         vLn[nv] = Vc[nv] + R(0.5) * dv;
       }
+      if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(Vc, vR, vLn);
       R Bn = R(0);
       if constexpr (PHYS != PHYS_HD) {
         Bn = (R)stg[buf][NV][tid];
@@ -346,7 +376,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
         vR[BX1 + DIR] = Bn;
       }
       CTFace<R> ct;
-      R cm = riemann<PHYS, RS, CT, DIR>(vL, vR, F, gamma, Bn, ct);
+      R cm = riemann<PHYS, RS, CT, DIR>(vL, vR, F, gamma, Bn, ct, err);
 #pragma unroll
       for (int nv = 0; nv < NV; nv++)
         if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) err |= ERR_NAN | ERR_QUIT;
@@ -557,6 +587,8 @@ __global__ void __launch_bounds__(256) finish_kernel(StageArgs<CTT> a, Grid3 g) 
       if (isnan(u[nv])) err |= ERR_NAN | ERR_QUIT;
     uint32_t le;
     if constexpr (PHYS == PHYS_MHD) le = mhd_cons2prim(u, v, a.gamma, a.small_rho, a.small_prs);
+    else if constexpr (PHYS == PHYS_RMHD)
+      le = rmhd_cons2prim(u, v, a.gamma, a.small_rho, a.small_prs);
     else le = hd_cons2prim(u, v, a.gamma, a.small_rho, a.small_prs);
     err |= le;
     if (le & ERR_CONS2PRIM_FAIL) err |= ERR_QUIT;
@@ -587,6 +619,7 @@ __global__ void prim2cons_kernel(const double* __restrict__ V, double* __restric
 #pragma unroll
   for (int nv = 0; nv < NV; nv++) v[nv] = V[nv * n + c];
   if constexpr (PHYS == PHYS_MHD) mhd_prim2cons(v, u, gamma - 1.0);
+  else if constexpr (PHYS == PHYS_RMHD) rmhd_prim2cons(v, u, gamma);
   else hd_prim2cons(v, u, gamma);
 #pragma unroll
   for (int nv = 0; nv < NV; nv++) U[nv * n + c] = u[nv];

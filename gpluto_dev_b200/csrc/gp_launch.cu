@@ -113,6 +113,13 @@ static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey
       return by_lim<PHYS_MHD, 8, NDIM, RS_HLL, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
     return -1;
   }
+  if (k.physics == PHYS_RMHD) {
+    if (k.riemann == RS_HLLD && k.ct == CT_UCT_HLL)
+      return by_lim<PHYS_RMHD, 8, NDIM, RS_HLLD, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
+    if (k.riemann == RS_HLL && k.ct == CT_UCT_HLL)
+      return by_lim<PHYS_RMHD, 8, NDIM, RS_HLL, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
+    return -1;
+  }
   if (k.physics == PHYS_HD) {
     if (k.riemann == RS_HLLC) return by_lim<PHYS_HD, 5, NDIM, RS_HLLC, 0>(a, g, k.limiter, seg, s, ev);
     if (k.riemann == RS_HLL) return by_lim<PHYS_HD, 5, NDIM, RS_HLL, 0>(a, g, k.limiter, seg, s, ev);
@@ -134,6 +141,7 @@ int launch_prim2cons(int physics, const double* V, double* U, long long n, doubl
                      cudaStream_t s) {
   const unsigned nb = (unsigned)((n + 255) / 256);
   if (physics == PHYS_MHD) prim2cons_kernel<PHYS_MHD, 8><<<nb, 256, 0, s>>>(V, U, n, gamma);
+  else if (physics == PHYS_RMHD) prim2cons_kernel<PHYS_RMHD, 8><<<nb, 256, 0, s>>>(V, U, n, gamma);
   else if (physics == PHYS_HD) prim2cons_kernel<PHYS_HD, 5><<<nb, 256, 0, s>>>(V, U, n, gamma);
   else return -1;
   return 0;

@@ -27,7 +27,7 @@ def make_solver(st, limiter, solver, ct, cfl=0.4, cfl_max_var=1.1, precision=api
     return api.Solver.from_state(st, sch)
 
 
-@pytest.mark.parametrize("name", gu.names())
+@pytest.mark.parametrize("name", [n for n in gu.names() if not n.startswith("rmhd")])
 def test_gpu_matches_reference_fixture_bitwise(name):
     g = gu.Golden(name)
     s = make_solver(g.ic, g.limiter, g.solver, g.ct, g.cfl, g.cfl_max_var)

@@ -1,0 +1,90 @@
+"""Special-relativistic MHD on the GPU against the reference and the oracle.
+
+The RMHD fast speeds come from a quartic solved with acos/cos/sin
+(Src/RMHD/rmhd.hpp:390-452).  CUDA's and glibc's versions of those functions
+may differ in the last bit, and the pressure-fix fallback of the inversion
+is discontinuous in its input, so the FP64 form is checked to a relative
+tolerance here (the bound is written in each test) instead of bit for bit.
+"""
+import numpy as np
+import pytest
+
+import golden_util as gu
+import oracle as orc
+from gpluto_dev_b200 import api, ics
+
+pytestmark = pytest.mark.gpu
+
+RMHD_FIXTURES = [n for n in gu.names() if n.startswith("rmhd")]
+
+
+def rel_linf(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def solver(st, lim, rs, cfl=0.3, precision=api.FP64):
+    sch = api.Scheme(physics=api.RMHD, limiter=lim, riemann=rs, ct_emf="uct_hll",
+                     precision=precision, gamma=st.gamma, cfl=cfl)
+    return api.Solver.from_state(st, sch)
+
+
+@pytest.mark.parametrize("name", RMHD_FIXTURES)
+def test_rmhd_fp64_matches_reference_fixture(name):
+    """Fixtures built with extreme parameters (Lorentz factors to 10, strong
+    field) that drive the reference through its pressure-fix fallback and the
+    HLL switch of the secant iteration.  Those decisions are discontinuous in
+    their inputs, so an ulp of difference in acos/cos/sin can flip them in a
+    few cells.  Bounds: dt sequence 1e-12; L1 per variable 1e-7; 99.9% of the
+    cells within 1e-10; L-infinity 1e-3."""
+    g = gu.Golden(name)
+    s = solver(g.ic, g.limiter, g.solver, g.cfl)
+    _, hist, out = s.run(g.nsteps, g.first_dt)
+    V, U, Bs = s.download()
+    assert out.err_bits & api.ERR_QUIT == 0
+    np.testing.assert_allclose(hist, g.dt[:-1], rtol=1e-12)
+    for nv in range(8):
+        d = np.abs(U[nv] - g.U[nv]) / max(np.abs(g.U[nv]).max(), 1e-300)
+        l1 = np.abs(U[nv] - g.U[nv]).mean() / np.abs(g.U[nv]).mean()
+        assert l1 <= 1e-7, (nv, l1)
+        assert np.mean(d <= 1e-10) >= 0.999, (nv, np.mean(d <= 1e-10))
+        assert d.max() <= 1e-3, (nv, d.max())
+    for a, b in zip(Bs, g.Bs):
+        assert rel_linf(a, b) <= 1e-3
+
+
+def test_rmhd_fp64_smooth_case_matches_oracle():
+    # smooth 3-D RMHD (no error bits raised): bound 1e-11 after 20 steps
+    st = ics.rmhd3d_turbulence(n=(24, 24, 24), seed=5, lorentz_max=3.0, sigma=0.3, p0=1.0)
+    o = orc.Oracle(st, limiter="mc", solver="hlld", ct="uct_hll", cfl=0.3)
+    oh, oerr = o.run(20, 1e-4)
+    Vo, Uo, Bo = o.state()
+    s = solver(st, "mc", "hlld")
+    _, hist, out = s.run(20, 1e-4)
+    V, U, Bs = s.download()
+    assert oerr == 0 and out.err_bits == 0
+    for nv in range(8):
+        assert rel_linf(U[nv], Uo[nv]) <= 1e-11, (nv, rel_linf(U[nv], Uo[nv]))
+
+
+def test_rmhd_mixed_error_bounded():
+    st = ics.rmhd3d_turbulence(n=(24, 24, 24), seed=5, lorentz_max=3.0, sigma=0.3, p0=1.0)
+    a = solver(st, "mc", "hlld")
+    b = solver(st, "mc", "hlld", precision=api.MIXED)
+    a.run(20, 1e-4)
+    b.run(20, 1e-4)
+    _, Ua, _ = a.download()
+    _, Ub, _ = b.download()
+    for nv in range(8):
+        l1 = np.abs(Ub[nv] - Ua[nv]).mean() / np.abs(Ua[nv]).mean()
+        assert l1 <= 1e-4, (nv, l1)
+
+
+def test_rmhd_192_config_runs_100_steps_without_errors():
+    st = ics.rmhd3d_turbulence(n=(192, 192, 192), seed=1)
+    s = solver(st, "mc", "hlld")
+    _, _, out = s.run(100, 1e-4, history=False)
+    assert out.err_bits == 0
+    _, _, Bs = s.download()
+    div = ((np.roll(Bs[0], -1, 2) - Bs[0]) + (np.roll(Bs[1], -1, 1) - Bs[1])
+           + (np.roll(Bs[2], -1, 0) - Bs[2]))
+    assert np.abs(div).max() / max(np.abs(b).max() for b in Bs) <= 1e-12
