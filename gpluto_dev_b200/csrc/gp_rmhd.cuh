@@ -409,10 +409,15 @@ __device__ __forceinline__ int hlld_riemann_state(RState<R>& P, R p, R Bx, int s
 }
 
 // Src/RMHD/hlld.cpp:561-644
+// One deliberate difference: when a Riemann state cannot be built (w < 0) the
+// reference discards that status and evaluates the admissibility checks on the
+// state's previous (or never set) fields, so with a negative pressure guess
+// the result depends on stale stack contents.  Here a failed state always
+// fails the star solution (HLL fallback), which is deterministic.
 template <int DIR, typename R>
 __device__ __forceinline__ R hlld_fstar(RState<R>& PaL, RState<R>& PaR, R p, R Bx, R& Sc) {
-  hlld_riemann_state<DIR>(PaL, p, Bx, -1);
-  hlld_riemann_state<DIR>(PaR, p, Bx, 1);
+  const int okL = hlld_riemann_state<DIR>(PaL, p, Bx, -1);
+  const int okR = hlld_riemann_state<DIR>(PaR, p, Bx, 1);
   R dK = PaR.Kx - PaL.Kx + R(1.e-12);
   R Bxc = Bx * dK;
   R Byc = PaR.By * (PaR.Kx - PaR.vx) - PaL.By * (PaL.Kx - PaL.vx) + Bx * (PaR.vy - PaL.vy);
@@ -433,7 +438,7 @@ __device__ __forceinline__ R hlld_fstar(RState<R>& PaL, RState<R>& PaR, R p, R B
   success *= (PaL.w - p) > R(0);
   success *= (PaL.Sa - PaL.S) > R(-1.e-6);
   success *= (PaR.S - PaR.Sa) > R(-1.e-6);
-  PaL.fail = !success;
+  PaL.fail = !(success && okL && okR);
   return fun;
 }
 
@@ -553,7 +558,7 @@ __device__ __forceinline__ R rmhd_riemann(const R* vl, const R* vr, R* flux, R g
     R p0, f0, p, f, Sc;
     const R dS_1 = R(1) / (Sr - Sl);
     R Uhll[8];
-    RState<R> PaL, PaR;
+    RState<R> PaL = {}, PaR = {};
 #pragma unroll
     for (int nv = 0; nv < 8; nv++) {
       Uhll[nv] = Sr * ur[nv] - Sl * ul[nv] + fl[nv] - fr[nv];

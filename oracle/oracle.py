@@ -55,6 +55,8 @@ def lib():
         L.orc_next_dt.argtypes = [ctypes.c_double] * 4
         L.orc_run.restype = ctypes.c_uint32
         L.orc_run.argtypes = [P, ctypes.c_int, ctypes.c_double, D]
+        L.orc_set_ulp_nudge.argtypes = [ctypes.c_int]
+        L.orc_set_rmhd_strict.argtypes = [ctypes.c_int]
         L.orc_prim_to_cons.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_long, D, D]
         _lib = L
     return _lib
@@ -62,6 +64,17 @@ def lib():
 
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def set_ulp_nudge(n: int) -> None:
+    """Checker knob: perturb the RMHD quartic's acos result by n ulps."""
+    lib().orc_set_ulp_nudge(int(n))
+
+
+def set_rmhd_strict(on: bool) -> None:
+    """Checker knob: fail the RMHD HLLD star state when a Riemann state cannot
+    be built (the rule the GPU kernels use); off reproduces the reference."""
+    lib().orc_set_rmhd_strict(1 if on else 0)
 
 
 def prim_to_cons(physics: int, gamma: float, V: np.ndarray) -> np.ndarray:

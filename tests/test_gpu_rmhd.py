@@ -28,28 +28,55 @@ def solver(st, lim, rs, cfl=0.3, precision=api.FP64):
     return api.Solver.from_state(st, sch)
 
 
+def deviation(U, G):
+    """Worst over the 8 conserved variables of: L1 relative error, fraction of
+    cells within 1e-10 of the variable's maximum, L-infinity relative error."""
+    l1, frac, linf = 0.0, 1.0, 0.0
+    for nv in range(8):
+        scale = max(np.abs(G[nv]).max(), 1e-300)
+        d = np.abs(U[nv] - G[nv])
+        l1 = max(l1, d.mean() / np.abs(G[nv]).mean())
+        frac = min(frac, float(np.mean(d / scale <= 1e-10)))
+        linf = max(linf, d.max() / scale)
+    return l1, frac, linf
+
+
 @pytest.mark.parametrize("name", RMHD_FIXTURES)
 def test_rmhd_fp64_matches_reference_fixture(name):
     """Fixtures built with extreme parameters (Lorentz factors to 10, strong
-    field) that drive the reference through its pressure-fix fallback and the
-    HLL switch of the secant iteration.  Those decisions are discontinuous in
-    their inputs, so an ulp of difference in acos/cos/sin can flip them in a
-    few cells.  Bounds: dt sequence 1e-12; L1 per variable 1e-7; 99.9% of the
-    cells within 1e-10; L-infinity 1e-3."""
+    field) drive the reference through its pressure-fix fallback and the HLL
+    switch of the secant iteration.  Those decisions are discontinuous, so
+    one ulp of difference in acos/cos/sin flips them in a few cells.  The
+    bound is calibrated on the oracle itself: the oracle run with its acos
+    result moved by +1 and -1 ulp gives the spread that libm rounding alone
+    produces; the GPU must stay within 4x that spread (L1 and L-infinity,
+    floors 1e-12 / 1e-11) and lose at most 1% more cells beyond 1e-10.
+    The dt sequence must agree to 1e-12."""
     g = gu.Golden(name)
+    spread = []
+    try:
+        for nudge in (1, -1):
+            orc.set_ulp_nudge(nudge)
+            o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct, cfl=g.cfl)
+            o.run(g.nsteps, g.first_dt)
+            spread.append(deviation(o.state()[1], g.U))
+    finally:
+        orc.set_ulp_nudge(0)
+    l1_ref = max(x[0] for x in spread)
+    frac_ref = min(x[1] for x in spread)
+    linf_ref = max(x[2] for x in spread)
+
     s = solver(g.ic, g.limiter, g.solver, g.cfl)
     _, hist, out = s.run(g.nsteps, g.first_dt)
     V, U, Bs = s.download()
     assert out.err_bits & api.ERR_QUIT == 0
     np.testing.assert_allclose(hist, g.dt[:-1], rtol=1e-12)
-    for nv in range(8):
-        d = np.abs(U[nv] - g.U[nv]) / max(np.abs(g.U[nv]).max(), 1e-300)
-        l1 = np.abs(U[nv] - g.U[nv]).mean() / np.abs(g.U[nv]).mean()
-        assert l1 <= 1e-7, (nv, l1)
-        assert np.mean(d <= 1e-10) >= 0.999, (nv, np.mean(d <= 1e-10))
-        assert d.max() <= 1e-3, (nv, d.max())
+    l1, frac, linf = deviation(U, g.U)
+    assert l1 <= max(4 * l1_ref, 1e-12), (l1, l1_ref)
+    assert linf <= max(4 * linf_ref, 1e-11), (linf, linf_ref)
+    assert frac >= frac_ref - 0.01, (frac, frac_ref)
     for a, b in zip(Bs, g.Bs):
-        assert rel_linf(a, b) <= 1e-3
+        assert rel_linf(a, b) <= max(4 * linf_ref, 1e-11)
 
 
 def test_rmhd_fp64_smooth_case_matches_oracle():

@@ -37,3 +37,40 @@ def test_oracle_divb_roundoff():
            + (np.roll(Bs[2], -1, 0) - Bs[2]) * nz)
     bmax = max(np.abs(b).max() for b in Bs)
     assert np.abs(div).max() / (bmax * max(nx, ny, nz)) < 1e-12
+
+
+def _run_state(g):
+    o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct, cfl=g.cfl)
+    o.run(g.nsteps, g.first_dt)
+    return o.state()[1]
+
+
+RMHD_FIXTURES = [n for n in gu.names() if n.startswith("rmhd")]
+
+
+def test_rmhd_strict_rule_leaves_fixtures_unchanged():
+    """The GPU fails the HLLD star state when a Riemann state cannot be built
+    (w < 0), where the reference goes on with that state's stale fields
+    (Src/RMHD/hlld.cpp:578-628).  On every fixture the oracle gives the same
+    bits under both rules, so the fixtures pin the GPU's rule too."""
+    for name in RMHD_FIXTURES:
+        g = gu.Golden(name)
+        try:
+            orc.set_rmhd_strict(True)
+            U = _run_state(g)
+        finally:
+            orc.set_rmhd_strict(False)
+        assert np.array_equal(U, g.U), name
+
+
+def test_ulp_nudge_moves_rmhd_and_resets():
+    """The acos nudge (checker knob) perturbs the RMHD result; back at 0 the
+    oracle is bitwise the reference again."""
+    g = gu.Golden(RMHD_FIXTURES[0])
+    try:
+        orc.set_ulp_nudge(1)
+        U1 = _run_state(g)
+    finally:
+        orc.set_ulp_nudge(0)
+    assert not np.array_equal(U1, g.U)
+    assert np.array_equal(_run_state(g), g.U)
