@@ -23,7 +23,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("GPLUTO_B200_LIB") or os.path.join(_HERE, "_build",
                                                              "libgpluto_b200.so")
 
-GP_OK, GP_ERR_QUIT, GP_ERR_NO_DEVICE = 0, -5, -6
+GP_OK, GP_ERR_INVALID, GP_ERR_QUIT, GP_ERR_NO_DEVICE = 0, -1, -5, -6
 HD, MHD, RMHD = 0, 1, 2
 LIMITERS = {"flat": 0, "minmod": 1, "vl": 2, "vanleer": 2, "mc": 3}
 SOLVERS = {"hll": 0, "hllc": 1, "hlld": 2}

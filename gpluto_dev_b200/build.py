@@ -25,6 +25,7 @@ UNITS = [
     ("gp_launch_fp64.o", "gp_launch.cu", ["-DGP_MIXED=0", "-fmad=false"]),
     ("gp_launch_mixed.o", "gp_launch.cu", ["-DGP_MIXED=1", "-fmad=true"]),
     ("gp_api.o", "gp_api.cu", ["-fmad=false"]),
+    ("gp_noalloc.o", "gp_noalloc.cu", ["-fmad=false"]),
 ]
 
 

@@ -143,6 +143,30 @@ int gp_profile_steps(gp_handle *h, int nsteps, double *dt, float *kernel_ms, int
 /* Name of launch q of a step (as ordered by gp_profile_steps). */
 const char *gp_kernel_name(const gp_handle *h, int q);
 
+/* Limits of gp_advance_step_noalloc: the largest grid it accepts (cells) and
+   the doubles of device scratch it keeps per cell. */
+#define GP_NOALLOC_MAX_CELLS 16384
+#define GP_NOALLOC_DOUBLES_PER_CELL 62
+
+/* One RK2 step (the same kernels and results as gp_advance_step) that
+   allocates nothing.  No counterpart in the reference: it exists for callers
+   that cannot call cudaMalloc -- hosts whose device memory belongs to
+   another allocator, loops that must not allocate or grow their device
+   footprint.  It synchronizes `stream` before returning (the step scalars
+   are read back).  Uc/Vc/Vs0..2 are DEVICE pointers the caller owns,
+   interior layout, updated in place (Vs1/Vs2 NULL where unused).  Every
+   intermediate lives in one static device array of
+   GP_NOALLOC_MAX_CELLS * GP_NOALLOC_DOUBLES_PER_CELL doubles (~8 MB) that
+   each GPU loading the library holds until exit; grids of more than
+   GP_NOALLOC_MAX_CELLS cells return GP_ERR_INVALID.  The first call on a
+   device looks up that array's device address (cudaGetSymbolAddress), so
+   make it before any stream capture.  All calls share the array: calls
+   that overlap on the GPU race.  Returns a gp_status (no gp_last_error
+   text); `out` as for gp_advance_step. */
+int gp_advance_step_noalloc(const gp_grid_desc *grid, const gp_scheme *scheme,
+                            double *Uc, double *Vc, double *Vs0, double *Vs1, double *Vs2,
+                            double dt, void *stream, gp_step_out *out);
+
 /* Text of the last error on this thread. */
 const char *gp_last_error(void);
 
