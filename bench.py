@@ -45,13 +45,17 @@ N = 256
 # per stage: 5 x 8 B x (NVAR + n_face)) for 3-D ideal MHD
 ALG_BYTES_ZONE = 440
 # compulsory bytes per cell of each kernel of the FP64 3-D MHD step (arrays
-# it must read and write once, 8 B each), indexed by (kernel, stage)
+# it must read and write once, 8 B each), indexed by (kernel, stage):
+#   sweep  V(8) + Bs_n(1) -> dU_dir(5) + C_dir(1) + UCT(6)            21 x 8
+#   emf    UCT(18) + Bs(3) -> Ee(3)                                    24 x 8
+#   finish dU(15) + C(3) + U0(5) [+ Uc(5)] + Ee(3) + Bs(3) [+ Bs0(3)]
+#          -> Bs'(3) + U(8) + V(8)                           48 x 8 [56 x 8]
 KERNEL_BYTES = {
     ("sweep_x", 1): 168, ("sweep_x", 2): 168,
-    ("sweep_y", 1): 216, ("sweep_y", 2): 216,
-    ("sweep_z", 1): 248, ("sweep_z", 2): 288,
+    ("sweep_y", 1): 168, ("sweep_y", 2): 168,
+    ("sweep_z", 1): 168, ("sweep_z", 2): 168,
     ("emf", 1): 192, ("emf", 2): 192,
-    ("finish", 1): 224, ("finish", 2): 248,
+    ("finish", 1): 384, ("finish", 2): 448,
 }
 REF_SAMPLE_N = 64
 REF_BINARY = os.path.join(ROOT, "oracle", "_ref", "mhd3d_mc_lim_hlld_uct_hlld", "pluto")
