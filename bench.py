@@ -2,6 +2,7 @@
 """Throughput of the B200 Godunov step on the 3-D 256^3 ideal-MHD blast.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload mhd3d_blast|ensemble]
 
 Workload (one "step" = one full RK2 step of the grid): 3-D ideal MHD, 256^3
 periodic on [0,1]^3, PLM with the MC limiter, HLLD, UCT_HLLD constrained
@@ -18,6 +19,13 @@ collective); value = zone updates of all ranks / max-over-ranks time.
 the reference sources into oracle/_ref by __graft_entry__.build()) on all
 host cores, one independent process per core, each step a bounded sample:
 one RK2 step of a 64^3 grid of the same scheme per process.
+
+``--workload ensemble`` (default 200 steps): 512 independent 2-D ideal-MHD
+grids (sides log-uniform 64..512, square and 2:1, half FP64 / half mixed,
+per-grid dt), advanced by the batched step -- one persistent kernel per RK
+stage over all grids, the steps replayed from a CUDA graph -- with tile
+shapes picked per size bin by gpluto_dev_b200.autotune on a sample of the
+grids first.  value = zone updates of all grids / device time.
 """
 from __future__ import annotations
 
@@ -404,19 +412,266 @@ def impl_ours(args):
     return 0
 
 
+# --------------------------------------------------------------------------
+# batched ensemble: many uneven 2-D grids, one persistent launch per stage
+# --------------------------------------------------------------------------
+ENSEMBLE_ALG_BYTES_ZONE = 400   # 2-D ideal MHD: 5 x 8 B x (8 + 2)
+REF_BINARY_2D = os.path.join(ROOT, "oracle", "_ref", "mhd2d_mc_lim_hlld_uct_hlld", "pluto")
+
+
+def ensemble_config(args, table=None):
+    from gpluto_dev_b200 import workloads
+    shapes = workloads.ensemble_shapes(args.grids)
+    cells = sum(a * b for (a, b), _ in shapes)
+    c = {"workload": f"ensemble_{args.grids}x_2d_ideal_mhd",
+         "grids": args.grids, "sides": "log-uniform 64..512, alternately square and 2:1",
+         "cells_total": cells, "precision": "half FP64, half mixed (FP32 flux)",
+         "scheme": "PLM-MC + HLLD + UCT_HLLD + RK2, CFL 0.4, gamma 5/3, per-grid dt",
+         "ic": "2-D turbulence (random |k|<=4 modes), seed = grid index",
+         "launch": "one persistent kernel per RK stage over all grids, CUDA graph",
+         "l2": "inputs larger than L2 (state of all grids ~15 GB), no flush",
+         "parallelism": "replicas x1"}
+    if table is not None:
+        c["tile_table"] = table
+    return c
+
+
+def run_reference_grids(states, nsteps_timed, nwarm, binary, ndim=2):
+    """The reference serial build on `states`, one concurrent process per
+    grid.  Returns (Mzone-updates/s aggregate, mean s/step)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle", "ref"))
+    from gpluto_dev_b200 import ics
+    import build_ref as br
+    total = nwarm + nsteps_timed
+    with tempfile.TemporaryDirectory() as tmp:
+        procs = []
+        for r, st in enumerate(states):
+            d = os.path.join(tmp, f"p{r}")
+            os.makedirs(d)
+            nx, ny, nz = st.shape
+            cfg = br.RefConfig(name="bench", physics="MHD", ndim=ndim, n=(nx, ny, nz),
+                               limiter="MC_LIM", solver="hlld", ct_emf="UCT_HLLD", cfl=0.4,
+                               first_dt=FIRST_DT)
+            open(os.path.join(d, "pluto.ini"), "w").write(cfg.ini())
+            icp = os.path.join(d, "ic.bin")
+            ics.write_ic(icp, st)
+            env = dict(os.environ, GPLUTO_FTZ_DAZ="0", GP_IC_FILE=icp,
+                       GP_DUMP_STEP=str(total + 1), GP_DUMP_FILE=os.path.join(d, "out.dump"))
+            procs.append((d, st, subprocess.Popen([binary, "-no-write", "-maxsteps", str(total + 1)],
+                                                  cwd=d, env=env, stdout=subprocess.DEVNULL,
+                                                  stderr=subprocess.DEVNULL)))
+        rate, per = 0.0, []
+        for d, st, p in procs:
+            p.wait()
+            w = br.read_dump(os.path.join(d, "out.dump")).wall
+            sps = (w[nwarm + nsteps_timed] - w[nwarm]) / nsteps_timed
+            per.append(sps)
+            rate += st.ncells / sps
+    return rate / 1e6, statistics.mean(per)
+
+
+def ensemble_cpu_baseline(args, nproc):
+    from gpluto_dev_b200 import workloads
+    members = workloads.ensemble(args.grids, members=set(range(0, args.grids, max(1, args.grids // nproc))))
+    members = members[:nproc]
+    states = [m.state for m in members]
+    if os.path.exists(REF_BINARY_2D):
+        v, sps = run_reference_grids(states, 2, 1, REF_BINARY_2D)
+        kind = "reference"
+    else:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(len(states), mp_context=mp.get_context("spawn")) as ex:
+            per = list(ex.map(_oracle_grid_worker, [(m.shape, m.seed) for m in members]))
+        v = sum(st.ncells / t for st, t in zip(states, per)) / 1e6
+        sps = statistics.mean(per)
+        kind = "port"
+    sample = (f"{len(states)} concurrent single-thread processes, each one ensemble member "
+              f"(every {max(1, args.grids // nproc)}th grid, FP64), 2 timed RK2 steps after 1 "
+              f"warm-up; Mzone-updates/s summed over processes")
+    return {"value": v, "unit": METRIC, "cores": len(states), "kind": kind, "sample": sample}, sps
+
+
+def _oracle_grid_worker(a):
+    shape, seed = a
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    from gpluto_dev_b200 import ics
+    o = orc.Oracle(ics.mhd2d_turbulence(n=shape, seed=seed), limiter="mc", solver="hlld",
+                   ct="uct_hlld")
+    dt = FIRST_DT
+    inv, _ = o.step(dt)
+    dt = orc.lib().orc_next_dt(inv, 0.4, 1.1, dt)
+    t0 = time.perf_counter()
+    for _ in range(2):
+        inv, _ = o.step(dt)
+        dt = orc.lib().orc_next_dt(inv, 0.4, 1.1, dt)
+    return (time.perf_counter() - t0) / 2
+
+
+def impl_ensemble(args):
+    import torch
+    from gpluto_dev_b200 import autotune, workloads
+    from gpluto_dev_b200 import batch as gb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    members = workloads.ensemble(args.grids, seed0=rank * args.grids)
+    cells = sum(m.state.ncells for m in members)
+    stream = torch.cuda.Stream()
+    pool = sum(gb.slot_bytes(m.state, m.scheme) for m in members) + (64 << 20)
+
+    # ---- autotune tile shapes per size bin on a sample (every 4th grid) ----
+    sample = members[::4]
+    tb = gb.Batch(sum(gb.slot_bytes(m.state, m.scheme) for m in sample) + (64 << 20),
+                  len(sample), stream=stream.cuda_stream)
+    info = {tb.add(m.state, m.scheme, FIRST_DT, 10 ** 7): (2, m.state.ncells) for m in sample}
+    trials = []
+    table = autotune.tune(tb, info, steps=3, reps=2, log=trials)
+    tb.close()
+    del tb
+
+    # ---- the run: all grids, warm-up then K timed steps -----------------
+    b = gb.Batch(pool, len(members), stream=stream.cuda_stream)
+    slots = [b.add(m.state, m.scheme, FIRST_DT, args.warmup + args.steps,
+                   autotune.shape_for(table, 2, m.state.ncells)) for m in members]
+    autotune.apply(b, table, {s: (2, m.state.ncells) for s, m in zip(slots, members)})
+    b.advance(args.warmup)
+    b.wait()
+    clock = ClockSampler(local)
+    barrier()
+    clock.start()
+    time.sleep(0.25)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream.synchronize()
+    e0.record(stream)
+    b.advance(args.steps)
+    e1.record(stream)
+    b.wait()
+    clocks = clock.stop()
+    barrier()
+    t_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    err = 0
+    done = []
+    for s in slots:
+        st = b.status(s)
+        err |= st.err_bits
+        done.append(st.steps_done)
+    ctas = b.info()["ctas"]
+    b.close()
+    del b
+    value = world * cells * args.steps / (t_ms * 1e-3) / 1e6
+    peak, peak_kind = peaks()
+    achieved = ENSEMBLE_ALG_BYTES_ZONE * cells * args.steps / (t_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "batch_stage_kernel (persistent, all grids)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "traffic": None,
+                "alg_bytes_per_zone_update": ENSEMBLE_ALG_BYTES_ZONE,
+                "note": "step-level algorithmic bytes (2-D MHD state read+written once per "
+                        "stage) over the whole-batch time"}
+
+    # ---- end to end: admission from host arrays, K steps, download -------
+    e2e = None
+    if not args.no_e2e:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b = gb.Batch(pool, len(members), stream=stream.cuda_stream)
+        sl = [b.add(m.state, m.scheme, FIRST_DT, args.steps,
+                    autotune.shape_for(table, 2, m.state.ncells)) for m in members]
+        autotune.apply(b, table, {s: (2, m.state.ncells) for s, m in zip(sl, members)})
+        b.advance(args.steps)
+        b.wait()
+        nout = 0
+        for s in sl:
+            V, U, Bs = b.download(s)
+            nout += (V.size + U.size + sum(x.size for x in Bs)) * 8
+        te = time.perf_counter() - t0
+        b.close()
+        nin = sum((m.state.V.size + sum(x.size for x in m.state.Bs)) * 8 for m in members)
+        if dist is not None:
+            tt = torch.tensor([te], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        e2e = {"value": world * cells * args.steps / te / 1e6, "unit": METRIC,
+               "h2d_bytes_per_step": nin / args.steps, "d2h_bytes_per_step": nout / args.steps,
+               "steps": args.steps,
+               "path": "gp_batch_add of every grid from host arrays, gp_batch_advance(K), "
+                       "gp_batch_download of every grid; bytes amortised over K steps"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu, _ = ensemble_cpu_baseline(args, max(1, min(os.cpu_count() or 1, 16)))
+
+    if dist is not None:
+        barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+            "data": "synthetic (seeded 2-D turbulence ensemble)",
+            "config": ensemble_config(args, table), "roofline": roofline,
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 2 * args.steps,
+            "clocks": clocks, "ctas": ctas, "err_bits": err,
+            "steps_done_min": min(done), "autotune_trials": len(trials)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def impl_reference_ensemble(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    nproc = max(1, min(os.cpu_count() or 1, 64))
+    cpu, sps = ensemble_cpu_baseline(args, nproc)
+    line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": METRIC,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": ensemble_config(args), "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mhd3d_blast", choices=["mhd3d_blast", "ensemble"])
     ap.add_argument("--n", type=int, default=N)
+    ap.add_argument("--grids", type=int, default=512)
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.steps is None:
+        args.steps = 200 if args.workload == "ensemble" else 100
+    if args.workload == "ensemble":
+        return impl_reference_ensemble(args) if args.impl == "reference" else impl_ensemble(args)
     if args.impl == "reference":
         return impl_reference(args)
     return impl_ours(args)

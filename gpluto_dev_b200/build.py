@@ -5,7 +5,9 @@
 Produces gpluto_dev_b200/_build/libgpluto_b200.so from csrc/ with nvcc:
 gp_launch.cu twice (FP64 form with -fmad=false so the plain form keeps the
 reference's rounding sequence; mixed form with contraction), gp_api.cu for
-the C ABI.  Objects are rebuilt only when a source is newer.
+the C ABI, and the batched step (gp_batch_tiles.cu twice + gp_batch.cu) as
+relocatable device code with its device-link object.  Objects are rebuilt
+only when a source is newer.
 """
 from __future__ import annotations
 
@@ -27,6 +29,16 @@ UNITS = [
     ("gp_api.o", "gp_api.cu", ["-fmad=false"]),
     ("gp_noalloc.o", "gp_noalloc.cu", ["-fmad=false"]),
 ]
+# Batched step: relocatable device code, so that one persistent kernel can
+# call the tile bodies of both forms (each compiled with its own contraction
+# rule); 168 registers = 3 blocks of 128 threads per SM, as the sweeps.
+RDC = ["-rdc=true", "-maxrregcount=168"]
+RDC_UNITS = [
+    ("gp_batch_tiles_fp64.o", "gp_batch_tiles.cu", ["-DGP_MIXED=0", "-fmad=false", *RDC]),
+    ("gp_batch_tiles_mixed.o", "gp_batch_tiles.cu", ["-DGP_MIXED=1", "-fmad=true", *RDC]),
+    ("gp_batch.o", "gp_batch.cu", ["-fmad=false", *RDC]),
+]
+DLINK = "gp_batch_dlink.o"
 
 
 def nvcc() -> str:
@@ -46,9 +58,12 @@ def build(verbose: bool = False, jobs: int = 3) -> str:
     newest = max(os.path.getmtime(p) for p in _deps())
     procs = []
     objs = []
-    for obj, src, flags in UNITS:
+    rdc_objs = []
+    for obj, src, flags in UNITS + RDC_UNITS:
         o = os.path.join(OUT, obj)
         objs.append(o)
+        if (obj, src, flags) in RDC_UNITS:
+            rdc_objs.append(o)
         if os.path.exists(o) and os.path.getmtime(o) >= newest:
             continue
         cmd = [nvcc(), *ARCH, *BASE, *flags, "-c", os.path.join(CSRC, src), "-o", o]
@@ -59,6 +74,11 @@ def build(verbose: bool = False, jobs: int = 3) -> str:
         out, _ = p.communicate()
         if p.returncode != 0:
             raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + out.decode()[-6000:])
+    dl = os.path.join(OUT, DLINK)
+    if (not os.path.exists(dl)) or os.path.getmtime(dl) < max(os.path.getmtime(o) for o in rdc_objs):
+        subprocess.run([nvcc(), *ARCH, "-Xcompiler", "-fPIC", "-dlink", *rdc_objs, "-o", dl],
+                       check=True)
+    objs.append(dl)
     if (not os.path.exists(LIB)) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
         subprocess.run(cmd, check=True)

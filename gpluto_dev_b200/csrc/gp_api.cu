@@ -229,6 +229,10 @@ int check_device() {
 
 }  // namespace
 
+namespace gp {
+int set_last_error(int code, const char* msg) { return fail(code, "%s", msg); }
+}  // namespace gp
+
 extern "C" {
 
 const char* gp_last_error(void) { return g_err; }

@@ -165,15 +165,22 @@ __device__ __forceinline__ void store_ct(const StageArgs<CTT>& a, int dir, long 
 // Face f (between cells f-1 and f) is computed by lane f%32; the lane then
 // updates cell f-1.  The first face's flux is kept for cell nx-1.
 // ---------------------------------------------------------------------
+// Staging area of one 128-thread block: [2 buffers][SL values][128 threads].
+template <int NV>
+constexpr int sweep_x_stage_doubles() { return 2 * (2 * NV + 1) * SWEEP_THREADS; }
+template <int NV>
+constexpr int sweep_m_stage_doubles() { return 2 * (NV + 1) * SWEEP_THREADS; }
+
+// One x-row per warp.  `stg_` is the block's staging area
+// (sweep_x_stage_doubles<NV>() doubles of shared memory), `tid` the thread's
+// index in its 128-thread block.
 template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, typename R, typename CTT>
-__global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
-    sweep_x_kernel(StageArgs<CTT> a, Grid3 g) {
+__device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3& g, int row,
+                                            double* stg_, int tid) {
   constexpr unsigned FULL = 0xffffffffu;
   constexpr int SL = 2 * NV + 1;  // staged doubles per lane: V[f], V[f+1], Bs[f]
-  __shared__ double stg[2][SL][SWEEP_THREADS];
-  const int tid = threadIdx.x;
-  const int lane = threadIdx.x & 31;
-  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  double(*stg)[SL][SWEEP_THREADS] = reinterpret_cast<double(*)[SL][SWEEP_THREADS]>(stg_);
+  const int lane = tid & 31;
   if (row >= g.ny * g.nz) return;  // warp-uniform
   const int nx = g.nx;
   const long long n = g.n;
@@ -303,6 +310,14 @@ __global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
   if (err) atomicOr(a.err, err);
 }
 
+template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, typename R, typename CTT>
+__global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
+    sweep_x_kernel(StageArgs<CTT> a, Grid3 g) {
+  __shared__ double stg[sweep_x_stage_doubles<NV>()];
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  sweep_x_row<PHYS, NV, NDIM, RS, CT, LIM, R, CTT>(a, g, row, stg, threadIdx.x);
+}
+
 // ---------------------------------------------------------------------
 // y / z sweep: thread per (x, pencil segment), marching along DIR with a
 // register window of three cells; the cell two steps ahead and the next face
@@ -310,17 +325,15 @@ __global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
 // is solved.  Writes the direction's flux differences, inverse-dt terms and
 // UCT face data (no loads besides the stencil).
 // ---------------------------------------------------------------------
+// One (x column i, transverse index t, pencil segment seg) per thread: t is
+// k for DIR=1 and j for DIR=2; the segment covers cells [seg*S, seg*S+S).
+// `stg_` is the block's staging area (sweep_m_stage_doubles<NV>() doubles).
 template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, int DIR, typename R,
           typename CTT>
-__global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
-    sweep_m_kernel(StageArgs<CTT> a, Grid3 g, int S) {
-  __shared__ double stg[2][NV + 1][SWEEP_THREADS];
-  const int tid = threadIdx.x;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void sweep_m_col(const StageArgs<CTT>& a, const Grid3& g, int i, int t,
+                                            int seg, int S, double* stg_, int tid) {
+  double(*stg)[NV + 1][SWEEP_THREADS] = reinterpret_cast<double(*)[NV + 1][SWEEP_THREADS]>(stg_);
   const int nd = (DIR == 1) ? g.ny : g.nz;
-  const int nseg = (nd + S - 1) / S;
-  const int t = blockIdx.y / nseg;       // k for DIR=1, j for DIR=2
-  const int seg = blockIdx.y - t * nseg;
   const long long n = g.n;
   const R gamma = (R)a.gamma;
   uint32_t err = 0;
@@ -399,6 +412,19 @@ __global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
   if (err) atomicOr(a.err, err);
 }
 
+template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, int DIR, typename R,
+          typename CTT>
+__global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
+    sweep_m_kernel(StageArgs<CTT> a, Grid3 g, int S) {
+  __shared__ double stg[sweep_m_stage_doubles<NV>()];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nd = (DIR == 1) ? g.ny : g.nz;
+  const int nseg = (nd + S - 1) / S;
+  const int t = blockIdx.y / nseg;
+  const int seg = blockIdx.y - t * nseg;
+  sweep_m_col<PHYS, NV, NDIM, RS, CT, LIM, DIR, R, CTT>(a, g, i, t, seg, S, stg, threadIdx.x);
+}
+
 // ---------------------------------------------------------------------
 // UCT edge EMF (Src/MHD/CT/ct_emf_average.cpp:535-995, reconstruction of
 // Src/array_reconstruct.cpp:45-206: face field with MC, stored velocities
@@ -428,9 +454,9 @@ __device__ __forceinline__ void face_coef(const StageArgs<CTT>& a, int d, long l
   dR = R(0.5) * ((R)a.ct[d][5][f1] + (R)a.ct[d][5][f2]);
 }
 
+// The edge EMFs whose lower corner is cell c (all three in 3-D, Ez in 2-D).
 template <int NDIM, int LIM, typename R, typename CTT>
-__global__ void __launch_bounds__(256) emf_kernel(StageArgs<CTT> a, Grid3 g) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g, long long c) {
   if (c >= g.n) return;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int i = (int)(c % nx);
@@ -510,6 +536,11 @@ __global__ void __launch_bounds__(256) emf_kernel(StageArgs<CTT> a, Grid3 g) {
   }
 }
 
+template <int NDIM, int LIM, typename R, typename CTT>
+__global__ void __launch_bounds__(256) emf_kernel(StageArgs<CTT> a, Grid3 g) {
+  emf_cell<NDIM, LIM, R, CTT>(a, g, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // ---------------------------------------------------------------------
 // Stage finish: CT update (Src/MHD/CT/ct_update.cpp:181-423), face RK
 // combine (Src/rk_step.cpp:378-385, 536-552), cell-centred average
@@ -545,9 +576,10 @@ __device__ __forceinline__ double face_new(const StageArgs<CTT>& a, int d, long 
   return 0.5 * a.Bs0[d][f] + 0.5 * bc + 0.5 * rs;
 }
 
+// Stage finish of cell c; returns its inverse-dt sum (0 outside the grid).
 template <int PHYS, int NV, int NDIM, typename CTT>
-__global__ void __launch_bounds__(256) finish_kernel(StageArgs<CTT> a, Grid3 g) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ double finish_cell(const StageArgs<CTT>& a, const Grid3& g,
+                                              long long c) {
   const long long n = g.n;
   double cdt = 0.0;
   if (c < n) {
@@ -599,14 +631,25 @@ __global__ void __launch_bounds__(256) finish_kernel(StageArgs<CTT> a, Grid3 g) 
     }
     if (err) atomicOr(a.err, err);
   }
-  if (a.stage == 1) {  // Src/update_stage.cpp:422-435, getMax 446-461
+  return cdt;
+}
+
+// Stage-1 CFL maximum (Src/update_stage.cpp:422-435, getMax 446-461): warp
+// maximum, then one atomic per warp.  All 32 lanes must call it.
+__device__ __forceinline__ void warp_invdt_max(unsigned long long* bits, double cdt, int lane) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double other = __shfl_xor_sync(0xffffffffu, cdt, o);
-      cdt = GP_MAX(cdt, other);
-    }
-    if ((threadIdx.x & 31) == 0) atomic_max_pos(a.invdt_bits, cdt);
+  for (int o = 16; o > 0; o >>= 1) {
+    const double other = __shfl_xor_sync(0xffffffffu, cdt, o);
+    cdt = GP_MAX(cdt, other);
   }
+  if (lane == 0) atomic_max_pos(bits, cdt);
+}
+
+template <int PHYS, int NV, int NDIM, typename CTT>
+__global__ void __launch_bounds__(256) finish_kernel(StageArgs<CTT> a, Grid3 g) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const double cdt = finish_cell<PHYS, NV, NDIM, CTT>(a, g, c);
+  if (a.stage == 1) warp_invdt_max(a.invdt_bits, cdt, threadIdx.x & 31);
 }
 
 // Start-up primitive -> conservative map (Src/startup.cpp:542-566).

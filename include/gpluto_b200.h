@@ -167,6 +167,69 @@ int gp_advance_step_noalloc(const gp_grid_desc *grid, const gp_scheme *scheme,
                             double *Uc, double *Vc, double *Vs0, double *Vs1, double *Vs2,
                             double dt, void *stream, gp_step_out *out);
 
+/* ---------------------------------------------------------------------
+   Batched step: many independent grids ("slots") in one device pool,
+   advanced together by one persistent kernel launch per RK stage, the
+   launches of a run of steps captured once as a CUDA graph.  Each slot keeps
+   its own dt sequence (NextTimeStep on the device, exactly as
+   gp_advance_steps) and its own step budget; a slot whose budget is spent,
+   or that raised ERR_QUIT, stops advancing.  Built schemes: ideal MHD with
+   PLM-MC + HLLD + UCT_HLLD and HD with PLM-MC + HLLC, 2-D and 3-D, FP64 or
+   mixed per slot, periodic boundaries.  The reference advances one grid per
+   process; this has no reference counterpart beyond the step it repeats.
+   --------------------------------------------------------------------- */
+typedef struct gp_batch gp_batch;
+
+/* Tile shape of one slot (0 = default): `seg` is the pencil segment of the
+   y/z sweeps (cells one thread marches), `cells_per_thread` the cells each
+   thread of an edge-EMF or finish tile handles. */
+typedef struct gp_tile_shape {
+  int seg;
+  int cells_per_thread;
+} gp_tile_shape;
+
+typedef struct gp_slot_status {
+  int steps_done;         /* steps completed since admission */
+  int steps_left;         /* budget left (0: finished or stopped) */
+  uint32_t err_bits;      /* OR of the ERR_* bits since admission */
+  double dt;              /* dt of the next step */
+  double invDt_hyp;       /* invDt_hyp of the last completed step */
+} gp_slot_status;
+
+/* Reserve a device pool of `pool_bytes` holding up to `max_slots` grids.
+   `ctas` = blocks of the persistent launch (0: all that fit on the device).
+   `stream` as for gp_create (NULL: the batch creates its own). */
+int gp_batch_create(size_t pool_bytes, int max_slots, int ctas, void *stream, gp_batch **out);
+int gp_batch_destroy(gp_batch *b);
+/* Device bytes a slot of this grid and scheme takes from the pool. */
+size_t gp_batch_slot_bytes(const gp_grid_desc *grid, const gp_scheme *scheme);
+/* Admit a grid: primitives Vc and face fields Vs0..2 (host, interior layout;
+   Vs* NULL for HD) become the slot's state (U from the start-up PrimToCons),
+   first step dt0, budget nsteps.  Returns GP_ERR_NOMEM when the pool or the
+   slot table is full.  Takes effect at the next gp_batch_advance. */
+int gp_batch_add(gp_batch *b, const gp_grid_desc *grid, const gp_scheme *scheme,
+                 const gp_tile_shape *shape, const double *Vc, const double *Vs0,
+                 const double *Vs1, const double *Vs2, double dt0, int nsteps, int *slot);
+/* Change a slot's tile shape, or the blocks of the persistent launch (0: all
+   that fit); results do not depend on either.  Take effect at the next
+   gp_batch_advance. */
+int gp_batch_set_shape(gp_batch *b, int slot, const gp_tile_shape *shape);
+int gp_batch_set_ctas(gp_batch *b, int ctas);
+/* Release a slot and its pool space (after gp_batch_wait). */
+int gp_batch_remove(gp_batch *b, int slot);
+/* Enqueue `nsteps` steps of every slot with budget left (asynchronous; the
+   graph for this step count is captured on first use). */
+int gp_batch_advance(gp_batch *b, int nsteps);
+/* Wait for the enqueued steps and refresh every slot's status. */
+int gp_batch_wait(gp_batch *b);
+int gp_batch_slot_status(const gp_batch *b, int slot, gp_slot_status *st);
+/* Copy a slot's state to the host (interior layout; any pointer may be NULL). */
+int gp_batch_download(gp_batch *b, int slot, double *Uc, double *Vc, double *Vs0,
+                      double *Vs1, double *Vs2);
+/* Pool occupancy, slot count and blocks of the persistent launch. */
+int gp_batch_info(const gp_batch *b, size_t *pool_used, size_t *pool_bytes, int *slots,
+                  int *ctas);
+
 /* Text of the last error on this thread. */
 const char *gp_last_error(void);
 

@@ -62,3 +62,33 @@ def test_no_cpu_fallback_without_device():
     with pytest.raises(api.GPError) as ei:
         api.Solver(2, (16, 16), api.Scheme())
     assert ei.value.code == api.GP_ERR_NO_DEVICE
+
+
+def test_batch_slot_bytes_formula():
+    """Pool bytes of one slot: U (2 copies), V, per-direction dU and C_dt,
+    3 face buffers, 6 UCT arrays per direction (float in the mixed form) and
+    the edge EMFs, each array rounded up to 256 bytes, plus the scalars."""
+    from gpluto_dev_b200 import batch as gb, ics
+    al = lambda x: (x + 255) // 256 * 256
+    st = ics.mhd2d_turbulence(n=(64, 48), seed=1)
+    n = 64 * 48
+    c = 8 * n
+    exp = 2 * al(8 * c) + al(8 * c) + al(16 * c) + al(2 * c) + 6 * al(c) + 12 * al(c) + al(c) + 256
+    assert gb.slot_bytes(st, api.Scheme()) == exp
+    mixed = gb.slot_bytes(st, api.Scheme(precision=api.MIXED))
+    assert exp - mixed == 12 * (al(c) - al(4 * n))
+    sh = ics.hd_turbulence(n=(20, 16, 12), seed=1)
+    n = 20 * 16 * 12
+    c = 8 * n
+    assert gb.slot_bytes(sh, api.Scheme(physics=api.HD, riemann="hllc")) == \
+        2 * al(5 * c) + al(5 * c) + al(15 * c) + al(3 * c) + 256
+
+
+def test_batch_has_no_cpu_path():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    from gpluto_dev_b200 import batch as gb
+    with pytest.raises(api.GPError) as ei:
+        gb.Batch(1 << 20, 4)
+    assert ei.value.code == api.GP_ERR_NO_DEVICE
