@@ -4,9 +4,9 @@ ctypes front end of the ``gp_batch_*`` entry points of
 include/gpluto_b200.h.  A :class:`Batch` owns one device pool; every
 admitted grid ("slot") keeps its state there, its own dt sequence (the
 reference's NextTimeStep, Src/next_time_step.cpp:80,125, evaluated on the
-device) and its own step budget.  :meth:`Batch.advance` runs one persistent
-kernel launch per RK stage over all slots, the launches of a run of steps
-replayed from a captured CUDA graph.
+device) and its own step budget.  :meth:`Batch.advance` runs, per RK stage,
+one persistent sweep launch and one persistent EMF/finish launch over all
+slots, the launches of a run of steps replayed from a captured CUDA graph.
 
 Each slot advances exactly like :class:`gpluto_dev_b200.api.Solver.run` on
 its own (same kernels, same operation order): the FP64 form is
@@ -136,7 +136,7 @@ class Batch:
         api._check(_lib().gp_batch_set_shape(self._h, slot, ctypes.byref(shape.to_c())))
 
     def set_ctas(self, ctas: int):
-        """Blocks of the persistent launch (0: all that fit on the device)."""
+        """Blocks of the sweep launch (0: all that fit on the device)."""
         api._check(_lib().gp_batch_set_ctas(self._h, ctas))
 
     def remove(self, slot: int):

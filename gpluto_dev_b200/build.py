@@ -5,7 +5,7 @@
 Produces gpluto_dev_b200/_build/libgpluto_b200.so from csrc/ with nvcc:
 gp_launch.cu twice (FP64 form with -fmad=false so the plain form keeps the
 reference's rounding sequence; mixed form with contraction), gp_api.cu for
-the C ABI, and the batched step (gp_batch_tiles.cu twice + gp_batch.cu) as
+the C ABI, and the batched step (gp_batch_tiles.cu four times + gp_batch.cu) as
 relocatable device code with its device-link object.  Objects are rebuilt
 only when a source is newer.
 """
@@ -31,12 +31,16 @@ UNITS = [
 ]
 # Batched step: relocatable device code, so that one persistent kernel can
 # call the tile bodies of both forms (each compiled with its own contraction
-# rule); 168 registers = 3 blocks of 128 threads per SM, as the sweeps.
-RDC = ["-rdc=true", "-maxrregcount=168"]
+# rule).  Sweep tiles: 168 registers = 3 blocks of 128 threads per SM, as the
+# single-grid sweeps; EMF/finish tiles: 64 registers = 8 blocks per SM.
+SWEEP_RDC = ["-rdc=true", "-maxrregcount=168", "-DGP_BATCH_PART=0"]
+CELL_RDC = ["-rdc=true", "-maxrregcount=64", "-DGP_BATCH_PART=1"]
 RDC_UNITS = [
-    ("gp_batch_tiles_fp64.o", "gp_batch_tiles.cu", ["-DGP_MIXED=0", "-fmad=false", *RDC]),
-    ("gp_batch_tiles_mixed.o", "gp_batch_tiles.cu", ["-DGP_MIXED=1", "-fmad=true", *RDC]),
-    ("gp_batch.o", "gp_batch.cu", ["-fmad=false", *RDC]),
+    ("gp_batch_sweeps_fp64.o", "gp_batch_tiles.cu", ["-DGP_MIXED=0", "-fmad=false", *SWEEP_RDC]),
+    ("gp_batch_sweeps_mixed.o", "gp_batch_tiles.cu", ["-DGP_MIXED=1", "-fmad=true", *SWEEP_RDC]),
+    ("gp_batch_cells_fp64.o", "gp_batch_tiles.cu", ["-DGP_MIXED=0", "-fmad=false", *CELL_RDC]),
+    ("gp_batch_cells_mixed.o", "gp_batch_tiles.cu", ["-DGP_MIXED=1", "-fmad=true", *CELL_RDC]),
+    ("gp_batch.o", "gp_batch.cu", ["-fmad=false", "-rdc=true"]),
 ]
 DLINK = "gp_batch_dlink.o"
 

@@ -1,16 +1,18 @@
 // gp_batch.cu -- batched step: one device pool, a slot table, a phase-ordered
-// tile table and one persistent kernel per RK stage; runs of steps captured
-// as CUDA graphs (C ABI in include/gpluto_b200.h).
+// tile table and two persistent launches per RK stage over all slots; runs
+// of steps captured as CUDA graphs (C ABI in include/gpluto_b200.h).
 //
-// A stage launch: every block repeatedly takes the next tile from an atomic
-// queue head.  Tiles are ordered sweeps -> edge EMFs -> finish; an EMF tile of
-// slot s first waits until all sweep tiles of s have completed, a finish
-// tile until all EMF tiles of s have (HD: all sweep tiles).  Each wait is a
-// bounded spin: after kSpinLimit polls the block records a batch error and
-// skips, and once that error is set every later wait gives up at once, so a
-// launch always ends.  The last finish tile of slot s in stage 2 evaluates
-// NextTimeStep for s (the same arithmetic as the single-grid path), rotates
-// its face buffers and counts the step.
+// In each launch every block repeatedly takes the next tile from an atomic
+// queue head.  The sweep launch (168 registers, 3 blocks/SM) takes the sweep
+// tiles of every slot; the cell launch (64 registers, 8 blocks/SM: the edge
+// EMF and finish bodies are latency-bound and want the occupancy) takes the
+// EMF tiles, then the finish tiles, and a finish tile of slot s first waits
+// until all EMF tiles of s have completed.  Each wait is a bounded spin:
+// after kSpinLimit polls the block records a batch error and skips, and once
+// that error is set every later wait gives up at once, so a launch always
+// ends.  The last finish tile of slot s in stage 2 evaluates NextTimeStep for
+// s (the same arithmetic as the single-grid path), rotates its face buffers
+// and counts the step.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -62,29 +64,30 @@ __device__ void step_epilogue(const BatchSlot& s) {
   if (sc->err & ERR_QUIT) sc->steps_left = 0;
 }
 
-__global__ void __launch_bounds__(BATCH_THREADS, GP_SWEEP_MINB)
-    batch_stage_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
-                       const int* __restrict__ ntiles_p, BatchCounters* ctr, int stage,
-                       uint32_t* batch_err) {
-  extern __shared__ double smem[];
+// Persistent loop of one launch: part 0 takes the sweep tiles [0, nsweep),
+// part 1 the EMF and finish tiles [nsweep, ntiles).
+template <int PART>
+__device__ __forceinline__ void batch_loop(const BatchSlot* __restrict__ slots,
+                                           const BatchTile* __restrict__ tiles,
+                                           const BatchTableHeader* __restrict__ hdr,
+                                           BatchCounters* ctr, int stage, uint32_t* batch_err,
+                                           double* smem) {
   __shared__ int s_tile;
   __shared__ int s_go;
-  const int ntiles = *ntiles_p;
+  const int t0 = PART == 0 ? 0 : hdr->nsweep;
+  const int t1 = PART == 0 ? hdr->nsweep : hdr->ntiles;
   for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(&ctr->head, 1);
+    if (threadIdx.x == 0) s_tile = t0 + atomicAdd(&ctr->head[PART], 1);
     __syncthreads();
     const int ti = s_tile;
-    if (ti >= ntiles) break;  // block-uniform
+    if (ti >= t1) break;  // block-uniform
     const BatchTile t = tiles[ti];
     const BatchSlot& s = slots[t.slot];
     if (threadIdx.x == 0) {
       int go = s.sc->steps_left > 0 && ld_volatile(batch_err) == 0u;
-      int dep = -1;
-      if (t.phase == BP_EMF) dep = BG_SWEEPS;
-      else if (t.phase == BP_FINISH) dep = (s.physics == PHYS_HD) ? BG_SWEEPS : BG_EMF;
-      if (go && dep >= 0) {
-        const int need = s.need[dep];
-        const int* c = &ctr->done[t.slot * BG_COUNT + dep];
+      if (go && PART == 1 && t.phase == BP_FINISH && s.physics != PHYS_HD) {
+        const int need = s.need[BG_EMF];
+        const int* c = &ctr->done[t.slot * BG_COUNT + BG_EMF];
         long long it = 0;
         while (ld_acquire(c) < need) {
           if (ld_volatile(batch_err) != 0u) { go = 0; break; }
@@ -101,12 +104,17 @@ __global__ void __launch_bounds__(BATCH_THREADS, GP_SWEEP_MINB)
     __syncthreads();
     const int go = s_go;
     if (go) {
-      if (s.precision == GP_MIXED) batch_tile_mixed(s, t, stage, smem);
-      else batch_tile_fp64(s, t, stage, smem);
+      if constexpr (PART == 0) {
+        if (s.precision == GP_MIXED) batch_sweep_tile_mixed(s, t, stage, smem);
+        else batch_sweep_tile_fp64(s, t, stage, smem);
+      } else {
+        if (s.precision == GP_MIXED) batch_cell_tile_mixed(s, t, stage);
+        else batch_cell_tile_fp64(s, t, stage);
+      }
     }
     __syncthreads();  // the tile's writes are done; s_tile/s_go may be reused
-    if (threadIdx.x == 0 && go) {
-      const int grp = t.phase <= BP_SWEEP_Z ? BG_SWEEPS : (t.phase == BP_EMF ? BG_EMF : BG_FINISH);
+    if (PART == 1 && threadIdx.x == 0 && go) {
+      const int grp = t.phase == BP_EMF ? BG_EMF : BG_FINISH;
       __threadfence();
       const int old = atomicAdd(&ctr->done[t.slot * BG_COUNT + grp], 1);
       if (grp == BG_FINISH && stage == 2 && old == s.need[BG_FINISH] - 1) {
@@ -115,6 +123,21 @@ __global__ void __launch_bounds__(BATCH_THREADS, GP_SWEEP_MINB)
       }
     }
   }
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS, GP_SWEEP_MINB)
+    batch_sweep_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
+                       const BatchTableHeader* __restrict__ hdr, BatchCounters* ctr, int stage,
+                       uint32_t* batch_err) {
+  extern __shared__ double smem[];
+  batch_loop<0>(slots, tiles, hdr, ctr, stage, batch_err, smem);
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS, GP_CELL_MINB)
+    batch_cell_kernel(const BatchSlot* __restrict__ slots, const BatchTile* __restrict__ tiles,
+                      const BatchTableHeader* __restrict__ hdr, BatchCounters* ctr, int stage,
+                      uint32_t* batch_err) {
+  batch_loop<1>(slots, tiles, hdr, ctr, stage, batch_err, nullptr);
 }
 
 int fail(int code, const char* fmt, ...) {
@@ -195,7 +218,8 @@ struct gp_batch {
   BatchSlot* slots_d;
   BatchTile* tiles_d;
   int tiles_cap;
-  int* ntiles_d;
+  gp::BatchTableHeader* hdr_d;
+  int cell_ctas;  // blocks of the cell launch
   gp::BatchCounters* ctr_d;
   size_t ctr_bytes;
   uint32_t* err_d;
@@ -251,7 +275,7 @@ void free_batch(gp_batch* b) {
   cudaFree(b->pool);
   cudaFree(b->slots_d);
   cudaFree(b->tiles_d);
-  cudaFree(b->ntiles_d);
+  cudaFree(b->hdr_d);
   cudaFree(b->ctr_d);
   cudaFree(b->err_d);
   cudaFreeHost(b->sc_h);
@@ -283,9 +307,10 @@ void tile_counts(BatchSlot& s) {
   s.need[gp::BG_FINISH] = s.ntiles[gp::BP_FINISH];
 }
 
-// Phase-ordered tile table: all sweeps, then all EMF tiles, then all finish
-// tiles; within a group, slots from the largest grid down, so that the
-// groups of the largest (longest) grids complete first.
+// Phase-ordered tile table: all sweeps (the sweep launch), then all EMF
+// tiles, then all finish tiles (the cell launch); within a group, slots from
+// the largest grid down, so that the EMF tiles of the largest (longest)
+// grids complete first.
 int rebuild_tiles(gp_batch* b) {
   std::vector<int> order;
   for (int i = 0; i < b->max_slots; i++)
@@ -296,13 +321,16 @@ int rebuild_tiles(gp_batch* b) {
   const int groups[3][3] = {{gp::BP_SWEEP_X, gp::BP_SWEEP_Y, gp::BP_SWEEP_Z},
                             {gp::BP_EMF, -1, -1},
                             {gp::BP_FINISH, -1, -1}};
-  for (int gi = 0; gi < 3; gi++)
+  int nsweep = 0;
+  for (int gi = 0; gi < 3; gi++) {
     for (int sidx : order)
       for (int q = 0; q < 3; q++) {
         const int ph = groups[gi][q];
         if (ph < 0) continue;
         for (int k = 0; k < b->slots[sidx].ntiles[ph]; k++) t.push_back(BatchTile{sidx, ph, k, 0});
       }
+    if (gi == 0) nsweep = (int)t.size();
+  }
   const int nt = (int)t.size();
   if (nt > b->tiles_cap) {
     // captured graphs hold the old table's address: drop them
@@ -315,7 +343,8 @@ int rebuild_tiles(gp_batch* b) {
     b->tiles_cap = cap;
   }
   if (nt) BATCH_CUDA(cudaMemcpy(b->tiles_d, t.data(), sizeof(BatchTile) * nt, cudaMemcpyHostToDevice));
-  BATCH_CUDA(cudaMemcpy(b->ntiles_d, &nt, sizeof(int), cudaMemcpyHostToDevice));
+  gp::BatchTableHeader h{nsweep, nt};
+  BATCH_CUDA(cudaMemcpy(b->hdr_d, &h, sizeof(h), cudaMemcpyHostToDevice));
   BATCH_CUDA(cudaMemcpy(b->slots_d, b->slots.data(), sizeof(BatchSlot) * b->max_slots,
                         cudaMemcpyHostToDevice));
   b->dirty = false;
@@ -330,8 +359,10 @@ int capture(gp_batch* b, int nsteps, cudaGraphExec_t* out) {
   for (int st = 0; st < nsteps && ok; st++)
     for (int stage = 1; stage <= 2 && ok; stage++) {
       if (cudaMemsetAsync(b->ctr_d, 0, b->ctr_bytes, b->stream) != cudaSuccess) ok = false;
-      gp::batch_stage_kernel<<<b->ctas, gp::BATCH_THREADS, smem, b->stream>>>(
-          b->slots_d, b->tiles_d, b->ntiles_d, b->ctr_d, stage, b->err_d);
+      gp::batch_sweep_kernel<<<b->ctas, gp::BATCH_THREADS, smem, b->stream>>>(
+          b->slots_d, b->tiles_d, b->hdr_d, b->ctr_d, stage, b->err_d);
+      gp::batch_cell_kernel<<<b->cell_ctas, gp::BATCH_THREADS, 0, b->stream>>>(
+          b->slots_d, b->tiles_d, b->hdr_d, b->ctr_d, stage, b->err_d);
       if (cudaGetLastError() != cudaSuccess) ok = false;
     }
   cudaError_t e = cudaStreamEndCapture(b->stream, &g);
@@ -388,24 +419,29 @@ int gp_batch_create(size_t pool_bytes, int max_slots, int ctas, void* stream, gp
   chk(cudaMalloc((void**)&b->pool, b->pool_bytes), "device pool");
   b->free_list[0] = b->pool_bytes;
   chk(cudaMalloc((void**)&b->slots_d, sizeof(BatchSlot) * max_slots), "slot table");
-  chk(cudaMalloc((void**)&b->ntiles_d, sizeof(int)), "tile count");
+  chk(cudaMalloc((void**)&b->hdr_d, sizeof(gp::BatchTableHeader)), "tile table header");
   b->ctr_bytes = sizeof(gp::BatchCounters) + sizeof(int) * (size_t)max_slots * gp::BG_COUNT;
   chk(cudaMalloc((void**)&b->ctr_d, b->ctr_bytes), "counters");
   chk(cudaMalloc((void**)&b->err_d, sizeof(uint32_t)), "error word");
   chk(cudaMallocHost((void**)&b->sc_h, sizeof(BatchScalars) * max_slots), "status mirror");
   if (rc == GP_OK) {
     chk(cudaMemset(b->slots_d, 0, sizeof(BatchSlot) * max_slots), "memset");
-    chk(cudaMemset(b->ntiles_d, 0, sizeof(int)), "memset");
+    chk(cudaMemset(b->hdr_d, 0, sizeof(gp::BatchTableHeader)), "memset");
     chk(cudaMemset(b->err_d, 0, sizeof(uint32_t)), "memset");
     std::memset(b->sc_h, 0, sizeof(BatchScalars) * max_slots);
     int per_sm = 0, nsm = 0, dev = 0;
     chk(cudaGetDevice(&dev), "device");
     chk(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "SM count");
-    chk(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gp::batch_stage_kernel,
+    chk(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gp::batch_sweep_kernel,
                                                       gp::BATCH_THREADS, gp::batch_smem_bytes()),
         "occupancy");
     b->ctas_full = std::max(1, per_sm) * nsm;
     b->ctas = ctas > 0 ? ctas : b->ctas_full;
+    int per_sm_cell = 0;
+    chk(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_cell, gp::batch_cell_kernel,
+                                                      gp::BATCH_THREADS, 0),
+        "occupancy");
+    b->cell_ctas = std::max(1, per_sm_cell) * nsm;
   }
   if (rc != GP_OK) {
     free_batch(b);

@@ -1,14 +1,16 @@
 // gp_batch.h -- device-side tables of the batched step (many independent
-// grids advanced by one persistent launch per RK stage).
+// grids advanced together by persistent launches).
 //
 // Each grid ("slot") keeps its own state in a region of one device pool, its
-// own dt sequence and step budget.  A stage launch walks a table of tiles
-// ordered by phase (all sweeps, then all edge-EMF tiles, then all finish
-// tiles); a tile of a later phase of slot s waits until every tile of the
-// earlier phase of s has completed (per-slot counters).  Tiles are taken
-// from an atomic queue head, so a waiting tile only ever waits on tiles that
-// running blocks have already taken: progress does not depend on how many
-// blocks are resident.
+// own dt sequence and step budget.  An RK stage is two persistent launches
+// over all slots: the sweep launch (register-heavy Riemann work, 3 blocks
+// per SM) takes every sweep tile; the cell launch (edge EMFs and the stage
+// finish, latency-bound, 8 blocks per SM) takes every EMF tile, then every
+// finish tile.  A finish tile of slot s waits until every EMF tile of s has
+// completed (per-slot counters).  Tiles are taken from an atomic queue head
+// in table order, so a waiting tile only ever waits on tiles that running
+// blocks have already taken: progress does not depend on how many blocks
+// are resident.
 #pragma once
 #include <cstdint>
 
@@ -61,18 +63,36 @@ struct BatchSlot {
 
 static_assert(sizeof(StageArgs<double>) == sizeof(StageArgs<float>), "StageArgs layout");
 
-// Queue head and per-slot group counters; cleared before every stage launch.
+// Tile table header: tiles [0, nsweep) are sweep tiles, [nsweep, ntiles)
+// EMF then finish tiles.
+struct BatchTableHeader {
+  int nsweep;
+  int ntiles;
+};
+
+// Queue heads of the two launches and per-slot group counters; cleared
+// before every stage.
 struct BatchCounters {
-  int head;
-  int pad[31];
+  int head[2];
+  int pad[30];
   int done[1];  // [max_slots][BG_COUNT]
 };
 
-// Stage tile dispatch, one per precision form (separate translation units,
-// relocatable device code: the FP64 form is compiled without contraction so
-// that it keeps the reference's rounding, the mixed form with it).
-__device__ void batch_tile_fp64(const BatchSlot& s, const BatchTile& t, int stage, double* smem);
-__device__ void batch_tile_mixed(const BatchSlot& s, const BatchTile& t, int stage, double* smem);
+// Tile dispatch, one per part and precision form (separate translation
+// units of relocatable device code: the FP64 form is compiled without
+// contraction so that it keeps the reference's rounding, the mixed form with
+// it; the sweep part with the sweeps' register budget, the cell part with a
+// small one).  Called by every thread of the block.
+__device__ void batch_sweep_tile_fp64(const BatchSlot& s, const BatchTile& t, int stage,
+                                      double* smem);
+__device__ void batch_sweep_tile_mixed(const BatchSlot& s, const BatchTile& t, int stage,
+                                       double* smem);
+__device__ void batch_cell_tile_fp64(const BatchSlot& s, const BatchTile& t, int stage);
+__device__ void batch_cell_tile_mixed(const BatchSlot& s, const BatchTile& t, int stage);
+
+#ifndef GP_CELL_MINB
+#define GP_CELL_MINB 8
+#endif
 
 // Shared memory a block needs (largest staging area of any phase).
 constexpr int batch_smem_bytes() {

@@ -1,8 +1,9 @@
 // gp_batch_tiles.cu -- one tile of a batched stage: the same per-row,
 // per-column and per-cell bodies as the single-grid kernels, applied to one
-// slot's StageArgs.  Compiled twice as relocatable device code: GP_MIXED=0
-// (FP64, -fmad=false: bit-identical to the single-grid FP64 step) and
-// GP_MIXED=1 (FP32 reconstruction/Riemann/EMF, contraction allowed).
+// slot's StageArgs.  Compiled four times as relocatable device code:
+// GP_BATCH_PART=0 (sweep tiles) or 1 (EMF and finish tiles), each with
+// GP_MIXED=0 (FP64, -fmad=false: bit-identical to the single-grid FP64 step)
+// and GP_MIXED=1 (FP32 reconstruction/Riemann/EMF, contraction allowed).
 //
 // Schemes built for batches: ideal MHD with PLM-MC + HLLD + UCT_HLLD and
 // hydrodynamics with PLM-MC + HLLC, in 2-D and 3-D (the ensemble and serving
@@ -12,17 +13,28 @@
 #ifndef GP_MIXED
 #define GP_MIXED 0
 #endif
+#ifndef GP_BATCH_PART
+#define GP_BATCH_PART 0
+#endif
 
 namespace gp {
 
 #if GP_MIXED
 using RT = float;
 using CTT = float;
-#define GP_BATCH_TILE batch_tile_mixed
+#if GP_BATCH_PART == 0
+#define GP_BATCH_TILE batch_sweep_tile_mixed
+#else
+#define GP_BATCH_TILE batch_cell_tile_mixed
+#endif
 #else
 using RT = double;
 using CTT = double;
-#define GP_BATCH_TILE batch_tile_fp64
+#if GP_BATCH_PART == 0
+#define GP_BATCH_TILE batch_sweep_tile_fp64
+#else
+#define GP_BATCH_TILE batch_cell_tile_fp64
+#endif
 #endif
 
 namespace {
@@ -49,6 +61,7 @@ __device__ __forceinline__ void run_tile(const StageArgs<CTT>& a, const Grid3& g
                                          int cpt, int phase, int idx, int stage, double* smem) {
   const int tid = threadIdx.x;
   switch (phase) {
+#if GP_BATCH_PART == 0
     case BP_SWEEP_X:
       sweep_x_row<PHYS, NV, NDIM, RS, CT, LIM, RT, CTT>(
           a, g, idx * BATCH_ROWS_PER_TILE + (tid >> 5), smem, tid);
@@ -62,6 +75,7 @@ __device__ __forceinline__ void run_tile(const StageArgs<CTT>& a, const Grid3& g
         sweep_m_item<PHYS, NV, NDIM, RS, CT, LIM, 2>(
             a, g, seg, (long long)idx * BATCH_THREADS + tid, smem, tid);
       break;
+#else
     case BP_EMF:
       if constexpr (PHYS != PHYS_HD) {
         const long long c0 = (long long)idx * BATCH_THREADS * cpt + tid;
@@ -79,6 +93,7 @@ __device__ __forceinline__ void run_tile(const StageArgs<CTT>& a, const Grid3& g
       if (stage == 1) warp_invdt_max(a.invdt_bits, mx, tid & 31);
       break;
     }
+#endif
     default:
       break;
   }
@@ -88,8 +103,12 @@ __device__ __forceinline__ void run_tile(const StageArgs<CTT>& a, const Grid3& g
 
 static_assert(sizeof(StageArgs<CTT>) % 8 == 0, "StageArgs copied as 8-byte words");
 
-// Called by every thread of the block.
+#if GP_BATCH_PART == 0
 __device__ void GP_BATCH_TILE(const BatchSlot& s, const BatchTile& t, int stage, double* smem) {
+#else
+__device__ void GP_BATCH_TILE(const BatchSlot& s, const BatchTile& t, int stage) {
+  double* smem = nullptr;  // the cell bodies stage nothing
+#endif
   // One copy of the slot's StageArgs per block, in shared memory: the bodies
   // store through the state pointers, and shared memory cannot alias them,
   // so the fields are read cheaply without a private copy per thread.

@@ -169,8 +169,9 @@ int gp_advance_step_noalloc(const gp_grid_desc *grid, const gp_scheme *scheme,
 
 /* ---------------------------------------------------------------------
    Batched step: many independent grids ("slots") in one device pool,
-   advanced together by one persistent kernel launch per RK stage, the
-   launches of a run of steps captured once as a CUDA graph.  Each slot keeps
+   advanced together: per RK stage one persistent sweep launch and one
+   persistent EMF/finish launch over all slots, the launches of a run of
+   steps captured once as a CUDA graph.  Each slot keeps
    its own dt sequence (NextTimeStep on the device, exactly as
    gp_advance_steps) and its own step budget; a slot whose budget is spent,
    or that raised ERR_QUIT, stops advancing.  Built schemes: ideal MHD with
@@ -197,7 +198,8 @@ typedef struct gp_slot_status {
 } gp_slot_status;
 
 /* Reserve a device pool of `pool_bytes` holding up to `max_slots` grids.
-   `ctas` = blocks of the persistent launch (0: all that fit on the device).
+   `ctas` = blocks of the sweep launch (0: all that fit on the device; the
+   EMF/finish launch always uses all that fit).
    `stream` as for gp_create (NULL: the batch creates its own). */
 int gp_batch_create(size_t pool_bytes, int max_slots, int ctas, void *stream, gp_batch **out);
 int gp_batch_destroy(gp_batch *b);
@@ -210,8 +212,8 @@ size_t gp_batch_slot_bytes(const gp_grid_desc *grid, const gp_scheme *scheme);
 int gp_batch_add(gp_batch *b, const gp_grid_desc *grid, const gp_scheme *scheme,
                  const gp_tile_shape *shape, const double *Vc, const double *Vs0,
                  const double *Vs1, const double *Vs2, double dt0, int nsteps, int *slot);
-/* Change a slot's tile shape, or the blocks of the persistent launch (0: all
-   that fit); results do not depend on either.  Take effect at the next
+/* Change a slot's tile shape, or the blocks of the sweep launch (0: all that
+   fit); results do not depend on either.  Take effect at the next
    gp_batch_advance. */
 int gp_batch_set_shape(gp_batch *b, int slot, const gp_tile_shape *shape);
 int gp_batch_set_ctas(gp_batch *b, int ctas);
