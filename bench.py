@@ -655,13 +655,94 @@ def impl_reference_ensemble(args):
     return 0
 
 
+# --------------------------------------------------------------------------
+# serving: Poisson arrivals, continuous batching, p50/p99 latency vs rate
+# --------------------------------------------------------------------------
+SERVE_RATES = (2.0, 4.0, 8.0, 16.0)
+
+
+def impl_serve(args):
+    import torch
+    from gpluto_dev_b200 import autotune, serve, workloads
+    from gpluto_dev_b200 import batch as gb
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:          # replicas only: the serving sweep runs on one GPU
+        return 0
+    nreq = args.requests
+    base = workloads.requests(nreq, 1.0, seed=7)          # unit-rate arrival times
+    states = [q.state() for q in base]                    # request payloads, built up front
+    work = sum(q.cells * q.nsteps for q in base)
+    stream = torch.cuda.Stream()
+    # tile shapes per size bin, tuned on a sample of the requests
+    sample = list(range(0, nreq, max(1, nreq // 16)))
+    tb = gb.Batch(sum(gb.slot_bytes(states[i], base[i].scheme()) for i in sample) + (64 << 20),
+                  len(sample), stream=stream.cuda_stream)
+    info = {tb.add(states[i], base[i].scheme(), 1e-4, 10 ** 7): (base[i].ndim, base[i].cells)
+            for i in sample}
+    table = autotune.tune(tb, info, steps=3, reps=2)
+    tb.close()
+    del tb
+    sweep = []
+    clock = ClockSampler(0)
+    clock.start()
+    for lam in args.rates:
+        jobs = [serve.Job(q.rid, q.arrival / lam, st, q.scheme(), q.nsteps)
+                for q, st in zip(base, states)]
+        srv = serve.Server(pool_bytes=args.hbm_budget, max_slots=1024, chunk=args.chunk,
+                           table=table, keep_results=True, stream=stream.cuda_stream)
+        t0 = time.perf_counter()
+        done = srv.serve(jobs, t0=t0)
+        makespan = time.perf_counter() - t0
+        row = serve.summary(done, srv.depth, makespan)
+        srv.close()
+        del srv
+        row["lambda_per_s"] = lam
+        row["steps_ok"] = all(j.status.steps_done == j.nsteps for j in done)
+        row["err_bits"] = 0
+        for j in done:
+            row["err_bits"] |= j.status.err_bits
+        sweep.append(row)
+    clocks = clock.stop()
+    # headline value: p99 latency at the highest rate of the sweep
+    head = sweep[-1]
+    line = {"metric": "p99 serve latency", "value": head["p99_s"], "unit": "s",
+            "n_gpus": 1, "steps": None, "warmup": None, "ms_per_step": None,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64+f32", "data": "synthetic (seeded serving stream)",
+            "config": {"workload": f"serve_poisson_{nreq}req",
+                       "requests": nreq, "rates_per_s": list(args.rates),
+                       "mix": "2-D/3-D ideal MHD (PLM-MC/HLLD/UCT_HLLD) or HD (PLM-MC/HLLC), "
+                              "cells log-uniform 32^2..128^3, steps log-uniform 50..2000, "
+                              "FP64 or mixed",
+                       "hbm_budget_bytes": args.hbm_budget, "chunk_steps": args.chunk,
+                       "work_zone_updates": work, "tile_table": table,
+                       "launch": "per chunk: CUDA graph of chunk x RK2 steps, 2 persistent "
+                                 "launches per stage over all active requests"},
+            "throughput_Mzone_updates_per_s": head["Mzone_updates_per_s"],
+            "sweep": sweep, "clocks": clocks,
+            "e2e": {"value": head["Mzone_updates_per_s"], "unit": METRIC,
+                    "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                    "path": "request payloads admitted from host arrays, results downloaded to "
+                            "host at completion; latency on the host clock"},
+            "gpu_launches": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mhd3d_blast", choices=["mhd3d_blast", "ensemble"])
+    ap.add_argument("--workload", default="mhd3d_blast",
+                    choices=["mhd3d_blast", "ensemble", "serve"])
+    ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--rates", type=float, nargs="+", default=list(SERVE_RATES))
+    ap.add_argument("--chunk", type=int, default=25)
+    ap.add_argument("--hbm-budget", type=int, default=150 * 10 ** 9)
     ap.add_argument("--n", type=int, default=N)
     ap.add_argument("--grids", type=int, default=512)
     ap.add_argument("--no-mixed", action="store_true")
@@ -674,6 +755,12 @@ def main():
         args.steps = 200 if args.workload == "ensemble" else 100
     if args.workload == "ensemble":
         return impl_reference_ensemble(args) if args.impl == "reference" else impl_ensemble(args)
+    if args.workload == "serve":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving "
+                              "loop; its CPU rate per zone is the ensemble/blast reference arm"}))
+            return 0
+        return impl_serve(args)
     if args.impl == "reference":
         return impl_reference(args)
     return impl_ours(args)
