@@ -233,6 +233,41 @@ def impl_reference(args):
 
 
 
+def mixed_error(make_solver, nsteps, st):
+    """Both forms for nsteps steps on the FP64 run's dt sequence; per
+    conserved variable the relative L1 (sum|d|/sum|fp64|) and L-infinity
+    (max|d|/max|fp64|) error of the mixed form, and its div(B)."""
+    import torch
+    from gpluto_dev_b200 import api
+    a = make_solver(api.FP64)
+    _, hist, _ = a.run(nsteps, FIRST_DT)
+    _, Ua, _ = a.download()
+    a.close()
+    del a
+    torch.cuda.empty_cache()
+    b = make_solver(api.MIXED)
+    for dt in hist:
+        b.AdvanceStep(float(dt))
+    _, Ub, Bb = b.download()
+    b.close()
+    del b
+    torch.cuda.empty_cache()
+    l1, linf = [], []
+    for nv in range(Ua.shape[0]):
+        den = float(np.abs(Ua[nv]).sum())
+        d = np.abs(Ub[nv] - Ua[nv])
+        l1.append(float(d.sum()) / den if den else 0.0)
+        linf.append(float(d.max()) / float(np.abs(Ua[nv]).max()) if den else 0.0)
+    nx, ny, nz = st.shape
+    dx = [1.0 / nx, 1.0 / ny, 1.0 / nz]
+    axes = {0: 2, 1: 1, 2: 0}
+    div = sum((np.roll(Bb[d], -1, axis=axes[d]) - Bb[d]) / dx[d] for d in range(3))
+    bmax = max(float(np.abs(x).max()) for x in Bb)
+    return {"steps": nsteps, "variables": ["rho", "mx", "my", "mz", "Bx", "By", "Bz", "E"],
+            "l1_rel": l1, "linf_rel": linf, "l1_rel_max": max(l1),
+            "divB_rel_max": float(np.abs(div).max()) / (bmax / min(dx))}
+
+
 def measure_e2e(make_solver, ncell, world, steps, barrier, dist):
     """End to end through the C ABI with host buffers.
 
@@ -380,8 +415,14 @@ def impl_ours(args):
         mixed = {"value": world * ncell * args.steps / (tm * 1e-3) / 1e6,
                  "ms_per_step": tm / args.steps}
         mixed["speedup_vs_fp64"] = mixed["value"] / value
+        mprof, _ = smx.profile(3, d2)
+        mixed["kernels"] = [{"kernel": nm, "stage": stg, "ms": ms} for nm, stg, ms in mprof]
         del smx
         torch.cuda.empty_cache()
+
+    # ---- mixed-form error against the FP64 form (the FP64 oracle) --------
+    if mixed is not None:
+        mixed["error_vs_fp64"] = mixed_error(solver, args.error_steps, st)
 
     # ---- end to end through the C ABI with host buffers ------------------
     # Per step: host (pinned) -> device upload of the full reference-layout
@@ -748,6 +789,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--error-steps", type=int, default=100)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -311,15 +311,17 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   alloc((void**)&h->U[0], cell * h->nvar);
   alloc((void**)&h->U[1], cell * h->nvar);
   alloc((void**)&h->V, cell * h->nvar);
-  alloc((void**)&h->dU, cell * h->nvar * 3);
-  alloc((void**)&h->Cdt, cell * 3);
+  // flux differences, inverse-dt terms, UCT data and EMFs: float in the mixed form
+  const size_t fcell = (h->mixed ? sizeof(float) : sizeof(double)) * h->n;
+  alloc((void**)&h->dU, fcell * h->nvar * 3);
+  alloc((void**)&h->Cdt, fcell * 3);
   if (scheme->physics != GP_HD) {
     for (int b = 0; b < 3; b++)
       for (int d = 0; d < h->ndim; d++) alloc((void**)&h->Bs[b][d], cell);
     for (int d = 0; d < h->ndim; d++)
       for (int r = 0; r < 6; r++) alloc(&h->ct[d][r], ctb);
     for (int d = 0; d < 3; d++)
-      if (h->ndim == 3 || d == 2) alloc((void**)&h->Ee[d], cell);
+      if (h->ndim == 3 || d == 2) alloc((void**)&h->Ee[d], fcell);
   }
   alloc((void**)&h->sc, sizeof(StepScalars));
   if (ok && cudaMallocHost((void**)&h->sc_host, sizeof(StepScalars)) != cudaSuccess) ok = false;
@@ -331,8 +333,8 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
     return fail(GP_ERR_NOMEM, "device allocation failed for %lld cells", ncell);
   }
   cudaMemsetAsync(h->sc, 0, sizeof(StepScalars), h->stream);
-  cudaMemsetAsync(h->dU, 0, cell * h->nvar * 3, h->stream);
-  cudaMemsetAsync(h->Cdt, 0, cell * 3, h->stream);
+  cudaMemsetAsync(h->dU, 0, fcell * h->nvar * 3, h->stream);
+  cudaMemsetAsync(h->Cdt, 0, fcell * 3, h->stream);
   h->bcur = 0;
   h->launches_per_step = 2 * gp::stage_launch_count(h->key) + 1;
   *out = h;

@@ -161,7 +161,8 @@ struct SlotLayout {
 };
 
 // Region of one slot: U[2], V, dU, Cdt, Bs[3 buffers][ndim], ct[ndim][6],
-// Ee, scalars.  Every array starts on a 256-byte boundary.
+// Ee, scalars.  Every array starts on a 256-byte boundary; dU, Cdt, ct and
+// Ee hold floats in the mixed form.
 SlotLayout slot_layout(const gp_grid_desc* g, const gp_scheme* sc) {
   SlotLayout L;
   L.ndim = g->ndim;
@@ -171,16 +172,17 @@ SlotLayout slot_layout(const gp_grid_desc* g, const gp_scheme* sc) {
   L.mixed = sc->precision == GP_MIXED;
   L.nvar = L.mhd ? 8 : 5;
   const size_t cell = sizeof(double) * (size_t)L.n;
+  // flux differences, inverse-dt terms, UCT data, EMFs: float in the mixed form
+  const size_t fcell = (L.mixed ? sizeof(float) : sizeof(double)) * (size_t)L.n;
   size_t b = 0;
   b += 2 * align_up(cell * L.nvar);           // U[0], U[1]
   b += align_up(cell * L.nvar);               // V
-  b += align_up(cell * L.nvar * L.ndim);      // dU
-  b += align_up(cell * L.ndim);               // Cdt
+  b += align_up(fcell * L.nvar * L.ndim);     // dU
+  b += align_up(fcell * L.ndim);              // Cdt
   if (L.mhd) {
     b += 3 * L.ndim * align_up(cell);         // face buffers
-    const size_t ctb = (L.mixed ? sizeof(float) : sizeof(double)) * (size_t)L.n;
-    b += L.ndim * 6 * align_up(ctb);          // UCT face data
-    b += (L.ndim == 3 ? 3 : 1) * align_up(cell);  // edge EMFs
+    b += L.ndim * 6 * align_up(fcell);        // UCT face data
+    b += (L.ndim == 3 ? 3 : 1) * align_up(fcell);  // edge EMFs
   }
   b += align_up(sizeof(BatchScalars));
   L.bytes = b;
@@ -492,22 +494,22 @@ int gp_batch_add(gp_batch* b, const gp_grid_desc* grid, const gp_scheme* scheme,
   auto take = [&](size_t bytes) { char* q = p; p += gp::align_up(bytes); return q; };
   const long long n = L.n;
   const size_t cell = sizeof(double) * (size_t)n;
+  const size_t fcell = (L.mixed ? sizeof(float) : sizeof(double)) * (size_t)n;
   double* U0 = (double*)take(cell * L.nvar);
   double* U1 = (double*)take(cell * L.nvar);
   double* V = (double*)take(cell * L.nvar);
-  double* dU = (double*)take(cell * L.nvar * L.ndim);
-  double* Cdt = (double*)take(cell * L.ndim);
+  double* dU = (double*)take(fcell * L.nvar * L.ndim);
+  double* Cdt = (double*)take(fcell * L.ndim);
   double* B[3][3] = {};
   void* ct[3][6] = {};
   double* Ee[3] = {};
   if (mhd) {
     for (int k = 0; k < 3; k++)
       for (int d = 0; d < L.ndim; d++) B[k][d] = (double*)take(cell);
-    const size_t ctb = (L.mixed ? sizeof(float) : sizeof(double)) * (size_t)n;
     for (int d = 0; d < L.ndim; d++)
-      for (int r = 0; r < 6; r++) ct[d][r] = take(ctb);
+      for (int r = 0; r < 6; r++) ct[d][r] = take(fcell);
     for (int d = 0; d < 3; d++)
-      if (L.ndim == 3 || d == 2) Ee[d] = (double*)take(cell);
+      if (L.ndim == 3 || d == 2) Ee[d] = (double*)take(fcell);
   }
   BatchScalars* sc = (BatchScalars*)take(sizeof(BatchScalars));
 
@@ -574,7 +576,7 @@ int gp_batch_add(gp_batch* b, const gp_grid_desc* grid, const gp_scheme* scheme,
     for (int d = 0; d < L.ndim; d++)
       chk(cudaMemcpyAsync(B[0][d], src[d], cell, cudaMemcpyHostToDevice, b->stream), "upload Vs");
   }
-  chk(cudaMemsetAsync(dU, 0, cell * L.nvar * L.ndim, b->stream), "clear dU");
+  chk(cudaMemsetAsync(dU, 0, fcell * L.nvar * L.ndim, b->stream), "clear dU");
   if (rc == GP_OK && gp::launch_prim2cons(scheme->physics, V, U0, n, scheme->gamma, b->stream) != 0)
     rc = gp::fail(GP_ERR_UNSUPPORTED, "start-up map");
   BatchScalars hs;

@@ -55,9 +55,9 @@ struct BatchSlot {
   double cfl, cfl_max_var;
   double dx[3];
   BatchScalars* sc;
-  // StageArgs for [stage-1][bcur]; the face-data pointers are float* in the
-  // mixed form (same layout: every member of StageArgs<double> and
-  // StageArgs<float> has the same size and offset).
+  // StageArgs for [stage-1][bcur]; the dU, Cdt, UCT-data and EMF pointers
+  // are float* in the mixed form (same layout: every member of
+  // StageArgs<double> and StageArgs<float> has the same size and offset).
   StageArgs<double> sa[2][3];
 };
 

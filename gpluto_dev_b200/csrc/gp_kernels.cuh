@@ -38,14 +38,14 @@ struct StageArgs {
   const double* Bs[3];    // stage-input face fields (left faces)
   const double* Bs0[3];   // face fields at t^n (stage 2)
   double* Bsout[3];       // face fields written by this stage
-  double* dU;             // [3][nvar][n] flux difference of each direction
-  double* Cdt;            // [3][n] inverse dt of each direction
+  CTT* dU;                // [3][nvar][n] flux difference of each direction
+  CTT* Cdt;               // [3][n] inverse dt of each direction
   const double* U0;       // U^n
   const double* Uc;       // stage-input U
   double* Uout;           // U written by this stage
   double* Vout;           // primitives written by this stage
   CTT* ct[3][6];          // UCT face data per direction: eb, et, aL, aR, dL, dR
-  double* Ee[3];          // edge EMFs: Ee[0]=Ex(i,j-1/2,k-1/2), Ee[1]=Ey, Ee[2]=Ez
+  CTT* Ee[3];             // edge EMFs: Ee[0]=Ex(i,j-1/2,k-1/2), Ee[1]=Ey, Ee[2]=Ez
   const double* dtdx;     // dt/dx_d (3 values in device memory, set per step)
   double dx[3];
   double gamma, small_rho, small_prs;
@@ -140,13 +140,13 @@ __device__ __forceinline__ void cell_update(const StageArgs<CTT>& a, long long n
                                             long long c, const R* Fl, const R* Fr,
                                             R cml, R cmr, int dir) {
   const double dtdx = a.dtdx[dir];
-  double* du = a.dU + (long long)dir * NV * n;
+  CTT* du = a.dU + (long long)dir * NV * n;
 #pragma unroll
   for (int nv = 0; nv < NV; nv++) {
     if (!rhs_var<PHYS, NDIM>(nv)) continue;
-    du[nv * n + c] = -dtdx * ((double)Fr[nv] - (double)Fl[nv]);
+    du[nv * n + c] = (CTT)(-dtdx * ((double)Fr[nv] - (double)Fl[nv]));
   }
-  a.Cdt[(long long)dir * n + c] = 0.5 * ((double)cml + (double)cmr) / a.dx[dir];
+  a.Cdt[(long long)dir * n + c] = (CTT)(0.5 * ((double)cml + (double)cmr) / a.dx[dir]);
 }
 
 template <typename R, typename CTT>
@@ -486,7 +486,7 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
     face_coef<R>(a, 1, id(i - 1, j, k), c, aL, aR, dL, dR);
     uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
     Ez += avg - phi;
-    a.Ee[2][c] = (double)Ez;
+    a.Ee[2][c] = (CTT)Ez;
   }
   if constexpr (NDIM == 3) {
     // Ey at (i-1/2, j, k-1/2)
@@ -509,7 +509,7 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
       face_coef<R>(a, 2, id(i - 1, j, k), c, aL, aR, dL, dR);
       uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
       Ey += avg + phi;
-      a.Ee[1][c] = (double)Ey;
+      a.Ee[1][c] = (CTT)Ey;
     }
     // Ex at (i, j-1/2, k-1/2)
     {
@@ -531,7 +531,7 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
       face_coef<R>(a, 2, id(i, j - 1, k), c, aL, aR, dL, dR);
       uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
       Ex += avg - phi;
-      a.Ee[0][c] = (double)Ex;
+      a.Ee[0][c] = (CTT)Ex;
     }
   }
 }
@@ -554,16 +554,17 @@ __device__ __forceinline__ double face_rs(const StageArgs<CTT>& a, const Grid3& 
   auto id = [&](int ii, int jj, int kk) -> long long {
     return wrapi(ii, nx) + (long long)nx * (wrapi(jj, ny) + (long long)ny * wrapi(kk, nz));
   };
+  auto E = [&](int q, int ii, int jj, int kk) -> double { return (double)a.Ee[q][id(ii, jj, kk)]; };
   double curlE;
   if (d == 0) {
-    curlE = 0.0 + a.dtdx[1] * (a.Ee[2][id(i, j + 1, k)] - a.Ee[2][id(i, j, k)]);
-    if (NDIM == 3) curlE = curlE - a.dtdx[2] * (a.Ee[1][id(i, j, k + 1)] - a.Ee[1][id(i, j, k)]);
+    curlE = 0.0 + a.dtdx[1] * (E(2, i, j + 1, k) - E(2, i, j, k));
+    if (NDIM == 3) curlE = curlE - a.dtdx[2] * (E(1, i, j, k + 1) - E(1, i, j, k));
   } else if (d == 1) {
-    curlE = -a.dtdx[0] * (a.Ee[2][id(i + 1, j, k)] - a.Ee[2][id(i, j, k)]);
-    if (NDIM == 3) curlE = curlE + a.dtdx[2] * (a.Ee[0][id(i, j, k + 1)] - a.Ee[0][id(i, j, k)]);
+    curlE = -a.dtdx[0] * (E(2, i + 1, j, k) - E(2, i, j, k));
+    if (NDIM == 3) curlE = curlE + a.dtdx[2] * (E(0, i, j, k + 1) - E(0, i, j, k));
   } else {
-    curlE = a.dtdx[0] * (a.Ee[1][id(i + 1, j, k)] - a.Ee[1][id(i, j, k)]) -
-            a.dtdx[1] * (a.Ee[0][id(i, j + 1, k)] - a.Ee[0][id(i, j, k)]);
+    curlE = a.dtdx[0] * (E(1, i + 1, j, k) - E(1, i, j, k)) -
+            a.dtdx[1] * (E(0, i, j + 1, k) - E(0, i, j, k));
   }
   return -curlE;
 }
@@ -589,14 +590,14 @@ __device__ __forceinline__ double finish_cell(const StageArgs<CTT>& a, const Gri
 #pragma unroll
     for (int nv = 0; nv < NV; nv++) {
       if (!rhs_var<PHYS, NDIM>(nv)) continue;
-      double Rc = a.dU[nv * n + c] + a.dU[(NV + nv) * n + c];
-      if (NDIM == 3) Rc = Rc + a.dU[(2 * NV + nv) * n + c];
+      double Rc = (double)a.dU[nv * n + c] + (double)a.dU[(NV + nv) * n + c];
+      if (NDIM == 3) Rc = Rc + (double)a.dU[(2 * NV + nv) * n + c];
       const double u0 = a.U0[nv * n + c];
       if (a.stage == 1) u[nv] = u0 + Rc;
       else u[nv] = 0.5 * u0 + 0.5 * a.Uc[nv * n + c] + 0.5 * Rc;
     }
-    cdt = a.Cdt[c] + a.Cdt[n + c];
-    if (NDIM == 3) cdt = cdt + a.Cdt[2 * n + c];
+    cdt = (double)a.Cdt[c] + (double)a.Cdt[n + c];
+    if (NDIM == 3) cdt = cdt + (double)a.Cdt[2 * n + c];
     if constexpr (PHYS != PHYS_HD) {
       const int nx = g.nx, ny = g.ny, nz = g.nz;
       const int i = (int)(c % nx);

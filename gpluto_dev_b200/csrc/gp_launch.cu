@@ -3,7 +3,10 @@
 // Compiled twice: with GP_MIXED=0 (FP64 everywhere, -fmad=false so that the
 // plain form keeps the reference's rounding sequence) and GP_MIXED=1 (FP32
 // reconstruction/limiter/Riemann/EMF arithmetic, FP64 accumulation, CT
-// update and con2prim).
+// update and con2prim).  In the mixed form the per-direction flux
+// differences, inverse-dt terms, UCT face data and edge EMFs -- all computed
+// from FP32 fluxes -- are stored as float (the StageDesc pointers then point
+// at float arrays); the FP64 form stores them as double.
 #include "gp_kernels.cuh"
 #include "gp_launch.h"
 
@@ -30,13 +33,13 @@ static StageArgs<CTT> make_args(const StageDesc& d) {
     a.Bs[q] = d.Bs[q];
     a.Bs0[q] = d.Bs0[q];
     a.Bsout[q] = d.Bsout[q];
-    a.Ee[q] = d.Ee[q];
+    a.Ee[q] = reinterpret_cast<CTT*>(d.Ee[q]);
     a.dx[q] = d.dx[q];
     for (int r = 0; r < 6; r++) a.ct[q][r] = static_cast<CTT*>(d.ct[q][r]);
   }
   a.dtdx = d.dtdx;
-  a.dU = d.dU;
-  a.Cdt = d.Cdt;
+  a.dU = reinterpret_cast<CTT*>(d.dU);
+  a.Cdt = reinterpret_cast<CTT*>(d.Cdt);
   a.U0 = d.U0;
   a.Uc = d.Uc;
   a.Uout = d.Uout;

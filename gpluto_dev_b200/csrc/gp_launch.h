@@ -12,14 +12,14 @@ struct StageDesc {
   const double* Bs[3];
   const double* Bs0[3];
   double* Bsout[3];
-  double* dU;
+  double* dU;          // float arrays in the mixed form (see gp_launch.cu)
   double* Cdt;
   const double* U0;
   const double* Uc;
   double* Uout;
   double* Vout;
   void* ct[3][6];      // double (FP64 form) or float (mixed form)
-  double* Ee[3];
+  double* Ee[3];       // float arrays in the mixed form
   const double* dtdx;  // device pointer to dt/dx_d
   double dx[3];
   double gamma, small_rho, small_prs;

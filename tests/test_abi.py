@@ -66,8 +66,8 @@ def test_no_cpu_fallback_without_device():
 
 def test_batch_slot_bytes_formula():
     """Pool bytes of one slot: U (2 copies), V, per-direction dU and C_dt,
-    3 face buffers, 6 UCT arrays per direction (float in the mixed form) and
-    the edge EMFs, each array rounded up to 256 bytes, plus the scalars."""
+    3 face buffers, 6 UCT arrays per direction and the edge EMFs, each array
+    rounded up to 256 bytes, plus the scalars."""
     from gpluto_dev_b200 import batch as gb, ics
     al = lambda x: (x + 255) // 256 * 256
     st = ics.mhd2d_turbulence(n=(64, 48), seed=1)
@@ -76,7 +76,9 @@ def test_batch_slot_bytes_formula():
     exp = 2 * al(8 * c) + al(8 * c) + al(16 * c) + al(2 * c) + 6 * al(c) + 12 * al(c) + al(c) + 256
     assert gb.slot_bytes(st, api.Scheme()) == exp
     mixed = gb.slot_bytes(st, api.Scheme(precision=api.MIXED))
-    assert exp - mixed == 12 * (al(c) - al(4 * n))
+    f = 4 * n    # dU, C_dt, UCT data and EMFs are float in the mixed form
+    assert mixed == (2 * al(8 * c) + al(8 * c) + al(16 * f) + al(2 * f) + 6 * al(c)
+                     + 12 * al(f) + al(f) + 256)
     sh = ics.hd_turbulence(n=(20, 16, 12), seed=1)
     n = 20 * 16 * 12
     c = 8 * n
