@@ -282,6 +282,10 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   h->ny = grid->nint[1];
   h->nz = grid->ndim == 3 ? grid->nint[2] : 1;
   h->n = (long long)h->nx * h->ny * h->nz;
+  if (h->n >= (1LL << 31)) {
+    delete h;
+    return fail(GP_ERR_UNSUPPORTED, "grids are limited to fewer than 2^31 cells");
+  }
   h->nvar = scheme->physics == GP_HD ? 5 : 8;
   h->ng = grid->nghost;
   for (int d = 0; d < 3; d++) {

@@ -485,6 +485,7 @@ int gp_batch_add(gp_batch* b, const gp_grid_desc* grid, const gp_scheme* scheme,
     if (!b->used[i]) { idx = i; break; }
   if (idx < 0) return gp::fail(GP_ERR_NOMEM, "slot table full (%d slots)", b->max_slots);
   const gp::SlotLayout L = gp::slot_layout(grid, scheme);
+  if (L.n >= (1LL << 31)) return gp::fail(GP_ERR_UNSUPPORTED, "grids are limited to fewer than 2^31 cells");
   size_t off = 0;
   if (!pool_alloc(b, L.bytes, &off))
     return gp::fail(GP_ERR_NOMEM, "pool full: %zu bytes requested, %zu of %zu in use", L.bytes,

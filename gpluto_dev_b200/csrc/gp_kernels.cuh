@@ -455,35 +455,44 @@ __device__ __forceinline__ void face_coef(const StageArgs<CTT>& a, int d, long l
 }
 
 // The edge EMFs whose lower corner is cell c (all three in 3-D, Ez in 2-D).
+// The wrapped offsets of the stencil rows (index - 2 .. index + 1 along each
+// direction) are formed once; every operand address is then a sum of three.
+// Offsets are 32-bit: grids are limited to fewer than 2^31 cells.
 template <int NDIM, int LIM, typename R, typename CTT>
 __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g, long long c) {
   if (c >= g.n) return;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const int i = (int)(c % nx);
-  const int j = (int)((c / nx) % ny);
-  const int k = (int)(c / ((long long)nx * ny));
-  auto id = [&](int ii, int jj, int kk) -> long long {
-    return wrapi(ii, nx) + (long long)nx * (wrapi(jj, ny) + (long long)ny * wrapi(kk, nz));
-  };
+  const int nxy = nx * ny;
+  const int ci = (int)c;
+  const int i = ci % nx;
+  const int j = (ci / nx) % ny;
+  const int k = ci / nxy;
+  int X[4], Y[4], Z[4];
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    X[m] = wrapi(i - 2 + m, nx);
+    Y[m] = nx * wrapi(j - 2 + m, ny);
+    Z[m] = NDIM == 3 ? nxy * wrapi(k - 2 + m, nz) : 0;
+  }
   R b[4], q[4], aL, aR, dL, dR, avg, phi;
   // Ez at (i-1/2, j-1/2, k)
   {
 #pragma unroll
     for (int m = 0; m < 4; m++) {
-      long long e = id(i - 2 + m, j, k);
+      const int e = X[m] + Y[2] + Z[2];
       b[m] = (R)a.Bs[1][e];
       q[m] = (R)a.ct[1][1][e];
     }
-    face_coef<R>(a, 0, id(i, j - 1, k), c, aL, aR, dL, dR);
+    face_coef<R>(a, 0, X[2] + Y[1] + Z[2], c, aL, aR, dL, dR);
     uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
     R Ez = avg + phi;
 #pragma unroll
     for (int m = 0; m < 4; m++) {
-      long long e = id(i, j - 2 + m, k);
+      const int e = X[2] + Y[m] + Z[2];
       b[m] = (R)a.Bs[0][e];
       q[m] = (R)a.ct[0][0][e];
     }
-    face_coef<R>(a, 1, id(i - 1, j, k), c, aL, aR, dL, dR);
+    face_coef<R>(a, 1, X[1] + Y[2] + Z[2], c, aL, aR, dL, dR);
     uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
     Ez += avg - phi;
     a.Ee[2][c] = (CTT)Ez;
@@ -493,20 +502,20 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
     {
 #pragma unroll
       for (int m = 0; m < 4; m++) {
-        long long e = id(i - 2 + m, j, k);
+        const int e = X[m] + Y[2] + Z[2];
         b[m] = (R)a.Bs[2][e];
         q[m] = (R)a.ct[2][0][e];
       }
-      face_coef<R>(a, 0, id(i, j, k - 1), c, aL, aR, dL, dR);
+      face_coef<R>(a, 0, X[2] + Y[2] + Z[1], c, aL, aR, dL, dR);
       uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
       R Ey = avg - phi;
 #pragma unroll
       for (int m = 0; m < 4; m++) {
-        long long e = id(i, j, k - 2 + m);
+        const int e = X[2] + Y[2] + Z[m];
         b[m] = (R)a.Bs[0][e];
         q[m] = (R)a.ct[0][1][e];
       }
-      face_coef<R>(a, 2, id(i - 1, j, k), c, aL, aR, dL, dR);
+      face_coef<R>(a, 2, X[1] + Y[2] + Z[2], c, aL, aR, dL, dR);
       uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
       Ey += avg + phi;
       a.Ee[1][c] = (CTT)Ey;
@@ -515,20 +524,20 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
     {
 #pragma unroll
       for (int m = 0; m < 4; m++) {
-        long long e = id(i, j - 2 + m, k);
+        const int e = X[2] + Y[m] + Z[2];
         b[m] = (R)a.Bs[2][e];
         q[m] = (R)a.ct[2][1][e];
       }
-      face_coef<R>(a, 1, id(i, j, k - 1), c, aL, aR, dL, dR);
+      face_coef<R>(a, 1, X[2] + Y[2] + Z[1], c, aL, aR, dL, dR);
       uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
       R Ex = avg + phi;
 #pragma unroll
       for (int m = 0; m < 4; m++) {
-        long long e = id(i, j, k - 2 + m);
+        const int e = X[2] + Y[2] + Z[m];
         b[m] = (R)a.Bs[1][e];
         q[m] = (R)a.ct[1][0][e];
       }
-      face_coef<R>(a, 2, id(i, j - 1, k), c, aL, aR, dL, dR);
+      face_coef<R>(a, 2, X[2] + Y[1] + Z[2], c, aL, aR, dL, dR);
       uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
       Ex += avg - phi;
       a.Ee[0][c] = (CTT)Ex;
@@ -537,7 +546,7 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
 }
 
 template <int NDIM, int LIM, typename R, typename CTT>
-__global__ void __launch_bounds__(256) emf_kernel(StageArgs<CTT> a, Grid3 g) {
+__global__ void __launch_bounds__(256, 4) emf_kernel(StageArgs<CTT> a, Grid3 g) {
   emf_cell<NDIM, LIM, R, CTT>(a, g, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
