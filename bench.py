@@ -578,14 +578,18 @@ def impl_ensemble(args):
     pool = sum(gb.slot_bytes(m.state, m.scheme) for m in members) + (64 << 20)
 
     # ---- autotune tile shapes per size bin on a sample (every 4th grid) ----
-    sample = members[::4]
-    tb = gb.Batch(sum(gb.slot_bytes(m.state, m.scheme) for m in sample) + (64 << 20),
-                  len(sample), stream=stream.cuda_stream)
-    info = {tb.add(m.state, m.scheme, FIRST_DT, 10 ** 7): (2, m.state.ncells) for m in sample}
     trials = []
-    table = autotune.tune(tb, info, steps=3, reps=2, log=trials)
-    tb.close()
-    del tb
+    if args.no_tune:
+        table = autotune.default_table()
+    else:
+        sample = members[::4]
+        tb = gb.Batch(sum(gb.slot_bytes(m.state, m.scheme) for m in sample) + (64 << 20),
+                      len(sample), stream=stream.cuda_stream)
+        info = {tb.add(m.state, m.scheme, FIRST_DT, 10 ** 7): (2, m.state.ncells)
+                for m in sample}
+        table = autotune.tune(tb, info, steps=3, reps=2, log=trials)
+        tb.close()
+        del tb
 
     # ---- the run: all grids, warm-up then K timed steps -----------------
     b = gb.Batch(pool, len(members), stream=stream.cuda_stream)
@@ -697,6 +701,158 @@ def impl_reference_ensemble(args):
 
 
 # --------------------------------------------------------------------------
+# special-relativistic MHD 192^3: both forms, and the mixed form's error
+# --------------------------------------------------------------------------
+RMHD_N = 192
+RMHD_ALG_BYTES_ZONE = 696   # 440 + 4 x 64: the stored primitives read and written per stage
+REF_BINARY_RMHD = os.path.join(ROOT, "oracle", "_ref", "rmhd3d_mc_lim_hlld_uct_hll", "pluto")
+
+
+def impl_rmhd(args):
+    import torch
+    from gpluto_dev_b200 import api, ics
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    n = args.n if args.n != N else RMHD_N
+    st = ics.rmhd3d_turbulence(n=(n, n, n), seed=1)
+    ncell = n ** 3
+
+    def solver(precision):
+        sch = api.Scheme(physics=api.RMHD, limiter="mc", riemann="hlld", ct_emf="uct_hll",
+                         precision=precision, gamma=st.gamma, cfl=0.3)
+        return api.Solver.from_state(st, sch)
+
+    forms = {}
+    clock = ClockSampler(0)
+    clocks = None
+    for prec, name in ((api.FP64, "fp64"), (api.MIXED, "mixed")):
+        s = solver(prec)
+        dt, _, _ = s.run(args.warmup, 1e-4, history=False)
+        torch.cuda.synchronize()
+        if name == "fp64":
+            clock.start()
+            time.sleep(0.25)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, _, out = s.run(args.steps, dt, history=False)
+        e1.record()
+        torch.cuda.synchronize()
+        if name == "fp64":
+            clocks = clock.stop()
+        ms = e0.elapsed_time(e1) / args.steps
+        prof, _ = s.profile(2, dt)
+        forms[name] = {"value": ncell / ms / 1e3, "ms_per_step": ms, "err_bits": out.err_bits,
+                       "kernels": [{"kernel": k, "stage": g, "ms": t} for k, g, t in prof]}
+        s.close()
+        del s
+        torch.cuda.empty_cache()
+    forms["mixed"]["speedup_vs_fp64"] = forms["mixed"]["value"] / forms["fp64"]["value"]
+    # error of the mixed form against FP64 after 100 steps on FP64's dt sequence
+    a = solver(api.FP64)
+    _, hist, _ = a.run(args.error_steps, 1e-4)
+    Va, Ua, _ = a.download()
+    a.close()
+    del a
+    torch.cuda.empty_cache()
+    b = solver(api.MIXED)
+    for dt in hist:
+        b.AdvanceStep(float(dt))
+    Vb, Ub, _ = b.download()
+    b.close()
+    l1 = [float(np.abs(Ub[v] - Ua[v]).sum() / np.abs(Ua[v]).sum()) for v in range(8)]
+    linf = [float(np.abs(Ub[v] - Ua[v]).max() / np.abs(Ua[v]).max()) for v in range(8)]
+    forms["mixed"]["error_vs_fp64"] = {"steps": args.error_steps, "l1_rel": l1, "linf_rel": linf,
+                                       "variables": ["D", "mx", "my", "mz", "Bx", "By", "Bz",
+                                                     "E-D"]}
+    value = forms["fp64"]["value"]
+    peak, peak_kind = peaks()
+    achieved = RMHD_ALG_BYTES_ZONE * ncell / (forms["fp64"]["ms_per_step"] * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu and os.path.exists(REF_BINARY_RMHD):
+        m = 32
+        states = [ics.rmhd3d_turbulence(n=(m, m, m), seed=1 + r)
+                  for r in range(max(1, min(os.cpu_count() or 1, 16)))]
+        v, _ = run_reference_grids_rmhd(states, 2, 1)
+        cpu = {"value": v, "unit": METRIC, "cores": len(states), "kind": "reference",
+               "sample": f"{len(states)} concurrent single-thread processes, each a {m}^3 "
+                         f"grid of the same RMHD scheme, 2 timed RK2 steps after 1 warm-up"}
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": forms["fp64"]["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded 3-D RMHD turbulence)",
+            "config": {"workload": f"3d_rmhd_{n}^3", "grid": [n, n, n],
+                       "scheme": "PLM-MC + RMHD HLLD + UCT_HLL + RK2, CFL 0.3, gamma 4/3",
+                       "ic": "rho = 1 + 0.5 f, p = 0.1, Lorentz factor log-uniform [1, 10] "
+                             "along one seeded bulk direction, sigma = 1",
+                       "l2": "inputs larger than L2, no flush", "parallelism": "replicas x1"},
+            "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "alg_bytes_per_zone_update": RMHD_ALG_BYTES_ZONE},
+            "forms": forms, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": args.steps * 11, "e2e": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def impl_reference_rmhd(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    from gpluto_dev_b200 import ics
+    if not os.path.exists(REF_BINARY_RMHD):
+        print(json.dumps({"impl": "reference", "unavailable": "reference RMHD binary not built "
+                          "(oracle/_ref/rmhd3d_mc_lim_hlld_uct_hll)"}))
+        return 0
+    m = 32
+    nproc = max(1, min(os.cpu_count() or 1, 64))
+    states = [ics.rmhd3d_turbulence(n=(m, m, m), seed=1 + r) for r in range(nproc)]
+    v, _ = run_reference_grids_rmhd(states, 2, 1)
+    cpu = {"value": v, "unit": METRIC, "cores": nproc, "kind": "reference",
+           "sample": f"{nproc} concurrent single-thread processes, each a {m}^3 grid of the "
+                     f"same RMHD scheme, 2 timed RK2 steps after 1 warm-up"}
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC,
+                      "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                      "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": f"3d_rmhd_{RMHD_N}^3"}, "cpu_baseline": cpu,
+                      "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}), flush=True)
+    return 0
+
+
+def run_reference_grids_rmhd(states, nsteps_timed, nwarm):
+    sys.path.insert(0, os.path.join(ROOT, "oracle", "ref"))
+    from gpluto_dev_b200 import ics
+    import build_ref as br
+    total = nwarm + nsteps_timed
+    with tempfile.TemporaryDirectory() as tmp:
+        procs = []
+        for r, st in enumerate(states):
+            d = os.path.join(tmp, f"p{r}")
+            os.makedirs(d)
+            cfg = br.RefConfig(name="bench", physics="RMHD", ndim=3, n=st.shape,
+                               limiter="MC_LIM", solver="hlld", ct_emf="UCT_HLL", cfl=0.3,
+                               first_dt=1e-4)
+            open(os.path.join(d, "pluto.ini"), "w").write(cfg.ini())
+            icp = os.path.join(d, "ic.bin")
+            ics.write_ic(icp, st)
+            env = dict(os.environ, GPLUTO_FTZ_DAZ="0", GP_IC_FILE=icp,
+                       GP_DUMP_STEP=str(total + 1), GP_DUMP_FILE=os.path.join(d, "out.dump"))
+            procs.append((d, st, subprocess.Popen([REF_BINARY_RMHD, "-no-write", "-maxsteps",
+                                                   str(total + 1)], cwd=d, env=env,
+                                                  stdout=subprocess.DEVNULL,
+                                                  stderr=subprocess.DEVNULL)))
+        rate = 0.0
+        for d, st, p in procs:
+            p.wait()
+            w = br.read_dump(os.path.join(d, "out.dump")).wall
+            rate += st.ncells / ((w[nwarm + nsteps_timed] - w[nwarm]) / nsteps_timed)
+    return rate / 1e6, None
+
+
+# --------------------------------------------------------------------------
 # serving: Poisson arrivals, continuous batching, p50/p99 latency vs rate
 # --------------------------------------------------------------------------
 SERVE_RATES = (2.0, 4.0, 8.0, 16.0)
@@ -779,7 +935,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mhd3d_blast",
-                    choices=["mhd3d_blast", "ensemble", "serve"])
+                    choices=["mhd3d_blast", "ensemble", "serve", "rmhd"])
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--rates", type=float, nargs="+", default=list(SERVE_RATES))
     ap.add_argument("--chunk", type=int, default=25)
@@ -790,6 +946,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--error-steps", type=int, default=100)
+    ap.add_argument("--no-tune", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -797,6 +954,10 @@ def main():
         args.steps = 200 if args.workload == "ensemble" else 100
     if args.workload == "ensemble":
         return impl_reference_ensemble(args) if args.impl == "reference" else impl_ensemble(args)
+    if args.workload == "rmhd":
+        if args.impl == "reference":
+            return impl_reference_rmhd(args)
+        return impl_rmhd(args)
     if args.workload == "serve":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving "

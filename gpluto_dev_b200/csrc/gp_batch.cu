@@ -310,9 +310,9 @@ void tile_counts(BatchSlot& s) {
 }
 
 // Phase-ordered tile table: all sweeps (the sweep launch), then all EMF
-// tiles, then all finish tiles (the cell launch); within a group, slots from
-// the largest grid down, so that the EMF tiles of the largest (longest)
-// grids complete first.
+// tiles, then all finish tiles (the cell launch); slots from the largest
+// grid down, so that the EMF tiles of the largest (longest) grids complete
+// first.
 int rebuild_tiles(gp_batch* b) {
   std::vector<int> order;
   for (int i = 0; i < b->max_slots; i++)
@@ -320,19 +320,26 @@ int rebuild_tiles(gp_batch* b) {
   std::stable_sort(order.begin(), order.end(),
                    [&](int x, int y) { return b->slots[x].n > b->slots[y].n; });
   std::vector<BatchTile> t;
-  const int groups[3][3] = {{gp::BP_SWEEP_X, gp::BP_SWEEP_Y, gp::BP_SWEEP_Z},
-                            {gp::BP_EMF, -1, -1},
-                            {gp::BP_FINISH, -1, -1}};
-  int nsweep = 0;
-  for (int gi = 0; gi < 3; gi++) {
-    for (int sidx : order)
-      for (int q = 0; q < 3; q++) {
-        const int ph = groups[gi][q];
-        if (ph < 0) continue;
-        for (int k = 0; k < b->slots[sidx].ntiles[ph]; k++) t.push_back(BatchTile{sidx, ph, k, 0});
-      }
-    if (gi == 0) nsweep = (int)t.size();
+  // Sweep tiles: grouped by code path -- (precision, physics, dimensions,
+  // direction) -- so that the blocks running at one time mostly execute the
+  // same instructions; EMF and finish tiles: slot by slot.
+  std::vector<std::pair<long long, BatchTile>> sw;
+  for (int sidx : order) {
+    const BatchSlot& s = b->slots[sidx];
+    for (int ph = gp::BP_SWEEP_X; ph <= gp::BP_SWEEP_Z; ph++) {
+      const long long key = ((long long)s.precision * 4 + s.physics) * 8 + s.ndim * 2 + 0;
+      for (int k = 0; k < s.ntiles[ph]; k++)
+        sw.push_back({key * 8 + ph, BatchTile{sidx, ph, k, 0}});
+    }
   }
+  std::stable_sort(sw.begin(), sw.end(),
+                   [](const std::pair<long long, BatchTile>& x,
+                      const std::pair<long long, BatchTile>& y) { return x.first < y.first; });
+  for (auto& e : sw) t.push_back(e.second);
+  const int nsweep = (int)t.size();
+  for (int ph : {gp::BP_EMF, gp::BP_FINISH})
+    for (int sidx : order)
+      for (int k = 0; k < b->slots[sidx].ntiles[ph]; k++) t.push_back(BatchTile{sidx, ph, k, 0});
   const int nt = (int)t.size();
   if (nt > b->tiles_cap) {
     // captured graphs hold the old table's address: drop them

@@ -56,43 +56,64 @@ __device__ __forceinline__ void sweep_m_item(const StageArgs<CTT>& a, const Grid
   sweep_m_col<PHYS, NV, NDIM, RS, CT, LIM, DIR, RT, CTT>(a, g, i, t, seg, S, smem, tid);
 }
 
+// One non-inlined function per (scheme, phase): each gets its own register
+// allocation, as the single-grid kernels do, instead of one allocation over
+// the union of every phase of every scheme.
+template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM>
+__device__ __noinline__ void tile_sweep_x(const StageArgs<CTT>& a, Grid3 g, int idx,
+                                          double* smem) {
+  const int tid = threadIdx.x;
+  sweep_x_row<PHYS, NV, NDIM, RS, CT, LIM, RT, CTT>(a, g, idx * BATCH_ROWS_PER_TILE + (tid >> 5),
+                                                    smem, tid);
+}
+
+template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, int DIR>
+__device__ __noinline__ void tile_sweep_m(const StageArgs<CTT>& a, Grid3 g, int seg, int idx,
+                                          double* smem) {
+  const int tid = threadIdx.x;
+  sweep_m_item<PHYS, NV, NDIM, RS, CT, LIM, DIR>(a, g, seg, (long long)idx * BATCH_THREADS + tid,
+                                                 smem, tid);
+}
+
+template <int NDIM, int LIM>
+__device__ __noinline__ void tile_emf(const StageArgs<CTT>& a, Grid3 g, int cpt, int idx) {
+  const long long c0 = (long long)idx * BATCH_THREADS * cpt + threadIdx.x;
+  for (int q = 0; q < cpt; q++) emf_cell<NDIM, LIM, RT, CTT>(a, g, c0 + (long long)q * BATCH_THREADS);
+}
+
+template <int PHYS, int NV, int NDIM>
+__device__ __noinline__ void tile_finish(const StageArgs<CTT>& a, Grid3 g, int cpt, int idx,
+                                         int stage) {
+  const long long c0 = (long long)idx * BATCH_THREADS * cpt + threadIdx.x;
+  double mx = 0.0;
+  for (int q = 0; q < cpt; q++) {
+    const double cdt = finish_cell<PHYS, NV, NDIM, CTT>(a, g, c0 + (long long)q * BATCH_THREADS);
+    mx = GP_MAX(mx, cdt);
+  }
+  if (stage == 1) warp_invdt_max(a.invdt_bits, mx, threadIdx.x & 31);
+}
+
 template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM>
 __device__ __forceinline__ void run_tile(const StageArgs<CTT>& a, const Grid3& g, int seg,
                                          int cpt, int phase, int idx, int stage, double* smem) {
-  const int tid = threadIdx.x;
   switch (phase) {
 #if GP_BATCH_PART == 0
     case BP_SWEEP_X:
-      sweep_x_row<PHYS, NV, NDIM, RS, CT, LIM, RT, CTT>(
-          a, g, idx * BATCH_ROWS_PER_TILE + (tid >> 5), smem, tid);
+      tile_sweep_x<PHYS, NV, NDIM, RS, CT, LIM>(a, g, idx, smem);
       break;
     case BP_SWEEP_Y:
-      sweep_m_item<PHYS, NV, NDIM, RS, CT, LIM, 1>(a, g, seg,
-                                                   (long long)idx * BATCH_THREADS + tid, smem, tid);
+      tile_sweep_m<PHYS, NV, NDIM, RS, CT, LIM, 1>(a, g, seg, idx, smem);
       break;
     case BP_SWEEP_Z:
-      if constexpr (NDIM == 3)
-        sweep_m_item<PHYS, NV, NDIM, RS, CT, LIM, 2>(
-            a, g, seg, (long long)idx * BATCH_THREADS + tid, smem, tid);
+      if constexpr (NDIM == 3) tile_sweep_m<PHYS, NV, NDIM, RS, CT, LIM, 2>(a, g, seg, idx, smem);
       break;
 #else
     case BP_EMF:
-      if constexpr (PHYS != PHYS_HD) {
-        const long long c0 = (long long)idx * BATCH_THREADS * cpt + tid;
-        for (int q = 0; q < cpt; q++)
-          emf_cell<NDIM, LIM, RT, CTT>(a, g, c0 + (long long)q * BATCH_THREADS);
-      }
+      if constexpr (PHYS != PHYS_HD) tile_emf<NDIM, LIM>(a, g, cpt, idx);
       break;
-    case BP_FINISH: {
-      const long long c0 = (long long)idx * BATCH_THREADS * cpt + tid;
-      double mx = 0.0;
-      for (int q = 0; q < cpt; q++) {
-        const double cdt = finish_cell<PHYS, NV, NDIM, CTT>(a, g, c0 + (long long)q * BATCH_THREADS);
-        mx = GP_MAX(mx, cdt);
-      }
-      if (stage == 1) warp_invdt_max(a.invdt_bits, mx, tid & 31);
+    case BP_FINISH:
+      tile_finish<PHYS, NV, NDIM>(a, g, cpt, idx, stage);
       break;
-    }
 #endif
     default:
       break;
