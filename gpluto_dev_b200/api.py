@@ -25,7 +25,8 @@ LIB_PATH = os.environ.get("GPLUTO_B200_LIB") or os.path.join(_HERE, "_build",
 
 GP_OK, GP_ERR_INVALID, GP_ERR_QUIT, GP_ERR_NO_DEVICE = 0, -1, -5, -6
 HD, MHD, RMHD = 0, 1, 2
-LIMITERS = {"flat": 0, "minmod": 1, "vl": 2, "vanleer": 2, "mc": 3}
+# "ppm" selects RECONSTRUCTION PARABOLIC (the limiter then plays no part)
+LIMITERS = {"flat": 0, "minmod": 1, "vl": 2, "vanleer": 2, "mc": 3, "ppm": 3}
 SOLVERS = {"hll": 0, "hllc": 1, "hlld": 2}
 CT_AVG = {"uct_hll": 0, "uct_hlld": 1}
 FP64, MIXED = 0, 1
@@ -45,7 +46,7 @@ class GpScheme(ctypes.Structure):
                 ("ct_emf", ctypes.c_int), ("rk_stages", ctypes.c_int), ("precision", ctypes.c_int),
                 ("gamma", ctypes.c_double), ("cfl", ctypes.c_double),
                 ("cfl_max_var", ctypes.c_double), ("small_rho", ctypes.c_double),
-                ("small_prs", ctypes.c_double)]
+                ("small_prs", ctypes.c_double), ("reconstruction", ctypes.c_int)]
 
 
 class GpStepOut(ctypes.Structure):
@@ -127,6 +128,7 @@ class Scheme:
         s = GpScheme()
         s.physics = self.physics
         s.limiter = LIMITERS[self.limiter]
+        s.reconstruction = 1 if self.limiter == "ppm" else 0
         s.riemann = SOLVERS[self.riemann]
         s.ct_emf = CT_AVG[self.ct_emf]
         s.rk_stages = 2

@@ -268,8 +268,15 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
     return fail(GP_ERR_UNSUPPORTED, "MHD HLLC not built");
   if (scheme->physics == GP_HD && scheme->riemann == GP_RS_HLLD)
     return fail(GP_ERR_UNSUPPORTED, "HD has no HLLD solver");
-  if (scheme->limiter < GP_LIM_MINMOD || scheme->limiter > GP_LIM_MC)
+  if (scheme->reconstruction != GP_REC_LINEAR && scheme->reconstruction != GP_REC_PARABOLIC)
+    return fail(GP_ERR_UNSUPPORTED, "reconstruction %d not built", scheme->reconstruction);
+  if (scheme->reconstruction == GP_REC_LINEAR &&
+      (scheme->limiter < GP_LIM_MINMOD || scheme->limiter > GP_LIM_MC))
     return fail(GP_ERR_UNSUPPORTED, "limiter %d not built", scheme->limiter);
+  if (scheme->reconstruction == GP_REC_PARABOLIC)
+    for (int d = 0; d < grid->ndim; d++)
+      if (grid->nint[d] < 4)
+        return fail(GP_ERR_INVALID, "PPM needs at least 4 cells along each direction");
   int rc = check_device();
   if (rc) return rc;
   gp_handle* h = new (std::nothrow) gp_handle;
@@ -297,7 +304,8 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   h->stream = (cudaStream_t)stream;
   h->mixed = scheme->precision == GP_MIXED;
   h->key = gp::SchemeKey{scheme->physics, grid->ndim, scheme->riemann, scheme->ct_emf,
-                         scheme->limiter};
+                         scheme->reconstruction == GP_REC_PARABOLIC ? 4 /* LIM_PPM */
+                                                                    : scheme->limiter};
   // pencil segment for the marching sweeps: enough threads to fill 148 SMs
   {
     long long cols = (long long)h->nx * (h->ndim == 3 ? h->nz : 1);

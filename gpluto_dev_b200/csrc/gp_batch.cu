@@ -191,7 +191,7 @@ SlotLayout slot_layout(const gp_grid_desc* g, const gp_scheme* sc) {
 
 bool scheme_built(const gp_scheme* sc) {
   if (sc->rk_stages != 2) return false;
-  if (sc->limiter != GP_LIM_MC) return false;
+  if (sc->limiter != GP_LIM_MC || sc->reconstruction != GP_REC_LINEAR) return false;
   if (sc->precision != GP_FP64 && sc->precision != GP_MIXED) return false;
   if (sc->physics == GP_MHD) return sc->riemann == GP_RS_HLLD && sc->ct_emf == GP_CT_UCT_HLLD;
   if (sc->physics == GP_HD) return sc->riemann == GP_RS_HLLC;

@@ -165,11 +165,171 @@ __device__ __forceinline__ void store_ct(const StageArgs<CTT>& a, int dir, long 
 // Face f (between cells f-1 and f) is computed by lane f%32; the lane then
 // updates cell f-1.  The first face's flux is kept for cell nx-1.
 // ---------------------------------------------------------------------
-// Staging area of one 128-thread block: [2 buffers][SL values][128 threads].
-template <int NV>
-constexpr int sweep_x_stage_doubles() { return 2 * (2 * NV + 1) * SWEEP_THREADS; }
+// Staging area of one 128-thread block: [2 buffers][SL values][128 threads]
+// (+ [2 buffers][4 warps][NV] for the second-next cell with PPM).
+template <int NV, int LIM = LIM_MC>
+constexpr int sweep_x_stage_doubles() {
+  return 2 * (2 * NV + 1) * SWEEP_THREADS + (LIM == LIM_PPM ? 2 * (SWEEP_THREADS / 32) * NV : 0);
+}
 template <int NV>
 constexpr int sweep_m_stage_doubles() { return 2 * (NV + 1) * SWEEP_THREADS; }
+
+// Piecewise parabolic x-row (one warp per row).  Lane l of a chunk owns
+// cell/face f = c0 + l: it forms the constrained value of face f from cells
+// f-2..f+1 (neighbours by shuffle, cells c0-1 and c0-2 carried from the
+// previous chunk), takes face f+1 from lane l+1 -- or, for lane 31 and the
+// last cell of the row, forms it itself from the staged cells f+1 and f+2 --
+// and limits the parabola of cell f.  Each face value is computed once,
+// which gives the same bits as the reference's per-cell evaluation
+// (Src/States/ppm_states.cpp:129-163): both evaluations are one expression
+// of the same four cells.
+template <int PHYS, int NV, int NDIM, int RS, int CT, typename R, typename CTT>
+__device__ __forceinline__ void sweep_x_row_ppm(const StageArgs<CTT>& a, const Grid3& g, int row,
+                                                double* stg_, int tid) {
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr int SL = 2 * NV + 1;  // staged doubles per lane: V[f], V[f+1], Bs[f]
+  constexpr int NW = SWEEP_THREADS / 32;
+  double(*stg)[SL][SWEEP_THREADS] = reinterpret_cast<double(*)[SL][SWEEP_THREADS]>(stg_);
+  double(*stg2)[NW][NV] = reinterpret_cast<double(*)[NW][NV]>(stg_ + 2 * SL * SWEEP_THREADS);
+  const int lane = tid & 31, w = tid >> 5;
+  if (row >= g.ny * g.nz) return;  // warp-uniform
+  const int nx = g.nx;
+  const long long n = g.n;
+  const long long rb = (long long)row * nx;
+  const R gamma = (R)a.gamma;
+
+  // carried: cells c0-1, c0-2; left state at face c0 (from cell c0-1); flux
+  // and signal speed of face c0-1
+  R pV1[NV], pV2[NV], pVLn[NV], pF[NV], pCm = R(0);
+  {
+    R q[5][NV];
+#pragma unroll
+    for (int m = 0; m < 5; m++) load_cell<NV>(a.V, n, rb + wrapi(nx - 3 + m, nx), q[m]);
+    R vrp[NV];
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      const R fa = ppm_face(q[0][nv], q[1][nv], q[2][nv], q[3][nv]);  // face nx-1
+      const R fb = ppm_face(q[1][nv], q[2][nv], q[3][nv], q[4][nv]);  // face nx = 0
+      R dvp, dvm;
+      ppm_cell(q[2][nv], fa, fb, dvp, dvm);
+      pVLn[nv] = q[2][nv] + dvp;
+      vrp[nv] = q[2][nv] + dvm;
+      pV1[nv] = q[2][nv];
+      pV2[nv] = q[1][nv];
+      pF[nv] = R(0);
+    }
+    if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(q[2], vrp, pVLn);
+  }
+  R fF[NV], fCm = R(0);
+  R F[NV], cm = R(0);
+#pragma unroll
+  for (int nv = 0; nv < NV; nv++) { fF[nv] = R(0); F[nv] = R(0); }
+  uint32_t err = 0;
+
+  auto stage_chunk = [&](int c0, int b) {
+    const int f = c0 + lane;
+    const int fc = f < nx ? f : nx - 1;
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][nv][tid], a.V + nv * n + rb + fc);
+    if (lane == 31 || f + 1 >= nx) {
+      const int fp = wrapi(fc + 1, nx);
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][NV + nv][tid], a.V + nv * n + rb + fp);
+    }
+    if (f < nx && (lane == 31 || f + 1 >= nx)) {  // one lane per chunk
+      const int fp2 = wrapi(fc + 2, nx);
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) cp_async8(&stg2[b][w][nv], a.V + nv * n + rb + fp2);
+    }
+    if constexpr (PHYS != PHYS_HD) cp_async8(&stg[b][2 * NV][tid], a.Bs[0] + rb + fc);
+    cp_async_commit();
+  };
+  stage_chunk(0, 0);
+  int buf = 0;
+  for (int c0 = 0; c0 < nx; c0 += 32, buf ^= 1) {
+    const int f = c0 + lane;
+    const bool act = f < nx;
+    stage_chunk(c0 + 32 < nx ? c0 + 32 : c0, buf ^ 1);   // prefetch the next chunk
+    cp_async_wait1();
+    const bool selfp1 = (lane == 31) || (f + 1 >= nx);
+    R Vc[NV], vL[NV], vR[NV], vLn[NV];
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      Vc[nv] = (R)stg[buf][nv][tid];
+      const R sp1 = selfp1 ? (R)stg[buf][NV + nv][tid] : R(0);
+      const R sp2 = (act && selfp1) ? (R)stg2[buf][w][nv] : R(0);
+      const R up1 = __shfl_up_sync(FULL, Vc[nv], 1);
+      const R up2 = __shfl_up_sync(FULL, Vc[nv], 2);
+      const R dn1 = __shfl_down_sync(FULL, Vc[nv], 1);
+      const R vm1 = (lane == 0) ? pV1[nv] : up1;
+      const R vm2 = (lane == 0) ? pV2[nv] : ((lane == 1) ? pV1[nv] : up2);
+      const R vp1 = selfp1 ? sp1 : dn1;
+      const R cf = ppm_face(vm2, vm1, Vc[nv], vp1);            // face f
+      const R nxt = __shfl_down_sync(FULL, cf, 1);
+      const R cfn = selfp1 ? ppm_face(vm1, Vc[nv], vp1, sp2) : nxt;  // face f+1
+      R dvp, dvm;
+      ppm_cell(Vc[nv], cf, cfn, dvp, dvm);
+      vR[nv] = Vc[nv] + dvm;
+      vLn[nv] = Vc[nv] + dvp;
+    }
+    if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(Vc, vR, vLn);
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      R l = __shfl_up_sync(FULL, vLn[nv], 1);
+      vL[nv] = (lane == 0) ? pVLn[nv] : l;
+    }
+    R Bn = R(0);
+    if constexpr (PHYS != PHYS_HD) {
+      Bn = (R)stg[buf][2 * NV][tid];
+      vL[BX1] = Bn;
+      vR[BX1] = Bn;
+    }
+    CTFace<R> ct;
+    cm = riemann<PHYS, RS, CT, 0>(vL, vR, F, gamma, Bn, ct, err);
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++)
+      if (act && rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) err |= ERR_NAN | ERR_QUIT;
+    if constexpr (PHYS != PHYS_HD) {
+      if (act) store_ct(a, 0, rb + f, ct);
+    }
+    R Fm1[NV];
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      R t = __shfl_up_sync(FULL, F[nv], 1);
+      Fm1[nv] = (lane == 0) ? pF[nv] : t;
+    }
+    R cmm1;
+    {
+      R t = __shfl_up_sync(FULL, cm, 1);
+      cmm1 = (lane == 0) ? pCm : t;
+    }
+    if (act && f >= 1)
+      cell_update<PHYS, NV, NDIM>(a, n, rb + (f - 1), Fm1, F, cmm1, cm, 0);
+    if (c0 == 0) {
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) fF[nv] = F[nv];
+      fCm = cm;
+    }
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      pV2[nv] = __shfl_sync(FULL, Vc[nv], 30);
+      pV1[nv] = __shfl_sync(FULL, Vc[nv], 31);
+      pVLn[nv] = __shfl_sync(FULL, vLn[nv], 31);
+      pF[nv] = __shfl_sync(FULL, F[nv], 31);
+    }
+    pCm = __shfl_sync(FULL, cm, 31);
+  }
+  cp_async_wait0();
+  {
+    R F0[NV];
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) F0[nv] = __shfl_sync(FULL, fF[nv], 0);
+    R cm0 = __shfl_sync(FULL, fCm, 0);
+    if (lane == ((nx - 1) & 31))
+      cell_update<PHYS, NV, NDIM>(a, n, rb + (nx - 1), F, F0, cm, cm0, 0);
+  }
+  if (err) atomicOr(a.err, err);
+}
 
 // One x-row per warp.  `stg_` is the block's staging area
 // (sweep_x_stage_doubles<NV>() doubles of shared memory), `tid` the thread's
@@ -177,6 +337,10 @@ constexpr int sweep_m_stage_doubles() { return 2 * (NV + 1) * SWEEP_THREADS; }
 template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, typename R, typename CTT>
 __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3& g, int row,
                                             double* stg_, int tid) {
+  if constexpr (LIM == LIM_PPM) {
+    sweep_x_row_ppm<PHYS, NV, NDIM, RS, CT, R, CTT>(a, g, row, stg_, tid);
+    return;
+  }
   constexpr unsigned FULL = 0xffffffffu;
   constexpr int SL = 2 * NV + 1;  // staged doubles per lane: V[f], V[f+1], Bs[f]
   double(*stg)[SL][SWEEP_THREADS] = reinterpret_cast<double(*)[SL][SWEEP_THREADS]>(stg_);
@@ -313,7 +477,7 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
 template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, typename R, typename CTT>
 __global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
     sweep_x_kernel(StageArgs<CTT> a, Grid3 g) {
-  __shared__ double stg[sweep_x_stage_doubles<NV>()];
+  __shared__ double stg[sweep_x_stage_doubles<NV, LIM>()];
   const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   sweep_x_row<PHYS, NV, NDIM, RS, CT, LIM, R, CTT>(a, g, row, stg, threadIdx.x);
 }
@@ -325,6 +489,102 @@ __global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
 // is solved.  Writes the direction's flux differences, inverse-dt terms and
 // UCT face data (no loads besides the stencil).
 // ---------------------------------------------------------------------
+// Piecewise parabolic y/z march: cells m-1, m, m+1 in registers, cell m+2
+// staged with cp.async (one iteration ahead: cell m+3 and face m+1 are
+// prefetched while face m is solved).  The constrained value of face m+1 is
+// formed from cells m-1..m+2 and carried to the next iteration as face m's.
+template <int PHYS, int NV, int NDIM, int RS, int CT, int DIR, typename R, typename CTT>
+__device__ __forceinline__ void sweep_m_col_ppm(const StageArgs<CTT>& a, const Grid3& g, int i,
+                                                int t, int seg, int S, double* stg_, int tid) {
+  double(*stg)[NV + 1][SWEEP_THREADS] = reinterpret_cast<double(*)[NV + 1][SWEEP_THREADS]>(stg_);
+  const int nd = (DIR == 1) ? g.ny : g.nz;
+  const long long n = g.n;
+  const R gamma = (R)a.gamma;
+  uint32_t err = 0;
+  if (i < g.nx) {
+    const long long stride = (DIR == 1) ? (long long)g.nx : (long long)g.nx * g.ny;
+    const long long base = (DIR == 1) ? i + (long long)g.nx * g.ny * t
+                                      : i + (long long)g.nx * t;
+    const int m0 = seg * S;
+    const int m1 = min(m0 + S, nd);
+    auto stage = [&](int mcell, int mface, int b) {
+      const long long cc = base + (long long)wrapi(mcell, nd) * stride;
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][nv][tid], a.V + nv * n + cc);
+      if constexpr (PHYS != PHYS_HD)
+        cp_async8(&stg[b][NV][tid], a.Bs[DIR] + base + (long long)wrapi(mface, nd) * stride);
+      cp_async_commit();
+    };
+    stage(m0 + 2, m0, 0);
+    R W0[NV], W1[NV], W2[NV], Fm[NV], vLn[NV], Fp[NV], cmp = R(0);
+    {
+      R q3[NV], q2[NV];
+      load_cell<NV>(a.V, n, base + wrapi(m0 - 3, nd) * stride, q3);
+      load_cell<NV>(a.V, n, base + wrapi(m0 - 2, nd) * stride, q2);
+      load_cell<NV>(a.V, n, base + wrapi(m0 - 1, nd) * stride, W0);
+      load_cell<NV>(a.V, n, base + (long long)m0 * stride, W1);
+      load_cell<NV>(a.V, n, base + wrapi(m0 + 1, nd) * stride, W2);
+      R vrp[NV];
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) {
+        const R fa = ppm_face(q3[nv], q2[nv], W0[nv], W1[nv]);   // face m0-1
+        Fm[nv] = ppm_face(q2[nv], W0[nv], W1[nv], W2[nv]);       // face m0
+        R dvp, dvm;
+        ppm_cell(W0[nv], fa, Fm[nv], dvp, dvm);                   // cell m0-1
+        vLn[nv] = W0[nv] + dvp;
+        vrp[nv] = W0[nv] + dvm;
+        Fp[nv] = R(0);
+      }
+      if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(W0, vrp, vLn);
+    }
+    int buf = 0;
+    for (int m = m0; m <= m1; m++, buf ^= 1) {
+      stage(m + 3, m + 1, buf ^ 1);   // prefetch for the next iteration
+      cp_async_wait1();
+      R vL[NV], vR[NV], F[NV], W3[NV];
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) {
+        W3[nv] = (R)stg[buf][nv][tid];                             // cell m+2
+        const R fn = ppm_face(W0[nv], W1[nv], W2[nv], W3[nv]);     // face m+1
+        R dvp, dvm;
+        ppm_cell(W1[nv], Fm[nv], fn, dvp, dvm);                   // cell m
+        vL[nv] = vLn[nv];
+        vR[nv] = W1[nv] + dvm;
+        vLn[nv] = W1[nv] + dvp;
+        Fm[nv] = fn;
+      }
+      if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(W1, vR, vLn);
+      R Bn = R(0);
+      if constexpr (PHYS != PHYS_HD) {
+        Bn = (R)stg[buf][NV][tid];
+        vL[BX1 + DIR] = Bn;
+        vR[BX1 + DIR] = Bn;
+      }
+      CTFace<R> ct;
+      R cm = riemann<PHYS, RS, CT, DIR>(vL, vR, F, gamma, Bn, ct, err);
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++)
+        if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) err |= ERR_NAN | ERR_QUIT;
+      if constexpr (PHYS != PHYS_HD) {
+        if (m < m1) store_ct(a, DIR, base + (long long)wrapi(m, nd) * stride, ct);
+      }
+      if (m > m0)
+        cell_update<PHYS, NV, NDIM>(a, n, base + (long long)(m - 1) * stride, Fp, F, cmp, cm,
+                                    DIR);
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) {
+        W0[nv] = W1[nv];
+        W1[nv] = W2[nv];
+        W2[nv] = W3[nv];
+        Fp[nv] = F[nv];
+      }
+      cmp = cm;
+    }
+    cp_async_wait0();
+  }
+  if (err) atomicOr(a.err, err);
+}
+
 // One (x column i, transverse index t, pencil segment seg) per thread: t is
 // k for DIR=1 and j for DIR=2; the segment covers cells [seg*S, seg*S+S).
 // `stg_` is the block's staging area (sweep_m_stage_doubles<NV>() doubles).
@@ -332,6 +592,10 @@ template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, int DIR, typename
           typename CTT>
 __device__ __forceinline__ void sweep_m_col(const StageArgs<CTT>& a, const Grid3& g, int i, int t,
                                             int seg, int S, double* stg_, int tid) {
+  if constexpr (LIM == LIM_PPM) {
+    sweep_m_col_ppm<PHYS, NV, NDIM, RS, CT, DIR, R, CTT>(a, g, i, t, seg, S, stg_, tid);
+    return;
+  }
   double(*stg)[NV + 1][SWEEP_THREADS] = reinterpret_cast<double(*)[NV + 1][SWEEP_THREADS]>(stg_);
   const int nd = (DIR == 1) ? g.ny : g.nz;
   const long long n = g.n;
@@ -435,12 +699,29 @@ __global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
 template <int LIM, typename R>
 __device__ __forceinline__ void uct_terms(const R* b, const R* q, R aL, R aR, R dL, R dR,
                                           R& avg, R& phi) {
-  R dbl = limit<LIM_MC>(b[2] - b[1], b[1] - b[0]);
-  R dbr = limit<LIM_MC>(b[3] - b[2], b[2] - b[1]);
-  R dql = limit<LIM>(q[2] - q[1], q[1] - q[0]);
-  R dqr = limit<LIM>(q[3] - q[2], q[2] - q[1]);
-  R bL = b[1] + R(0.5) * dbl, bR = b[2] - R(0.5) * dbr;
-  R vL = q[1] + R(0.5) * dql, vR = q[2] - R(0.5) * dqr;
+  R bL, bR, vL, vR;
+  if constexpr (LIM == LIM_PPM) {
+    // parabolic reconstruction of both the face field and the velocity
+    // (Src/MHD/CT/ct_emf_average.cpp:556-559 with RECONSTRUCTION PARABOLIC)
+    R p1, m1, p2, m2;
+    par3_cell(b[0], b[1], b[2], p1, m1);
+    par3_cell(b[1], b[2], b[3], p2, m2);
+    bL = b[1] + p1;
+    bR = b[2] + m2;
+    par3_cell(q[0], q[1], q[2], p1, m1);
+    par3_cell(q[1], q[2], q[3], p2, m2);
+    vL = q[1] + p1;
+    vR = q[2] + m2;
+  } else {
+    R dbl = limit<LIM_MC>(b[2] - b[1], b[1] - b[0]);
+    R dbr = limit<LIM_MC>(b[3] - b[2], b[2] - b[1]);
+    R dql = limit<LIM>(q[2] - q[1], q[1] - q[0]);
+    R dqr = limit<LIM>(q[3] - q[2], q[2] - q[1]);
+    bL = b[1] + R(0.5) * dbl;
+    bR = b[2] - R(0.5) * dbr;
+    vL = q[1] + R(0.5) * dql;
+    vR = q[2] - R(0.5) * dqr;
+  }
   phi = dR * bR - dL * bL;
   avg = aL * vL * bL + aR * vR * bR;
 }

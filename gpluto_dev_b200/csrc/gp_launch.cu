@@ -100,6 +100,7 @@ static int by_lim(const StageArgs<CTT>& a, const GridDims& g, int lim, int seg, 
     case LIM_MC: run_stage<PHYS, NV, NDIM, RS, CT, LIM_MC>(a, g, seg, s, ev); return 0;
     case LIM_VL: run_stage<PHYS, NV, NDIM, RS, CT, LIM_VL>(a, g, seg, s, ev); return 0;
     case LIM_MINMOD: run_stage<PHYS, NV, NDIM, RS, CT, LIM_MINMOD>(a, g, seg, s, ev); return 0;
+    case LIM_PPM: run_stage<PHYS, NV, NDIM, RS, CT, LIM_PPM>(a, g, seg, s, ev); return 0;
     default: return -1;
   }
 }

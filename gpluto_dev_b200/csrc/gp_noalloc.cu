@@ -150,7 +150,10 @@ extern "C" int gp_advance_step_noalloc(const gp_grid_desc* grid, const gp_scheme
     for (int r = 0; r < 6; r++) d.ct[q][r] = ct[q][r];
   }
   gp::GridDims g{nx, ny, nz, n};
-  gp::SchemeKey key{scheme->physics, ndim, scheme->riemann, scheme->ct_emf, scheme->limiter};
+  const bool ppm = scheme->reconstruction == GP_REC_PARABOLIC;
+  if (ppm && (nx < 4 || ny < 4 || (ndim == 3 && nz < 4))) return GP_ERR_INVALID;
+  gp::SchemeKey key{scheme->physics, ndim, scheme->riemann, scheme->ct_emf,
+                    ppm ? 4 /* LIM_PPM */ : scheme->limiter};
   int seg = 64;
   {
     const long long cols = (long long)nx * (ndim == 3 ? nz : 1);

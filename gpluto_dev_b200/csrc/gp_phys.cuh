@@ -31,7 +31,9 @@ constexpr uint32_t ERR_NAN = 1u << 11;
 constexpr uint32_t ERR_QUIT = 1u << 15;
 
 enum : int { PHYS_HD = 0, PHYS_MHD = 1, PHYS_RMHD = 2 };
-enum : int { LIM_FLAT = 0, LIM_MINMOD = 1, LIM_VL = 2, LIM_MC = 3 };
+// LIM_PPM selects piecewise parabolic reconstruction (RECONSTRUCTION
+// PARABOLIC); it is carried in the limiter slot of the scheme templates.
+enum : int { LIM_FLAT = 0, LIM_MINMOD = 1, LIM_VL = 2, LIM_MC = 3, LIM_PPM = 4 };
 enum : int { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2 };
 enum : int { CT_UCT_HLL = 0, CT_UCT_HLLD = 1 };
 
@@ -63,6 +65,63 @@ __device__ __forceinline__ R limit(R dvp, R dvm) {
     return (dvp * dvm > R(0) ? (rabs(dvp) < rabs(dvm) ? dvp : dvm) : R(0));
   } else {
     return R(0);
+  }
+}
+
+// Src/macros.hpp:200
+template <typename R>
+__device__ __forceinline__ R minmod(R a, R b) {
+  return (a * b > R(0) ? (rabs(a) < rabs(b) ? a : b) : R(0));
+}
+
+// PPM constrained face value between cells q0 and qp (stencil qm, q0, qp,
+// qpp): the uniform-grid 4-point value of
+// Src/States/reconstruction_geometry.hpp:97-101, limited to lie between the
+// adjacent cell values (Src/States/ppm_states.cpp:139-145).  The reference
+// evaluates it once as the right face of cell q0 and once as the left face
+// of cell qp; both are this same expression, so it is computed once here.
+template <typename R>
+__device__ __forceinline__ R ppm_face(R qm, R q0, R qp, R qpp) {
+  R f = (-qm + R(7) * (q0 + qp) - qpp) / R(12);
+  return q0 + minmod(f - q0, qp - q0);
+}
+
+// Parabolic limiter of a cell with constrained face values fm (left) and fp
+// (right): Src/States/ppm_states.cpp:147-163.  Returns the increments.
+template <typename R>
+__device__ __forceinline__ void ppm_cell(R v, R fm, R fp, R& dvp, R& dvm) {
+  dvp = fp - v;
+  dvm = fm - v;
+  if (dvp * dvm >= R(0)) {
+    dvp = R(0);
+    dvm = R(0);
+  } else {
+    if (rabs(dvp) >= R(2) * rabs(dvm)) dvp = -R(2) * dvm;
+    else if (rabs(dvm) >= R(2) * rabs(dvp)) dvm = -R(2) * dvp;
+  }
+}
+
+// 3-point parabolic reconstruction of the UCT edge data with PPM
+// (Src/array_reconstruct.cpp:208-270, uniform grid): increments of cell q0
+// to its right (dqp) and left (dqm) faces.
+template <typename R>
+__device__ __forceinline__ void par3_cell(R qm, R q0, R qp, R& dqp, R& dqm) {
+  R fp = (-qm + R(5) * q0 + R(2) * qp) / R(6);
+  R fm = (R(2) * qm + R(5) * q0 - qp) / R(6);
+  dqp = fp - q0;
+  dqm = fm - q0;
+  R dq = qp - q0;
+  fp = q0 + minmod(dqp, dq);
+  dq = q0 - qm;
+  fm = q0 + minmod(dqm, -dq);
+  dqp = fp - q0;
+  dqm = fm - q0;
+  if (dqp * dqm >= R(0)) {
+    dqp = R(0);
+    dqm = R(0);
+  } else {
+    if (rabs(dqp) >= R(2) * rabs(dqm)) dqp = -R(2) * dqm;
+    else if (rabs(dqm) >= R(2) * rabs(dqp)) dqm = -R(2) * dqp;
   }
 }
 

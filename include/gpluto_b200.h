@@ -57,6 +57,9 @@ enum { GP_RS_HLL = 0, GP_RS_HLLC = 1, GP_RS_HLLD = 2 };
 enum { GP_CT_UCT_HLL = 0, GP_CT_UCT_HLLD = 1 };
 /* [Boundary] types (Src/boundary.cpp) */
 enum { GP_BC_PERIODIC = 0 };
+/* RECONSTRUCTION (definitions.hpp): LINEAR (PLM with LIMITER) or PARABOLIC
+   (PPM, Src/States/ppm_states.cpp) */
+enum { GP_REC_LINEAR = 0, GP_REC_PARABOLIC = 1 };
 /* arithmetic form */
 enum { GP_FP64 = 0, GP_MIXED = 1 };
 /* host array layouts */
@@ -86,6 +89,7 @@ typedef struct gp_scheme {
   double cfl_max_var;     /* Runtime::cfl_max_var */
   double small_rho;       /* RunConfig::small_rho (1e-12 default) */
   double small_prs;       /* RunConfig::small_prs (1e-12 default) */
+  int reconstruction;     /* GP_REC_LINEAR (limiter applies) or GP_REC_PARABOLIC */
 } gp_scheme;
 
 /* Per-step result: what the host needs for NextTimeStep and error handling. */

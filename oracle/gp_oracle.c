@@ -597,6 +597,38 @@ static double Limit(int lim, double dvp, double dvm) {
   return dv;
 }
 
+/* Src/macros.hpp:200 */
+static double Minmod(double a, double b) {
+  return (a*b > 0.0 ? (fabs(a) < fabs(b) ? a : b) : 0.0);
+}
+
+/* Piecewise parabolic states of cell i (primitive limiting):
+   Src/States/ppm_states.cpp:129-163 with the uniform-grid face value of
+   Src/States/reconstruction_geometry.hpp:97-101.  v points at cell i of a
+   pencil with stride `st`; returns the increments to the right (dvp) and
+   left (dvm) faces. */
+static void PPM_Cell(const double *v, long st, double *dvp_out, double *dvm_out) {
+  double vim2 = v[-2*st], vim1 = v[-st], vi = v[0], vip1 = v[st], vip2 = v[2*st];
+  double vp = (-vim1 + 7.0*(vi + vip1) - vip2)/12.0;
+  double vm = (-vim2 + 7.0*(vim1 + vi) - vip1)/12.0;
+  double dv, dvp, dvm;
+  dv  = vip1 - vi;
+  dvp = vp - vi;
+  vp  = vi + Minmod(dvp, dv);
+  dv  = vi - vim1;
+  dvm = vm - vim1;
+  vm  = vim1 + Minmod(dvm, dv);
+  dvp = vp - vi;
+  dvm = vm - vi;
+  if (dvp*dvm >= 0.0) dvp = dvm = 0.0;
+  else {
+    if      (fabs(dvp) >= 2.0*fabs(dvm)) dvp = -2.0*dvm;
+    else if (fabs(dvm) >= 2.0*fabs(dvp)) dvm = -2.0*dvp;
+  }
+  *dvp_out = dvp;
+  *dvm_out = dvm;
+}
+
 /* ------------------------------------------------------------------ */
 /* boundary: Src/boundary.cpp:67-322 + PeriodicBoundary 502-675         */
 /* ------------------------------------------------------------------ */
@@ -677,9 +709,17 @@ static void Sweep(orc_t *o, int dir, double dt) {
       for (nv = 0; nv < nvar; nv++) v[i*nvar + nv] = *VC(o, o->Vc, nv, ti, tj, tk);
       if (isMHD) Bn[i] = o->Vs[dir][SI(o, dir, ti, tj, tk)];
     }
-    /* Reconstruct: Src/States/plm_states.cpp:99-141 */
+    /* Reconstruct: Src/States/plm_states.cpp:99-141, or (PARABOLIC)
+       Src/States/ppm_states.cpp:110-164 */
     for (nv = 0; nv < nvar; nv++)
       for (i = ib-1; i <= ie+1; i++) {
+        if (o->c.limiter == ORC_LIM_PPM) {
+          double dvp, dvm;
+          PPM_Cell(v + i*nvar + nv, nvar, &dvp, &dvm);
+          vL[(i+1)*nvar + nv] = v[i*nvar + nv] + dvp;
+          vR[i*nvar + nv]     = v[i*nvar + nv] + dvm;
+          continue;
+        }
         double dvp = v[(i+1)*nvar + nv] - v[i*nvar + nv];
         double dvm = v[i*nvar + nv] - v[(i-1)*nvar + nv];
         double dv = Limit(o->c.limiter, dvp, dvm);
@@ -750,6 +790,29 @@ static void ArrayRec(orc_t *o, int dir, int t1, int t2, int stag, const double *
     TrueIdx(dir, i, t1, t2, &ti, &tj, &tk);
     q[i] = (stag >= 0) ? o->Vs[stag][SI(o, stag, ti, tj, tk)] : Qe[EI(o, ti, tj, tk)];
   }
+  if (lim == ORC_LIM_PPM) {
+    /* PARABOLIC branch, Src/array_reconstruct.cpp:208-270 (uniform grid) */
+    for (i = 1; i < nd-1; i++) {
+      double qp = (    -q[i-1] + 5.0*q[i] + 2.0*q[i+1])/6.0;
+      double qm = ( 2.0*q[i-1] + 5.0*q[i] -     q[i+1])/6.0;
+      double dqp = qp - q[i];
+      double dqm = qm - q[i];
+      double dq  = q[i+1] - q[i];
+      qp  = q[i] + Minmod(dqp, dq);
+      dq  = q[i] - q[i-1];
+      qm  = q[i] + Minmod(dqm, -dq);
+      dqp = qp - q[i];
+      dqm = qm - q[i];
+      if (dqp*dqm >= 0.0) dqp = dqm = 0.0;
+      else {
+        if      (fabs(dqp) >= 2.0*fabs(dqm)) dqp = -2.0*dqm;
+        else if (fabs(dqm) >= 2.0*fabs(dqp)) dqm = -2.0*dqp;
+      }
+      qL[i+1] = q[i] + dqp;
+      qR[i]   = q[i] + dqm;
+    }
+    return;
+  }
   for (i = 1; i < nd-1; i++) {
     double dqp = q[i+1] - q[i];
     double dqm = q[i] - q[i-1];
@@ -761,7 +824,9 @@ static void ArrayRec(orc_t *o, int dir, int t1, int t2, int stag, const double *
 
 static void ComputeEMF(orc_t *o) {
   const int ndim = o->c.ndim;
-  int recV = o->c.limiter, recB = ORC_LIM_MC;
+  /* Src/MHD/CT/ct_emf_average.cpp:553-559: MC for B and the scheme limiter
+     for velocities with linear reconstruction; parabolic for both with PPM */
+  int recV = o->c.limiter, recB = (o->c.limiter == ORC_LIM_PPM ? ORC_LIM_PPM : ORC_LIM_MC);
   int ib = o->beg[0], ie = o->end[0] + 1;
   int jb = o->beg[1], je = o->end[1] + 1;
   int kb = o->beg[2], ke = o->end[2] + (ndim == 3);
@@ -1082,7 +1147,7 @@ void *orc_create(const orc_cfg *cfg) {
   int d, e;
   o->c = *cfg;
   o->nvar = (cfg->physics == ORC_HD) ? 5 : 8;
-  o->ng = 2;   /* PLM: Src/get_nghost.cpp */
+  o->ng = (cfg->limiter == ORC_LIM_PPM) ? 3 : 2;   /* Src/get_nghost.cpp:33-44 */
   o->ncell = 1;
   for (d = 0; d < 3; d++) {
     if (d < cfg->ndim) { o->nt[d] = cfg->n[d] + 2*o->ng; o->beg[d] = o->ng; }

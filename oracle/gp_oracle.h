@@ -7,7 +7,8 @@
 #include <stdint.h>
 
 enum { ORC_HD = 0, ORC_MHD = 1, ORC_RMHD = 2 };
-enum { ORC_LIM_FLAT = 0, ORC_LIM_MINMOD = 1, ORC_LIM_VL = 2, ORC_LIM_MC = 3 };
+enum { ORC_LIM_FLAT = 0, ORC_LIM_MINMOD = 1, ORC_LIM_VL = 2, ORC_LIM_MC = 3,
+       ORC_LIM_PPM = 4 /* RECONSTRUCTION PARABOLIC (no slope limiter) */ };
 enum { ORC_HLL = 0, ORC_HLLC = 1, ORC_HLLD = 2 };
 enum { ORC_UCT_HLL = 0, ORC_UCT_HLLD = 1 };
 

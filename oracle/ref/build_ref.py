@@ -37,7 +37,7 @@ set_geometry set_grid set_output set_var_names show_config split_source startup
 sweep_alloc timing tools write_data write_tab write_vtk vector_curl
 userdef_output""".split()
 _MATH_OBJ = "math_lu_decomp math_funcs math_misc math_quadrature math_random".split()
-_STEP_OBJ = "plm_states rk_step update_stage".split()
+_STEP_OBJ = "plm_states rk_step update_stage".split()   # ppm_states for PARABOLIC
 _PHYS = {
     "MHD": ("mappers roe set_solver tvdlf hlld hll hllc rhs gforce".split(),
             ["MHD"]),
@@ -143,7 +143,9 @@ class RefConfig:
     def makefile(self) -> str:
         src = os.path.join(REF_ROOT, "Src")
         phys_obj, phys_dirs = _PHYS[self.physics]
-        objs = _DEFAULT_OBJ + _MATH_OBJ + _STEP_OBJ + phys_obj
+        step = [("ppm_states" if (o == "plm_states" and self.reconstruction == "PARABOLIC")
+                 else o) for o in _STEP_OBJ]
+        objs = _DEFAULT_OBJ + _MATH_OBJ + step + phys_obj
         vdirs = [src, f"{src}/States", f"{src}/Math_Tools"] + [f"{src}/{d}" for d in phys_dirs]
         incs = ["-I.", f"-I{src}"] + [f"-I{src}/{d}" for d in phys_dirs] + [f"-I{src}/States", f"-I{src}/Math_Tools"]
         if self.physics in ("MHD", "RMHD"):

@@ -63,12 +63,30 @@ CASES = {
     "hd3d_vl_hll": (ics.hd_turbulence, dict(n=(12, 12, 10), seed=9),
                     dict(physics="HD", ndim=3, limiter="VANLEER_LIM", solver="hll",
                          cfl=0.4, first_dt=1e-4), 10),
+    # piecewise parabolic reconstruction (RECONSTRUCTION PARABOLIC)
+    "mhd2d_ppm_hlld_ucthlld": (ics.mhd2d_turbulence, dict(n=(32, 32), seed=21),
+                               dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",
+                                    ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4,
+                                    reconstruction="PARABOLIC"), 20),
+    "mhd3d_ppm_hlld_ucthlld": (ics.mhd3d_turbulence, dict(n=(12, 10, 8), seed=22),
+                               dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                    ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4,
+                                    reconstruction="PARABOLIC"), 10),
+    "hd2d_ppm_hllc": (ics.hd_turbulence, dict(n=(32, 24), seed=23),
+                      dict(physics="HD", ndim=2, limiter="MC_LIM", solver="hllc",
+                           cfl=0.4, first_dt=1e-4, reconstruction="PARABOLIC"), 20),
+    "rmhd3d_ppm_hlld_ucthll": (ics.rmhd3d_turbulence,
+                               dict(n=(8, 10, 12), seed=24, lorentz_max=3.0),
+                               dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                    ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
+                                    reconstruction="PARABOLIC"), 8),
 }
 
 
 def ref_cfg_name(rc: dict) -> str:
-    return "{physics}{ndim}d_{limiter}_{solver}_{ct}".format(
-        ct=rc.get("ct_emf", "none"), **rc).lower()
+    lim = "ppm" if rc.get("reconstruction") == "PARABOLIC" else rc["limiter"]
+    return "{physics}{ndim}d_{lim}_{solver}_{ct}".format(
+        ct=rc.get("ct_emf", "none"), lim=lim, **rc).lower()
 
 
 def _as2d(st):
@@ -100,7 +118,8 @@ def make(name: str) -> str:
         V0=st.V, Bs0=np.array(st.Bs) if st.Bs else np.zeros(0),
         V=d.V, U=d.U, Bs=np.array(d.Bs) if d.Bs else np.zeros(0), dt=d.dt, nsteps=nsteps,
         limiter=rc["limiter"], solver=rc["solver"], ct=rc.get("ct_emf", "none"),
-        cfl=rc["cfl"], cfl_max_var=1.1, first_dt=rc["first_dt"])
+        cfl=rc["cfl"], cfl_max_var=1.1, first_dt=rc["first_dt"],
+        reconstruction=rc.get("reconstruction", "LINEAR"))
     return out
 
 

@@ -39,3 +39,6 @@ class Golden:
         self.cfl = float(z["cfl"])
         self.cfl_max_var = float(z["cfl_max_var"])
         self.first_dt = float(z["first_dt"])
+        self.reconstruction = str(z["reconstruction"]) if "reconstruction" in z else "LINEAR"
+        if self.reconstruction == "PARABOLIC":
+            self.limiter = "ppm"

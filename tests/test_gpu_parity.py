@@ -51,6 +51,12 @@ CASES = [
     (ics.mhd3d_turbulence, dict(n=(16, 20, 12), seed=25), "minmod", "hll", "uct_hll", 8),
     (ics.hd_turbulence, dict(n=(40, 36), seed=26), "mc", "hllc", "uct_hll", 20),
     (ics.hd_turbulence, dict(n=(16, 12, 20), seed=27), "vl", "hll", "uct_hll", 10),
+    # PPM: rows of 33 and 65 cells (a last chunk of 1 lane), a row shorter
+    # than a warp, a 5-cell direction
+    (ics.mhd2d_turbulence, dict(n=(33, 17), seed=28), "ppm", "hlld", "uct_hlld", 15),
+    (ics.mhd3d_turbulence, dict(n=(20, 18, 16), seed=29), "ppm", "hlld", "uct_hlld", 8),
+    (ics.hd_turbulence, dict(n=(65, 5), seed=30), "ppm", "hllc", "uct_hll", 12),
+    (ics.mhd2d_turbulence, dict(n=(6, 40), seed=31), "ppm", "hll", "uct_hll", 10),
 ]
 
 
