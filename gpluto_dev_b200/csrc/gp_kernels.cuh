@@ -92,6 +92,19 @@ __device__ __forceinline__ void cp_async_wait0() {
 #endif
 constexpr int SWEEP_THREADS = 128;
 
+// Resident 128-thread blocks per SM the sweep kernels are compiled for
+// (register budget 65536 / (128 * blocks)), measured at 256^3 on 3-D MHD:
+// FP64 x-sweep 3 (168 registers), FP64 y/z sweeps 4 (128), mixed form 5
+// (102); the relativistic solver (FP64 in both forms) keeps 3.
+template <int PHYS, typename R>
+constexpr int sweep_x_minb() {
+  return PHYS == PHYS_RMHD ? 3 : (sizeof(R) == 4 ? 5 : 3);
+}
+template <int PHYS, typename R>
+constexpr int sweep_m_minb() {
+  return PHYS == PHYS_RMHD ? 3 : (sizeof(R) == 4 ? 5 : 4);
+}
+
 // whether conserved component nv receives a flux difference that survives
 // the stage (the cell-centred field along active directions is overwritten
 // by the face average, Src/MHD/CT/ct_field_average.cpp:378-410)
@@ -475,7 +488,7 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
 }
 
 template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, typename R, typename CTT>
-__global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
+__global__ void __launch_bounds__(SWEEP_THREADS, (sweep_x_minb<PHYS, R>()))
     sweep_x_kernel(StageArgs<CTT> a, Grid3 g) {
   __shared__ double stg[sweep_x_stage_doubles<NV, LIM>()];
   const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -678,7 +691,7 @@ __device__ __forceinline__ void sweep_m_col(const StageArgs<CTT>& a, const Grid3
 
 template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, int DIR, typename R,
           typename CTT>
-__global__ void __launch_bounds__(SWEEP_THREADS, GP_SWEEP_MINB)
+__global__ void __launch_bounds__(SWEEP_THREADS, (sweep_m_minb<PHYS, R>()))
     sweep_m_kernel(StageArgs<CTT> a, Grid3 g, int S) {
   __shared__ double stg[sweep_m_stage_doubles<NV>()];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
