@@ -149,7 +149,9 @@ class Solver:
     """Device-resident state of one grid and its Godunov step."""
 
     def __init__(self, ndim: int, shape, scheme: Scheme, xbeg=(0.0, 0.0, 0.0),
-                 xend=(1.0, 1.0, 1.0), nghost: int = 2, stream=None):
+                 xend=(1.0, 1.0, 1.0), nghost: int = 2, stream=None, outflow: int = 0):
+        """``outflow``: bit 2d (2d+1) makes the low (high) side of direction d
+        an OUTFLOW boundary; other sides are periodic."""
         g = GpGridDesc()
         g.ndim = ndim
         nx, ny, nz = (tuple(shape) + (1, 1, 1))[:3]
@@ -157,7 +159,9 @@ class Solver:
         g.nghost = nghost
         for d in range(3):
             g.xbeg[d], g.xend[d] = xbeg[d], xend[d]
-            g.lbound[d] = g.rbound[d] = 0
+            g.lbound[d] = (outflow >> (2 * d)) & 1
+            g.rbound[d] = (outflow >> (2 * d + 1)) & 1
+        self.outflow = outflow
         self.ndim, self.shape = ndim, (nx, ny, nz if ndim == 3 else 1)
         self.scheme = scheme
         self.nvar = 5 if scheme.physics == HD else 8

@@ -80,18 +80,28 @@ __global__ void gather_kernel(const double* __restrict__ src, double* __restrict
   dst[t] = src[(long long)nv * sx * sy * sz + s];
 }
 
-// fill a ghosted array from the interior with periodic wrap (what Boundary()
-// produces for periodic sides); `stag` adds the extra face along that dir.
+// ghost index of the reference layout: periodic wrap, or the nearest
+// interior cell on an outflow side
+__device__ int ghost_src(int i, int n, unsigned outflow, int d) {
+  if (i < 0 && ((outflow >> (2 * d)) & 1u)) return 0;
+  if (i >= n && ((outflow >> (2 * d + 1)) & 1u)) return n - 1;
+  return (i % n + n) % n;
+}
+
+// fill a ghosted array from the interior the way Boundary() fills Vc: periodic
+// wrap, or the zero-gradient copy on outflow sides; `stag` adds the extra face
+// along that dir.
 __global__ void scatter_kernel(const double* __restrict__ src, double* __restrict__ dst,
                                int nvar, int sx, int sy, int sz, int ox, int oy, int oz,
-                               int nx, int ny, int nz) {
+                               int nx, int ny, int nz, unsigned outflow) {
   long long ns = (long long)sx * sy * sz;
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ns * nvar) return;
   int nv = (int)(t / ns);
   long long s = t - (long long)nv * ns;
   int i = (int)(s % sx), j = (int)((s / sx) % sy), k = (int)(s / ((long long)sx * sy));
-  int ii = ((i - ox) % nx + nx) % nx, jj = ((j - oy) % ny + ny) % ny, kk = ((k - oz) % nz + nz) % nz;
+  int ii = ghost_src(i - ox, nx, outflow, 0), jj = ghost_src(j - oy, ny, outflow, 1),
+      kk = ghost_src(k - oz, nz, outflow, 2);
   dst[t] = src[(long long)nv * nx * ny * nz + ii + (long long)nx * (jj + (long long)ny * kk)];
 }
 
@@ -130,6 +140,7 @@ struct gp_handle {
   double* stage_buf;     // device staging for reference-layout transfers
   size_t stage_bytes;
   int launches_per_step;
+  unsigned outflow;      // outflow sides (bit 2d low, 2d+1 high)
 };
 
 namespace {
@@ -172,7 +183,7 @@ int enqueue_step(gp_handle* h, double* hist, int slot, cudaEvent_t* ev = nullptr
   d.err = &h->sc->err;
   const int per_stage = gp::stage_launch_count(h->key);
   auto launch = [&](const gp::StageDesc& sd) {
-    gp::GridDims g{h->nx, h->ny, h->nz, h->n};
+    gp::GridDims g{h->nx, h->ny, h->nz, h->n, h->outflow};
     cudaEvent_t* e = ev ? ev + (sd.stage - 1) * 2 * per_stage : nullptr;
     return h->mixed ? gp::launch_stage_mixed(sd, g, h->key, h->seg, h->stream, e)
                     : gp::launch_stage_fp64(sd, g, h->key, h->seg, h->stream, e);
@@ -258,8 +269,15 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   for (int d = 0; d < 3; d++) {
     if (d < grid->ndim) {
       if (grid->nint[d] < 2) return fail(GP_ERR_INVALID, "nint[%d] < 2", d);
-      if (grid->lbound[d] != GP_BC_PERIODIC || grid->rbound[d] != GP_BC_PERIODIC)
-        return fail(GP_ERR_UNSUPPORTED, "only periodic boundaries are built");
+      const int lb = grid->lbound[d], rb = grid->rbound[d];
+      if ((lb != GP_BC_PERIODIC && lb != GP_BC_OUTFLOW) ||
+          (rb != GP_BC_PERIODIC && rb != GP_BC_OUTFLOW))
+        return fail(GP_ERR_UNSUPPORTED, "boundary types are periodic or outflow");
+      if ((lb == GP_BC_PERIODIC) != (rb == GP_BC_PERIODIC))
+        return fail(GP_ERR_INVALID, "a periodic direction needs both sides periodic");
+      if (lb == GP_BC_OUTFLOW && scheme->physics != GP_HD)
+        return fail(GP_ERR_UNSUPPORTED, "outflow boundaries are built for HD "
+                    "(constrained-transport ghost faces are not)");
       if (!uniform(grid->dx[d], grid->nint[d] + 2 * grid->nghost))
         return fail(GP_ERR_UNSUPPORTED, "non-uniform grid along %d", d);
     }
@@ -289,6 +307,10 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   h->ny = grid->nint[1];
   h->nz = grid->ndim == 3 ? grid->nint[2] : 1;
   h->n = (long long)h->nx * h->ny * h->nz;
+  for (int d = 0; d < grid->ndim; d++) {
+    if (grid->lbound[d] == GP_BC_OUTFLOW) h->outflow |= 1u << (2 * d);
+    if (grid->rbound[d] == GP_BC_OUTFLOW) h->outflow |= 1u << (2 * d + 1);
+  }
   if (h->n >= (1LL << 31)) {
     delete h;
     return fail(GP_ERR_UNSUPPORTED, "grids are limited to fewer than 2^31 cells");
@@ -414,7 +436,8 @@ static int download_one(gp_handle* h, int layout, const double* src, double* dst
   int rc = ensure_stage(h, sizeof(double) * tot);
   if (rc) return rc;
   scatter_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, h->stream>>>(
-      src, h->stage_buf, nvar, s[0], s[1], s[2], o[0], o[1], o[2], h->nx, h->ny, h->nz);
+      src, h->stage_buf, nvar, s[0], s[1], s[2], o[0], o[1], o[2], h->nx, h->ny, h->nz,
+      h->outflow);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaMemcpyAsync(dst, h->stage_buf, sizeof(double) * tot, cudaMemcpyDeviceToHost,
                            h->stream));

@@ -30,6 +30,9 @@ namespace gp {
 struct Grid3 {
   int nx, ny, nz;
   long long n;  // nx*ny*nz
+  // outflow sides: bit 2d = low side of direction d, bit 2d+1 = high side;
+  // every other side is periodic
+  unsigned outflow = 0u;
 };
 
 template <typename CTT>
@@ -56,6 +59,15 @@ struct StageArgs {
 
 __device__ __forceinline__ int wrapi(int i, int n) {
   return i < 0 ? i + n : (i >= n ? i - n : i);
+}
+
+// Cell index along direction d for an index up to n past either end: a
+// periodic side wraps; an outflow side gives the nearest interior cell, the
+// value OutflowBoundary copies into the ghost zone (Src/boundary.cpp:677-780).
+__device__ __forceinline__ int gidx(int i, int n, unsigned outflow, int d) {
+  if (i < 0) return ((outflow >> (2 * d)) & 1u) ? 0 : i + n;
+  if (i >= n) return ((outflow >> (2 * d + 1)) & 1u) ? n - 1 : i - n;
+  return i;
 }
 
 template <int NV, typename R>
@@ -207,6 +219,9 @@ __device__ __forceinline__ void sweep_x_row_ppm(const StageArgs<CTT>& a, const G
   const int lane = tid & 31, w = tid >> 5;
   if (row >= g.ny * g.nz) return;  // warp-uniform
   const int nx = g.nx;
+  const unsigned ob = g.outflow;
+  // faces solved: nx (periodic: face nx is face 0) or nx+1 (outflow high side)
+  const int nf = nx + (int)((ob >> 1) & 1u);
   const long long n = g.n;
   const long long rb = (long long)row * nx;
   const R gamma = (R)a.gamma;
@@ -217,7 +232,7 @@ __device__ __forceinline__ void sweep_x_row_ppm(const StageArgs<CTT>& a, const G
   {
     R q[5][NV];
 #pragma unroll
-    for (int m = 0; m < 5; m++) load_cell<NV>(a.V, n, rb + wrapi(nx - 3 + m, nx), q[m]);
+    for (int m = 0; m < 5; m++) load_cell<NV>(a.V, n, rb + gidx(m - 3, nx, ob, 0), q[m]);
     R vrp[NV];
 #pragma unroll
     for (int nv = 0; nv < NV; nv++) {
@@ -244,13 +259,13 @@ __device__ __forceinline__ void sweep_x_row_ppm(const StageArgs<CTT>& a, const G
     const int fc = f < nx ? f : nx - 1;
 #pragma unroll
     for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][nv][tid], a.V + nv * n + rb + fc);
-    if (lane == 31 || f + 1 >= nx) {
-      const int fp = wrapi(fc + 1, nx);
+    if (lane == 31 || f + 1 >= nf) {
+      const int fp = gidx(fc + 1, nx, ob, 0);
 #pragma unroll
       for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][NV + nv][tid], a.V + nv * n + rb + fp);
     }
-    if (f < nx && (lane == 31 || f + 1 >= nx)) {  // one lane per chunk
-      const int fp2 = wrapi(fc + 2, nx);
+    if (f < nf && (lane == 31 || f + 1 >= nf)) {  // one lane per chunk
+      const int fp2 = gidx(fc + 2, nx, ob, 0);
 #pragma unroll
       for (int nv = 0; nv < NV; nv++) cp_async8(&stg2[b][w][nv], a.V + nv * n + rb + fp2);
     }
@@ -259,12 +274,12 @@ __device__ __forceinline__ void sweep_x_row_ppm(const StageArgs<CTT>& a, const G
   };
   stage_chunk(0, 0);
   int buf = 0;
-  for (int c0 = 0; c0 < nx; c0 += 32, buf ^= 1) {
+  for (int c0 = 0; c0 < nf; c0 += 32, buf ^= 1) {
     const int f = c0 + lane;
-    const bool act = f < nx;
-    stage_chunk(c0 + 32 < nx ? c0 + 32 : c0, buf ^ 1);   // prefetch the next chunk
+    const bool act = f < nf;
+    stage_chunk(c0 + 32 < nf ? c0 + 32 : c0, buf ^ 1);   // prefetch the next chunk
     cp_async_wait1();
-    const bool selfp1 = (lane == 31) || (f + 1 >= nx);
+    const bool selfp1 = (lane == 31) || (f + 1 >= nf);
     R Vc[NV], vL[NV], vR[NV], vLn[NV];
 #pragma unroll
     for (int nv = 0; nv < NV; nv++) {
@@ -333,7 +348,7 @@ __device__ __forceinline__ void sweep_x_row_ppm(const StageArgs<CTT>& a, const G
     pCm = __shfl_sync(FULL, cm, 31);
   }
   cp_async_wait0();
-  {
+  if (nf == nx) {  // periodic: the last cell's right face is face 0
     R F0[NV];
 #pragma unroll
     for (int nv = 0; nv < NV; nv++) F0[nv] = __shfl_sync(FULL, fF[nv], 0);
@@ -360,6 +375,9 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
   const int lane = tid & 31;
   if (row >= g.ny * g.nz) return;  // warp-uniform
   const int nx = g.nx;
+  const unsigned ob = g.outflow;
+  // faces solved: nx (periodic: face nx is face 0) or nx+1 (outflow high side)
+  const int nf = nx + (int)((ob >> 1) & 1u);
   const long long n = g.n;
   const long long rb = (long long)row * nx;
   const R gamma = (R)a.gamma;
@@ -368,8 +386,8 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
   R pV[NV], pVLn[NV], pF[NV], pCm = R(0);
   {
     R vm[NV], v0[NV], vp[NV];
-    load_cell<NV>(a.V, n, rb + wrapi(nx - 2, nx), vm);
-    load_cell<NV>(a.V, n, rb + (nx - 1), v0);
+    load_cell<NV>(a.V, n, rb + gidx(-2, nx, ob, 0), vm);
+    load_cell<NV>(a.V, n, rb + gidx(-1, nx, ob, 0), v0);
     load_cell<NV>(a.V, n, rb + 0, vp);
     R pVR[NV];
 #pragma unroll
@@ -395,8 +413,8 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
     const int fc = f < nx ? f : nx - 1;
 #pragma unroll
     for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][nv][tid], a.V + nv * n + rb + fc);
-    if (lane == 31 || f + 1 >= nx) {
-      const int fp = wrapi(fc + 1, nx);
+    if (lane == 31 || f + 1 >= nf) {
+      const int fp = gidx(fc + 1, nx, ob, 0);
 #pragma unroll
       for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][NV + nv][tid], a.V + nv * n + rb + fp);
     }
@@ -405,13 +423,13 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
   };
   stage_chunk(0, 0);
   int buf = 0;
-  for (int c0 = 0; c0 < nx; c0 += 32, buf ^= 1) {
+  for (int c0 = 0; c0 < nf; c0 += 32, buf ^= 1) {
     const int f = c0 + lane;
-    const bool act = f < nx;
-    stage_chunk(c0 + 32 < nx ? c0 + 32 : c0, buf ^ 1);   // prefetch the next chunk
+    const bool act = f < nf;
+    stage_chunk(c0 + 32 < nf ? c0 + 32 : c0, buf ^ 1);   // prefetch the next chunk
     cp_async_wait1();
     R Vc[NV], Vm1[NV], Vp1[NV], vL[NV], vR[NV], vLn[NV];
-    const bool selfp1 = (lane == 31) || (f + 1 >= nx);
+    const bool selfp1 = (lane == 31) || (f + 1 >= nf);
 #pragma unroll
     for (int nv = 0; nv < NV; nv++) {
       Vc[nv] = (R)stg[buf][nv][tid];
@@ -475,8 +493,9 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
     pCm = __shfl_sync(FULL, cm, 31);
   }
   cp_async_wait0();
-  // cell nx-1 uses F[nx-1] (lane (nx-1)%32 of the last chunk) and F[nx] = F[0]
-  {
+  // periodic: cell nx-1 uses F[nx-1] (lane (nx-1)%32 of the last chunk) and
+  // F[nx] = F[0]; with an outflow high side face nx was solved in the loop
+  if (nf == nx) {
     R F0[NV];
 #pragma unroll
     for (int nv = 0; nv < NV; nv++) F0[nv] = __shfl_sync(FULL, fF[nv], 0);
@@ -521,22 +540,22 @@ __device__ __forceinline__ void sweep_m_col_ppm(const StageArgs<CTT>& a, const G
     const int m0 = seg * S;
     const int m1 = min(m0 + S, nd);
     auto stage = [&](int mcell, int mface, int b) {
-      const long long cc = base + (long long)wrapi(mcell, nd) * stride;
+      const long long cc = base + (long long)gidx(mcell, nd, g.outflow, DIR) * stride;
 #pragma unroll
       for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][nv][tid], a.V + nv * n + cc);
       if constexpr (PHYS != PHYS_HD)
-        cp_async8(&stg[b][NV][tid], a.Bs[DIR] + base + (long long)wrapi(mface, nd) * stride);
+        cp_async8(&stg[b][NV][tid], a.Bs[DIR] + base + (long long)gidx(mface, nd, g.outflow, DIR) * stride);
       cp_async_commit();
     };
     stage(m0 + 2, m0, 0);
     R W0[NV], W1[NV], W2[NV], Fm[NV], vLn[NV], Fp[NV], cmp = R(0);
     {
       R q3[NV], q2[NV];
-      load_cell<NV>(a.V, n, base + wrapi(m0 - 3, nd) * stride, q3);
-      load_cell<NV>(a.V, n, base + wrapi(m0 - 2, nd) * stride, q2);
-      load_cell<NV>(a.V, n, base + wrapi(m0 - 1, nd) * stride, W0);
+      load_cell<NV>(a.V, n, base + gidx(m0 - 3, nd, g.outflow, DIR) * stride, q3);
+      load_cell<NV>(a.V, n, base + gidx(m0 - 2, nd, g.outflow, DIR) * stride, q2);
+      load_cell<NV>(a.V, n, base + gidx(m0 - 1, nd, g.outflow, DIR) * stride, W0);
       load_cell<NV>(a.V, n, base + (long long)m0 * stride, W1);
-      load_cell<NV>(a.V, n, base + wrapi(m0 + 1, nd) * stride, W2);
+      load_cell<NV>(a.V, n, base + gidx(m0 + 1, nd, g.outflow, DIR) * stride, W2);
       R vrp[NV];
 #pragma unroll
       for (int nv = 0; nv < NV; nv++) {
@@ -579,7 +598,7 @@ __device__ __forceinline__ void sweep_m_col_ppm(const StageArgs<CTT>& a, const G
       for (int nv = 0; nv < NV; nv++)
         if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) err |= ERR_NAN | ERR_QUIT;
       if constexpr (PHYS != PHYS_HD) {
-        if (m < m1) store_ct(a, DIR, base + (long long)wrapi(m, nd) * stride, ct);
+        if (m < m1) store_ct(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
       }
       if (m > m0)
         cell_update<PHYS, NV, NDIM>(a, n, base + (long long)(m - 1) * stride, Fp, F, cmp, cm,
@@ -621,19 +640,19 @@ __device__ __forceinline__ void sweep_m_col(const StageArgs<CTT>& a, const Grid3
     const int m0 = seg * S;
     const int m1 = min(m0 + S, nd);
     auto stage = [&](int mcell, int mface, int b) {
-      const long long cc = base + (long long)wrapi(mcell, nd) * stride;
+      const long long cc = base + (long long)gidx(mcell, nd, g.outflow, DIR) * stride;
 #pragma unroll
       for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][nv][tid], a.V + nv * n + cc);
       if constexpr (PHYS != PHYS_HD)
-        cp_async8(&stg[b][NV][tid], a.Bs[DIR] + base + (long long)wrapi(mface, nd) * stride);
+        cp_async8(&stg[b][NV][tid], a.Bs[DIR] + base + (long long)gidx(mface, nd, g.outflow, DIR) * stride);
       cp_async_commit();
     };
     stage(m0 + 1, m0, 0);
     R Vp[NV], Vc[NV], vLn[NV], Fp[NV], cmp = R(0);
     {
       R vmm[NV];
-      load_cell<NV>(a.V, n, base + wrapi(m0 - 2, nd) * stride, vmm);
-      load_cell<NV>(a.V, n, base + wrapi(m0 - 1, nd) * stride, Vp);
+      load_cell<NV>(a.V, n, base + gidx(m0 - 2, nd, g.outflow, DIR) * stride, vmm);
+      load_cell<NV>(a.V, n, base + gidx(m0 - 1, nd, g.outflow, DIR) * stride, Vp);
       load_cell<NV>(a.V, n, base + (long long)m0 * stride, Vc);
       R vrp[NV];
 #pragma unroll
@@ -671,7 +690,7 @@ __device__ __forceinline__ void sweep_m_col(const StageArgs<CTT>& a, const Grid3
       for (int nv = 0; nv < NV; nv++)
         if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) err |= ERR_NAN | ERR_QUIT;
       if constexpr (PHYS != PHYS_HD) {
-        if (m < m1) store_ct(a, DIR, base + (long long)wrapi(m, nd) * stride, ct);
+        if (m < m1) store_ct(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
       }
       if (m > m0)
         cell_update<PHYS, NV, NDIM>(a, n, base + (long long)(m - 1) * stride, Fp, F, cmp, cm,

@@ -56,7 +56,7 @@ static StageArgs<CTT> make_args(const StageDesc& d) {
 template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM>
 static void run_stage(const StageArgs<CTT>& a, const GridDims& gd, int seg, cudaStream_t s,
                       cudaEvent_t* ev) {
-  Grid3 g{gd.nx, gd.ny, gd.nz, gd.n};
+  Grid3 g{gd.nx, gd.ny, gd.nz, gd.n, gd.outflow};
   int kidx = 0;
   auto pre = [&]() { if (ev) cudaEventRecord(ev[2 * kidx], s); };
   auto post = [&]() { if (ev) cudaEventRecord(ev[2 * kidx + 1], s); kidx++; };

@@ -31,6 +31,7 @@ struct StageDesc {
 struct GridDims {
   int nx, ny, nz;
   long long n;
+  unsigned outflow = 0u;  // bit 2d / 2d+1: low / high side of direction d is outflow
 };
 
 struct SchemeKey {

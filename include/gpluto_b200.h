@@ -55,8 +55,9 @@ enum { GP_LIM_FLAT = 0, GP_LIM_MINMOD = 1, GP_LIM_VANLEER = 2, GP_LIM_MC = 3 };
 enum { GP_RS_HLL = 0, GP_RS_HLLC = 1, GP_RS_HLLD = 2 };
 /* CT_EMF_AVERAGE (Src/MHD/CT/ct.hpp:19-27) */
 enum { GP_CT_UCT_HLL = 0, GP_CT_UCT_HLLD = 1 };
-/* [Boundary] types (Src/boundary.cpp) */
-enum { GP_BC_PERIODIC = 0 };
+/* [Boundary] types (Src/boundary.cpp): periodic, or outflow (zero-gradient
+   ghost copy, OutflowBoundary Src/boundary.cpp:677-780; built for HD) */
+enum { GP_BC_PERIODIC = 0, GP_BC_OUTFLOW = 1 };
 /* RECONSTRUCTION (definitions.hpp): LINEAR (PLM with LIMITER) or PARABOLIC
    (PPM, Src/States/ppm_states.cpp) */
 enum { GP_REC_LINEAR = 0, GP_REC_PARABOLIC = 1 };

@@ -657,6 +657,19 @@ static void Boundary(orc_t *o) {
     int shift = beg ? o->c.n[d] : -o->c.n[d];
     if (beg) { lo[d] = 0; hi[d] = o->beg[d]-1; }
     else     { lo[d] = o->end[d]+1; hi[d] = o->nt[d]-1; }
+    if ((o->c.outflow >> side) & 1) {
+      /* OutflowBoundary, Src/boundary.cpp:677-708: every ghost cell copies
+         the interior cell next to the boundary (HD: no staggered fields) */
+      int i0 = beg ? o->beg[d] : o->end[d];
+      for (nv = 0; nv < o->nvar; nv++)
+        for (k = lo[2]; k <= hi[2]; k++)
+        for (j = lo[1]; j <= hi[1]; j++)
+        for (i = lo[0]; i <= hi[0]; i++) {
+          int s[3] = {i, j, k}; s[d] = i0;
+          *VC(o, o->Vc, nv, i, j, k) = *VC(o, o->Vc, nv, s[0], s[1], s[2]);
+        }
+      continue;
+    }
     for (nv = 0; nv < o->nvar; nv++)
       for (k = lo[2]; k <= hi[2]; k++)
       for (j = lo[1]; j <= hi[1]; j++)

@@ -19,6 +19,7 @@ typedef struct {
   double gamma;
   double dx[3];
   double cfl, cfl_max_var;
+  int outflow;   /* bit 2d / 2d+1: low / high side of direction d is OUTFLOW (HD) */
 } orc_cfg;
 
 void    *orc_create(const orc_cfg *cfg);

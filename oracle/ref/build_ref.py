@@ -65,6 +65,7 @@ class RefConfig:
     cfl_max_var: float = 1.1
     first_dt: float = 1.0e-4
     reconstruction: str = "LINEAR"
+    bc: tuple = ("periodic", "periodic", "periodic")   # per direction, both sides
 
     def definitions(self) -> str:
         lines = [
@@ -118,7 +119,7 @@ class RefConfig:
             f"first_dt         {self.first_dt!r}", "",
             "[Solver]", "", f"Solver           {self.solver}", "",
             "[Boundary]", "",
-            *[f"X{d}-{s}        periodic" for d in (1, 2, 3) for s in ("beg", "end")], "",
+            *[f"X{d}-{s}        {self.bc[d - 1]}" for d in (1, 2, 3) for s in ("beg", "end")], "",
             "[Static Grid Output]", "",
             "uservar    0",
             "dbl       -1.0  -1   single_file",

@@ -75,6 +75,19 @@ CASES = {
     "hd2d_ppm_hllc": (ics.hd_turbulence, dict(n=(32, 24), seed=23),
                       dict(physics="HD", ndim=2, limiter="MC_LIM", solver="hllc",
                            cfl=0.4, first_dt=1e-4, reconstruction="PARABOLIC"), 20),
+    # outflow boundaries (HD): x only, all sides with PPM, all sides with VL/HLL
+    "hd2d_mc_hllc_outflowx": (ics.hd_turbulence, dict(n=(33, 24), seed=41),
+                              dict(physics="HD", ndim=2, limiter="MC_LIM", solver="hllc",
+                                   cfl=0.4, first_dt=1e-4,
+                                   bc=("outflow", "periodic", "periodic")), 20),
+    "hd3d_ppm_hllc_outflow": (ics.hd_turbulence, dict(n=(12, 10, 9), seed=42),
+                              dict(physics="HD", ndim=3, limiter="MC_LIM", solver="hllc",
+                                   cfl=0.4, first_dt=1e-4, reconstruction="PARABOLIC",
+                                   bc=("outflow", "outflow", "outflow")), 10),
+    "hd2d_vl_hll_outflow": (ics.hd_turbulence, dict(n=(24, 32), seed=43),
+                            dict(physics="HD", ndim=2, limiter="VANLEER_LIM", solver="hll",
+                                 cfl=0.4, first_dt=1e-4,
+                                 bc=("outflow", "outflow", "periodic")), 20),
     "rmhd3d_ppm_hlld_ucthll": (ics.rmhd3d_turbulence,
                                dict(n=(8, 10, 12), seed=24, lorentz_max=3.0),
                                dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
@@ -98,6 +111,15 @@ def _as2d(st):
     return ics.PrimState(st.physics, 2, (st.shape[0], st.shape[1], 1), st.gamma, V, Bs)
 
 
+def outflow_mask(rc: dict) -> int:
+    """Bits 2d and 2d+1 set for each direction d with outflow sides."""
+    m = 0
+    for d, t in enumerate(rc.get("bc", ("periodic",) * 3)):
+        if t == "outflow" and d < rc["ndim"]:
+            m |= 3 << (2 * d)
+    return m
+
+
 def make(name: str) -> str:
     gen, kw, rc, nsteps = CASES[name]
     st = gen(**kw)
@@ -119,7 +141,7 @@ def make(name: str) -> str:
         V=d.V, U=d.U, Bs=np.array(d.Bs) if d.Bs else np.zeros(0), dt=d.dt, nsteps=nsteps,
         limiter=rc["limiter"], solver=rc["solver"], ct=rc.get("ct_emf", "none"),
         cfl=rc["cfl"], cfl_max_var=1.1, first_dt=rc["first_dt"],
-        reconstruction=rc.get("reconstruction", "LINEAR"))
+        reconstruction=rc.get("reconstruction", "LINEAR"), outflow=outflow_mask(rc))
     return out
 
 

@@ -40,5 +40,6 @@ class Golden:
         self.cfl_max_var = float(z["cfl_max_var"])
         self.first_dt = float(z["first_dt"])
         self.reconstruction = str(z["reconstruction"]) if "reconstruction" in z else "LINEAR"
+        self.outflow = int(z["outflow"]) if "outflow" in z else 0
         if self.reconstruction == "PARABOLIC":
             self.limiter = "ppm"

@@ -21,16 +21,17 @@ def rel_linf(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-def make_solver(st, limiter, solver, ct, cfl=0.4, cfl_max_var=1.1, precision=api.FP64):
+def make_solver(st, limiter, solver, ct, cfl=0.4, cfl_max_var=1.1, precision=api.FP64,
+                outflow=0):
     sch = api.Scheme(physics=st.physics, limiter=limiter, riemann=solver, ct_emf=ct,
                      precision=precision, gamma=st.gamma, cfl=cfl, cfl_max_var=cfl_max_var)
-    return api.Solver.from_state(st, sch)
+    return api.Solver.from_state(st, sch, outflow=outflow)
 
 
 @pytest.mark.parametrize("name", [n for n in gu.names() if not n.startswith("rmhd")])
 def test_gpu_matches_reference_fixture_bitwise(name):
     g = gu.Golden(name)
-    s = make_solver(g.ic, g.limiter, g.solver, g.ct, g.cfl, g.cfl_max_var)
+    s = make_solver(g.ic, g.limiter, g.solver, g.ct, g.cfl, g.cfl_max_var, outflow=g.outflow)
     dt_after, hist, out = s.run(g.nsteps, g.first_dt)
     V, U, Bs = s.download()
     assert out.err_bits & api.ERR_QUIT == 0
@@ -76,6 +77,52 @@ def test_gpu_matches_oracle_bitwise(case):
     np.testing.assert_array_equal(U, Uo)
     for a, b in zip(Bs, Bo):
         np.testing.assert_array_equal(a, b)
+
+
+OUTFLOW_CASES = [
+    # (generator, kwargs, limiter, solver, outflow mask, nsteps): rows of 33
+    # and 65 cells (the extra boundary face starts a new chunk), a row
+    # shorter than a warp, both PLM and PPM
+    (ics.hd_turbulence, dict(n=(32, 20), seed=51), "mc", "hllc", 0b0011, 15),
+    (ics.hd_turbulence, dict(n=(65, 7), seed=52), "ppm", "hllc", 0b1111, 12),
+    (ics.hd_turbulence, dict(n=(6, 33), seed=53), "vl", "hll", 0b1100, 12),
+    (ics.hd_turbulence, dict(n=(13, 11, 9), seed=54), "ppm", "hll", 0b111111, 8),
+    (ics.hd_turbulence, dict(n=(31, 10, 12), seed=55), "mc", "hllc", 0b110000, 8),
+]
+
+
+@pytest.mark.parametrize("case", range(len(OUTFLOW_CASES)))
+def test_gpu_outflow_matches_oracle_bitwise(case):
+    gen, kw, lim, rs, ob, nsteps = OUTFLOW_CASES[case]
+    st = gen(**kw)
+    o = orc.Oracle(st, limiter=lim, solver=rs, ct="uct_hll", outflow=ob)
+    ohist, oerr = o.run(nsteps, 1e-4)
+    Vo, Uo, _ = o.state()
+    s = make_solver(st, lim, rs, "uct_hll", outflow=ob)
+    dt_after, hist, out = s.run(nsteps, 1e-4)
+    V, U, _ = s.download()
+    assert out.err_bits == oerr
+    np.testing.assert_array_equal(hist, ohist[:-1])
+    np.testing.assert_array_equal(V, Vo)
+    np.testing.assert_array_equal(U, Uo)
+
+
+def test_outflow_reference_layout_ghosts_copy_the_boundary_cells():
+    st = ics.hd_turbulence(n=(20, 12), seed=56)
+    s = make_solver(st, "mc", "hllc", "uct_hll", outflow=0b0011)
+    s.run(3, 1e-4)
+    V, _, _ = s.download()
+    cshape, _ = s.reference_shapes()
+    Vr = np.empty(cshape)
+    api._check(api.lib().gp_download_state(s._h, api.LAYOUT_REFERENCE, None, api._dp(Vr),
+                                           None, None, None))
+    g = s.nghost
+    inner = Vr[:, :, g:-g, g:-g]
+    np.testing.assert_array_equal(inner, V)
+    for k in range(g):       # x: outflow copies of the boundary columns
+        np.testing.assert_array_equal(Vr[:, :, g:-g, k], V[:, :, :, 0])
+        np.testing.assert_array_equal(Vr[:, :, g:-g, -1 - k], V[:, :, :, -1])
+    np.testing.assert_array_equal(Vr[:, :, :g, g:-g], V[:, :, -g:, :])   # y: periodic
 
 
 def test_host_dt_path_equals_device_dt_path():

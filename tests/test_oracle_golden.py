@@ -16,7 +16,7 @@ import oracle as orc
 def test_oracle_matches_reference_bitwise(name):
     g = gu.Golden(name)
     o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct,
-                   cfl=g.cfl, cfl_max_var=g.cfl_max_var)
+                   cfl=g.cfl, cfl_max_var=g.cfl_max_var, outflow=g.outflow)
     hist, err = o.run(g.nsteps, g.first_dt)
     V, U, Bs = o.state()
     assert err & (1 << 15) == 0, f"oracle raised ERR_QUIT ({err:#x})"
