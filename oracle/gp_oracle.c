@@ -648,6 +648,53 @@ static void AverageStaggered(orc_t *o, int ib, int ie, int jb, int je, int kb, i
   }
 }
 
+/* Normal staggered field in the ghost zone of an outflow side from
+   div B = 0, marching away from the domain: CT_FillStaggeredFields,
+   Src/MHD/CT/ct_fill_mag_field.cpp:96-330, with the Cartesian face areas of
+   Src/set_geometry.cpp:124,147,165 (uniform grid).  The loops run over the
+   whole ghosted extent of the other directions. */
+static void CT_FillNormal(orc_t *o, int d, int beg) {
+  const int ndim = o->c.ndim;
+  const double dx = o->c.dx[0], dy = o->c.dx[1], dz = o->c.dx[2];
+  double A[3];
+  if (ndim == 2) { A[0] = 1.0*dy; A[1] = dx*1.0; A[2] = 0.0; }
+  else           { A[0] = 1.0*dy*dz; A[1] = dx*1.0*dz; A[2] = dx*dy*1.0; }
+  int lo[3] = {0, 0, 0}, hi[3] = {o->nt[0]-1, o->nt[1]-1, o->nt[2]-1};
+  int i, j, k;
+  /* a loop over the two transverse directions; the normal index marches */
+  int a = (d == 0) ? 1 : 0, b = (d == 2) ? 1 : 2;
+  int t1, t2, m;
+  for (t2 = lo[b]; t2 <= hi[b]; t2++)
+  for (t1 = lo[a]; t1 <= hi[a]; t1++) {
+    int mfirst = beg ? o->beg[d]-1 : o->end[d]+1;
+    int mlast  = beg ? 0 : o->nt[d]-1;
+    int step = beg ? -1 : 1;
+    for (m = mfirst; beg ? (m >= mlast) : (m <= mlast); m += step) {
+      int ijk[3];
+      ijk[d] = m; ijk[a] = t1; ijk[b] = t2;
+      i = ijk[0]; j = ijk[1]; k = ijk[2];
+      double dB[3] = {0.0, 0.0, 0.0};
+      int c;
+      for (c = 0; c < ndim; c++) {
+        int di = (c == 0), dj = (c == 1), dk = (c == 2);
+        double Bp = o->Vs[c][SI(o,c,i+di,j+dj,k+dk)], Bm = o->Vs[c][SI(o,c,i,j,k)];
+        dB[c] = A[c]*Bp - A[c]*Bm;
+      }
+      int di = (d == 0), dj = (d == 1), dk = (d == 2);
+      /* the two transverse contributions in the reference's order */
+      double t_a = dB[a], t_b = (b < ndim) ? dB[b] : 0.0;
+      if (d == 2) { t_a = dB[0]; t_b = dB[1]; }
+      if (beg) {
+        double Bp = o->Vs[d][SI(o,d,i+di,j+dj,k+dk)];
+        o->Vs[d][SI(o,d,i,j,k)] = (A[d]*Bp + t_a + t_b)/A[d];
+      } else {
+        double Bm = o->Vs[d][SI(o,d,i,j,k)];
+        o->Vs[d][SI(o,d,i+di,j+dj,k+dk)] = (A[d]*Bm - (t_a + t_b))/A[d];
+      }
+    }
+  }
+}
+
 static void Boundary(orc_t *o) {
   int side, nv, i, j, k;
   int isMHD = (o->c.physics != ORC_HD);
@@ -658,8 +705,9 @@ static void Boundary(orc_t *o) {
     if (beg) { lo[d] = 0; hi[d] = o->beg[d]-1; }
     else     { lo[d] = o->end[d]+1; hi[d] = o->nt[d]-1; }
     if ((o->c.outflow >> side) & 1) {
-      /* OutflowBoundary, Src/boundary.cpp:677-708: every ghost cell copies
-         the interior cell next to the boundary (HD: no staggered fields) */
+      /* OutflowBoundary, Src/boundary.cpp:677-780: every ghost cell copies
+         the interior cell next to the boundary; the tangential staggered
+         fields are copied the same way (BOXJ/BOXK loops, one face wider) */
       int i0 = beg ? o->beg[d] : o->end[d];
       for (nv = 0; nv < o->nvar; nv++)
         for (k = lo[2]; k <= hi[2]; k++)
@@ -668,6 +716,23 @@ static void Boundary(orc_t *o) {
           int s[3] = {i, j, k}; s[d] = i0;
           *VC(o, o->Vc, nv, i, j, k) = *VC(o, o->Vc, nv, s[0], s[1], s[2]);
         }
+      if (isMHD) {
+        int c;
+        for (c = 0; c < o->c.ndim; c++) {
+          if (c == d) continue;
+          int h[3] = {hi[0], hi[1], hi[2]};
+          h[c] += 1;
+          for (k = lo[2]; k <= h[2]; k++)
+          for (j = lo[1]; j <= h[1]; j++)
+          for (i = lo[0]; i <= h[0]; i++) {
+            int s[3] = {i, j, k}; s[d] = i0;
+            o->Vs[c][SI(o,c,i,j,k)] = o->Vs[c][SI(o,c,s[0],s[1],s[2])];
+          }
+        }
+        CT_FillNormal(o, d, beg);
+        /* Src/boundary.cpp:285-307: ghost cell B from faces, copied to Vc */
+        AverageStaggered(o, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], 1);
+      }
       continue;
     }
     for (nv = 0; nv < o->nvar; nv++)

@@ -88,6 +88,28 @@ CASES = {
                             dict(physics="HD", ndim=2, limiter="VANLEER_LIM", solver="hll",
                                  cfl=0.4, first_dt=1e-4,
                                  bc=("outflow", "outflow", "periodic")), 20),
+    # outflow boundaries with constrained transport (MHD, RMHD)
+    "mhd2d_mc_hlld_ucthlld_outflowx": (ics.mhd2d_turbulence, dict(n=(32, 24), seed=61),
+                                       dict(physics="MHD", ndim=2, limiter="MC_LIM",
+                                            solver="hlld", ct_emf="UCT_HLLD", cfl=0.4,
+                                            first_dt=1e-4,
+                                            bc=("outflow", "periodic", "periodic")), 20),
+    "mhd3d_mc_hlld_ucthlld_outflow": (ics.mhd3d_turbulence, dict(n=(12, 10, 9), seed=62),
+                                      dict(physics="MHD", ndim=3, limiter="MC_LIM",
+                                           solver="hlld", ct_emf="UCT_HLLD", cfl=0.4,
+                                           first_dt=1e-4,
+                                           bc=("outflow", "outflow", "outflow")), 10),
+    "mhd2d_ppm_hlld_ucthlld_outflow": (ics.mhd2d_turbulence, dict(n=(24, 28), seed=63),
+                                       dict(physics="MHD", ndim=2, limiter="MC_LIM",
+                                            solver="hlld", ct_emf="UCT_HLLD", cfl=0.4,
+                                            first_dt=1e-4, reconstruction="PARABOLIC",
+                                            bc=("outflow", "outflow", "periodic")), 16),
+    "rmhd3d_mc_hlld_ucthll_outflowz": (ics.rmhd3d_turbulence,
+                                       dict(n=(8, 10, 12), seed=64, lorentz_max=3.0),
+                                       dict(physics="RMHD", ndim=3, limiter="MC_LIM",
+                                            solver="hlld", ct_emf="UCT_HLL", cfl=0.3,
+                                            first_dt=1e-4,
+                                            bc=("periodic", "periodic", "outflow")), 8),
     "rmhd3d_ppm_hlld_ucthll": (ics.rmhd3d_turbulence,
                                dict(n=(8, 10, 12), seed=24, lorentz_max=3.0),
                                dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",

@@ -22,10 +22,10 @@ def rel_linf(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-def solver(st, lim, rs, cfl=0.3, precision=api.FP64):
+def solver(st, lim, rs, cfl=0.3, precision=api.FP64, outflow=0):
     sch = api.Scheme(physics=api.RMHD, limiter=lim, riemann=rs, ct_emf="uct_hll",
                      precision=precision, gamma=st.gamma, cfl=cfl)
-    return api.Solver.from_state(st, sch)
+    return api.Solver.from_state(st, sch, outflow=outflow)
 
 
 def deviation(U, G):
@@ -53,11 +53,14 @@ def test_rmhd_fp64_matches_reference_fixture(name):
     floors 1e-12 / 1e-11) and lose at most 1% more cells beyond 1e-10.
     The dt sequence must agree to 1e-12."""
     g = gu.Golden(name)
+    if g.outflow:
+        pytest.skip("outflow with constrained transport is not built on the GPU yet")
     spread = []
     try:
         for nudge in (1, -1):
             orc.set_ulp_nudge(nudge)
-            o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct, cfl=g.cfl)
+            o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct, cfl=g.cfl,
+                           outflow=g.outflow)
             o.run(g.nsteps, g.first_dt)
             spread.append(deviation(o.state()[1], g.U))
     finally:
@@ -66,7 +69,7 @@ def test_rmhd_fp64_matches_reference_fixture(name):
     frac_ref = min(x[1] for x in spread)
     linf_ref = max(x[2] for x in spread)
 
-    s = solver(g.ic, g.limiter, g.solver, g.cfl)
+    s = solver(g.ic, g.limiter, g.solver, g.cfl, outflow=g.outflow)
     _, hist, out = s.run(g.nsteps, g.first_dt)
     V, U, Bs = s.download()
     assert out.err_bits & api.ERR_QUIT == 0

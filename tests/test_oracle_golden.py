@@ -29,7 +29,7 @@ def test_oracle_matches_reference_bitwise(name):
 
 def test_oracle_divb_roundoff():
     g = gu.Golden("mhd3d_mc_hlld_ucthlld")
-    o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct)
+    o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct, outflow=g.outflow)
     o.run(g.nsteps, g.first_dt)
     _, _, Bs = o.state()
     nx, ny, nz = g.shape
@@ -40,7 +40,8 @@ def test_oracle_divb_roundoff():
 
 
 def _run_state(g):
-    o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct, cfl=g.cfl)
+    o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct, cfl=g.cfl,
+                   outflow=g.outflow)
     o.run(g.nsteps, g.first_dt)
     return o.state()[1]
 
