@@ -66,43 +66,173 @@ __global__ void dt_update_kernel(StepScalars* sc, double ndim, double cfl, doubl
   sc->invdt_bits = 0ull;
 }
 
-// interior <-> reference (ghosted) layout for one 3-D array
+constexpr int kBX1 = 4;  // first field component (Src/MHD/mhd.hpp:21-41, Src/RMHD/rmhd.hpp:21-42)
+
+// Device array extents: the domain (n*) sits at offset l* inside the
+// allocated extents p* (p = n, l = 0 unless the direction is padded).
+struct Pad {
+  int nx, ny, nz, px, py, pz, lx, ly, lz;
+};
+
+// host layout with extents s* and domain offset o* (reference layout, or
+// interior layout with s = n, o = 0) -> domain of the device array
 __global__ void gather_kernel(const double* __restrict__ src, double* __restrict__ dst,
-                              int nvar, int sx, int sy, int sz, int ox, int oy, int oz,
-                              int nx, int ny, int nz) {
-  long long n = (long long)nx * ny * nz;
+                              int nvar, int sx, int sy, int sz, int ox, int oy, int oz, Pad p) {
+  long long n = (long long)p.nx * p.ny * p.nz;
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n * nvar) return;
   int nv = (int)(t / n);
   long long c = t - (long long)nv * n;
-  int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+  int i = (int)(c % p.nx), j = (int)((c / p.nx) % p.ny), k = (int)(c / ((long long)p.nx * p.ny));
   long long s = (long long)(i + ox) + (long long)sx * ((j + oy) + (long long)sy * (k + oz));
-  dst[t] = src[(long long)nv * sx * sy * sz + s];
+  long long d = (long long)(i + p.lx) + (long long)p.px * ((j + p.ly) + (long long)p.py * (k + p.lz));
+  dst[(long long)nv * p.px * p.py * p.pz + d] = src[(long long)nv * sx * sy * sz + s];
 }
 
-// ghost index of the reference layout: periodic wrap, or the nearest
-// interior cell on an outflow side
-__device__ int ghost_src(int i, int n, unsigned outflow, int d) {
-  if (i < 0 && ((outflow >> (2 * d)) & 1u)) return 0;
-  if (i >= n && ((outflow >> (2 * d + 1)) & 1u)) return n - 1;
-  return (i % n + n) % n;
+// device index of host-layout position i (domain-relative) along d: with
+// `own` a padded direction reads its own ghost cells; otherwise periodic
+// wrap, or the nearest domain cell on an outflow side
+__device__ int ghost_src(int i, int n, int l, int own, unsigned clamp, int d) {
+  if (own && l > 0) return i + l;
+  if (i < 0 && ((clamp >> (2 * d)) & 1u)) return l;
+  if (i >= n && ((clamp >> (2 * d + 1)) & 1u)) return l + n - 1;
+  return (i % n + n) % n + l;
 }
 
-// fill a ghosted array from the interior the way Boundary() fills Vc: periodic
-// wrap, or the zero-gradient copy on outflow sides; `stag` adds the extra face
-// along that dir.
+// device array -> host layout with extents s* and domain offset o*; the
+// ghost zones come out the way Boundary() fills them.  `clamp` lists the
+// outflow sides filled by copying the nearest domain cell.
 __global__ void scatter_kernel(const double* __restrict__ src, double* __restrict__ dst,
-                               int nvar, int sx, int sy, int sz, int ox, int oy, int oz,
-                               int nx, int ny, int nz, unsigned outflow) {
+                               int nvar, int sx, int sy, int sz, int ox, int oy, int oz, Pad p,
+                               unsigned clamp, int own) {
   long long ns = (long long)sx * sy * sz;
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ns * nvar) return;
   int nv = (int)(t / ns);
   long long s = t - (long long)nv * ns;
   int i = (int)(s % sx), j = (int)((s / sx) % sy), k = (int)(s / ((long long)sx * sy));
-  int ii = ghost_src(i - ox, nx, outflow, 0), jj = ghost_src(j - oy, ny, outflow, 1),
-      kk = ghost_src(k - oz, nz, outflow, 2);
-  dst[t] = src[(long long)nv * nx * ny * nz + ii + (long long)nx * (jj + (long long)ny * kk)];
+  int ii = ghost_src(i - ox, p.nx, p.lx, own, clamp, 0),
+      jj = ghost_src(j - oy, p.ny, p.ly, own, clamp, 1),
+      kk = ghost_src(k - oz, p.nz, p.lz, own, clamp, 2);
+  dst[t] = src[(long long)nv * p.px * p.py * p.pz + ii + (long long)p.px * (jj + (long long)p.py * kk)];
+}
+
+// high-side face of a padded direction d (left face of the first ghost cell)
+// from the low-side face: the periodic completion of an interior-layout field
+__global__ void wrap_face_kernel(double* B, Pad p, int d) {
+  const int P[3] = {p.px, p.py, p.pz};
+  const int L[3] = {p.lx, p.ly, p.lz};
+  const int N[3] = {p.nx, p.ny, p.nz};
+  const int a = (d == 0) ? 1 : 0, b = (d == 2) ? 1 : 2;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)P[a] * P[b]) return;
+  int q[3];
+  q[a] = (int)(t % P[a]);
+  q[b] = (int)(t / P[a]);
+  q[d] = L[d];
+  const long long c0 = (long long)q[0] + (long long)P[0] * (q[1] + (long long)P[1] * q[2]);
+  q[d] = L[d] + N[d];
+  const long long c1 = (long long)q[0] + (long long)P[0] * (q[1] + (long long)P[1] * q[2]);
+  B[c1] = B[c0];
+}
+
+// Outflow side of a padded grid with constrained transport (Boundary(),
+// Src/boundary.cpp:184-307 for one side): the ghost cells of the side copy
+// the domain cell next to it (OutflowBoundary, Src/boundary.cpp:677-780),
+// tangential staggered fields likewise; the normal staggered field is
+// marched outward from div B = 0 with the Cartesian face areas
+// (CT_FillStaggeredFields, Src/MHD/CT/ct_fill_mag_field.cpp:96-330); the
+// ghost cells' B is then the average of their faces
+// (Src/MHD/CT/ct_field_average.cpp:175-200).  One thread per transverse
+// position of the side, over the whole padded extent of the other
+// directions; the sides run in the reference's order.  The march reads the
+// tangential faces of the neighbouring positions, so every side takes two
+// launches: the copies (outflow_copy_kernel), then the march and the
+// averages (outflow_march_kernel).
+struct SideGeom {
+  int P[3], L[3], N[3], d, a, b;
+  long long pn;
+  __device__ long long idx(int m, int ia, int ib) const {
+    int q[3];
+    q[d] = m;
+    q[a] = ia;
+    q[b] = ib;
+    return (long long)q[0] + (long long)P[0] * (q[1] + (long long)P[1] * q[2]);
+  }
+};
+
+__device__ __forceinline__ SideGeom side_geom(const Pad& p, int d) {
+  SideGeom s;
+  s.P[0] = p.px; s.P[1] = p.py; s.P[2] = p.pz;
+  s.L[0] = p.lx; s.L[1] = p.ly; s.L[2] = p.lz;
+  s.N[0] = p.nx; s.N[1] = p.ny; s.N[2] = p.nz;
+  s.d = d;
+  s.a = (d == 0) ? 1 : 0;
+  s.b = (d == 2) ? 1 : 2;
+  s.pn = (long long)p.px * p.py * p.pz;
+  return s;
+}
+
+__global__ void outflow_copy_kernel(double* __restrict__ V, int nvar, double* B0, double* B1,
+                                    double* B2, int ndim, Pad p, int d, int beg) {
+  const SideGeom s = side_geom(p, d);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)s.P[s.a] * s.P[s.b]) return;
+  const int ta = (int)(t % s.P[s.a]), tb = (int)(t / s.P[s.a]);
+  double* B[3] = {B0, B1, B2};
+  const int m0 = beg ? s.L[d] : s.L[d] + s.N[d] - 1;      // domain cell next to the side
+  const int g0 = beg ? 0 : s.L[d] + s.N[d], g1 = beg ? s.L[d] - 1 : s.P[d] - 1;  // ghosts
+  const long long c0 = s.idx(m0, ta, tb);
+  for (int g = g0; g <= g1; g++) {
+    const long long c = s.idx(g, ta, tb);
+    for (int nv = 0; nv < nvar; nv++) V[nv * s.pn + c] = V[nv * s.pn + c0];
+    for (int e = 0; e < ndim; e++)
+      if (e != d) B[e][c] = B[e][c0];
+  }
+}
+
+__global__ void outflow_march_kernel(double* __restrict__ V, double* B0, double* B1, double* B2,
+                                     int ndim, Pad p, int d, int beg, double A0, double A1,
+                                     double A2) {
+  const SideGeom s = side_geom(p, d);
+  const int a = s.a, b = s.b;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)s.P[a] * s.P[b]) return;
+  const int ta = (int)(t % s.P[a]), tb = (int)(t / s.P[a]);
+  const int L = s.L[d], N = s.N[d], P = s.P[d];
+  double* B[3] = {B0, B1, B2};
+  const double A[3] = {A0, A1, A2};
+  // transverse difference A_e*(B_e(next along e) - B_e(here)) at ghost cell m
+  auto dB = [&](int e, int m) -> double {
+    if (e >= ndim) return 0.0;
+    int ia = ta, ib = tb;
+    if (e == a) ia = (ta + 1) % s.P[a];
+    else ib = (tb + 1) % s.P[b];
+    return A[e] * B[e][s.idx(m, ia, ib)] - A[e] * B[e][s.idx(m, ta, tb)];
+  };
+  if (beg) {
+    for (int m = L - 1; m >= 0; m--)
+      B[d][s.idx(m, ta, tb)] = (A[d] * B[d][s.idx(m + 1, ta, tb)] + dB(a, m) + dB(b, m)) / A[d];
+  } else {
+    for (int m = L + N; m + 1 < P; m++)
+      B[d][s.idx(m + 1, ta, tb)] = (A[d] * B[d][s.idx(m, ta, tb)] - (dB(a, m) + dB(b, m))) / A[d];
+  }
+  const int g0 = beg ? 0 : L + N, g1 = beg ? L - 1 : P - 1;
+  for (int g = g0; g <= g1; g++) {
+    const long long c = s.idx(g, ta, tb);
+    for (int e = 0; e < ndim; e++) {
+      long long cn;
+      if (e == d) {
+        if (g + 1 >= P) continue;  // the extra padding cell: not a reference ghost
+        cn = s.idx(g + 1, ta, tb);
+      } else if (e == a) {
+        cn = s.idx(g, (ta + 1) % s.P[a], tb);
+      } else {
+        cn = s.idx(g, ta, (tb + 1) % s.P[b]);
+      }
+      V[(kBX1 + e) * s.pn + c] = 0.5 * (B[e][c] + B[e][cn]);
+    }
+  }
 }
 
 bool uniform(const double* dx, int n) {
@@ -141,6 +271,14 @@ struct gp_handle {
   size_t stage_bytes;
   int launches_per_step;
   unsigned outflow;      // outflow sides (bit 2d low, 2d+1 high)
+  // Outflow with constrained transport pads the outflow directions with
+  // ghost cells filled before every stage (S = ghost cells of the scheme,
+  // plus one on the high side so that the outermost ghost's faces exist).
+  bool padded;
+  int lo[3], hi[3];      // padding cells below / above the domain
+  int px, py, pz;        // allocated extents
+  long long pn;          // allocated cells
+  double A[3];           // Cartesian face areas (Src/set_geometry.cpp:124-165)
 };
 
 namespace {
@@ -163,6 +301,43 @@ void free_all(gp_handle* h) {
   cudaFree(h->stage_buf);
 }
 
+Pad pad_of(const gp_handle* h) {
+  return Pad{h->nx, h->ny, h->nz, h->px, h->py, h->pz, h->lo[0], h->lo[1], h->lo[2]};
+}
+
+gp::GridDims grid_dims(const gp_handle* h) {
+  gp::GridDims g{h->px, h->py, h->pz, h->pn, h->padded ? 0u : h->outflow};
+  if (h->padded) {
+    const int n[3] = {h->nx, h->ny, h->nz};
+    for (int d = 0; d < 3; d++) {
+      if (h->lo[d] == 0 && h->hi[d] == 0) continue;  // periodic: every cell counts
+      g.ilo[d] = h->lo[d];
+      g.ihi[d] = h->lo[d] + n[d] - 1;
+      g.glo[d] = 0;                                    // the reference's ghost zone
+      g.ghi[d] = h->lo[d] + n[d] - 1 + h->lo[d];
+    }
+  }
+  return g;
+}
+
+// ghost zones of the outflow sides of a padded grid, sides in the
+// reference's order (Src/boundary.cpp:144-190)
+void fill_outflow(gp_handle* h, double* const* Bs) {
+  const Pad p = pad_of(h);
+  const int P[3] = {h->px, h->py, h->pz};
+  for (int side = 0; side < 2 * h->ndim; side++) {
+    if (!((h->outflow >> side) & 1u)) continue;
+    const int d = side / 2, beg = side % 2 == 0;
+    const int a = (d == 0) ? 1 : 0, b = (d == 2) ? 1 : 2;
+    const long long nt = (long long)P[a] * P[b];
+    const unsigned nb = (unsigned)((nt + 127) / 128);
+    outflow_copy_kernel<<<nb, 128, 0, h->stream>>>(h->V, h->nvar, Bs[0], Bs[1], Bs[2], h->ndim,
+                                                   p, d, beg);
+    outflow_march_kernel<<<nb, 128, 0, h->stream>>>(h->V, Bs[0], Bs[1], Bs[2], h->ndim, p, d,
+                                                    beg, h->A[0], h->A[1], h->A[2]);
+  }
+}
+
 int enqueue_step(gp_handle* h, double* hist, int slot, cudaEvent_t* ev = nullptr) {
   const int b0 = h->bcur, b1 = (h->bcur + 1) % 3, b2 = (h->bcur + 2) % 3;
   const bool mhd = h->scheme.physics != GP_HD;
@@ -183,12 +358,13 @@ int enqueue_step(gp_handle* h, double* hist, int slot, cudaEvent_t* ev = nullptr
   d.err = &h->sc->err;
   const int per_stage = gp::stage_launch_count(h->key);
   auto launch = [&](const gp::StageDesc& sd) {
-    gp::GridDims g{h->nx, h->ny, h->nz, h->n, h->outflow};
+    gp::GridDims g = grid_dims(h);
     cudaEvent_t* e = ev ? ev + (sd.stage - 1) * 2 * per_stage : nullptr;
     return h->mixed ? gp::launch_stage_mixed(sd, g, h->key, h->seg, h->stream, e)
                     : gp::launch_stage_fp64(sd, g, h->key, h->seg, h->stream, e);
   };
   // stage 1: (U^n, B^n) -> (U1, B1)
+  if (h->padded) fill_outflow(h, h->Bs[b0]);
   d.stage = 1;
   d.V = h->V;
   d.Vout = h->V;
@@ -202,6 +378,7 @@ int enqueue_step(gp_handle* h, double* hist, int slot, cudaEvent_t* ev = nullptr
   }
   if (launch(d) != 0) return fail(GP_ERR_UNSUPPORTED, "scheme not compiled");
   // stage 2: (U^n, U1, B^n, B1) -> (U^{n+1} in place of U^n, B^{n+1})
+  if (h->padded) fill_outflow(h, h->Bs[b1]);
   d.stage = 2;
   d.Uc = h->U[1];
   d.Uout = h->U[0];
@@ -275,9 +452,7 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
         return fail(GP_ERR_UNSUPPORTED, "boundary types are periodic or outflow");
       if ((lb == GP_BC_PERIODIC) != (rb == GP_BC_PERIODIC))
         return fail(GP_ERR_INVALID, "a periodic direction needs both sides periodic");
-      if (lb == GP_BC_OUTFLOW && scheme->physics != GP_HD)
-        return fail(GP_ERR_UNSUPPORTED, "outflow boundaries are built for HD "
-                    "(constrained-transport ghost faces are not)");
+
       if (!uniform(grid->dx[d], grid->nint[d] + 2 * grid->nghost))
         return fail(GP_ERR_UNSUPPORTED, "non-uniform grid along %d", d);
     }
@@ -311,7 +486,24 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
     if (grid->lbound[d] == GP_BC_OUTFLOW) h->outflow |= 1u << (2 * d);
     if (grid->rbound[d] == GP_BC_OUTFLOW) h->outflow |= 1u << (2 * d + 1);
   }
-  if (h->n >= (1LL << 31)) {
+  // outflow with constrained transport: pad the outflow directions
+  h->padded = h->outflow != 0 && scheme->physics != GP_HD;
+  {
+    const int S = scheme->reconstruction == GP_REC_PARABOLIC ? 3 : 2;
+    const int nn[3] = {h->nx, h->ny, h->nz};
+    int pp[3];
+    for (int d = 0; d < 3; d++) {
+      const bool pd = h->padded && d < grid->ndim && ((h->outflow >> (2 * d)) & 3u);
+      h->lo[d] = pd ? S : 0;
+      h->hi[d] = pd ? S + 1 : 0;
+      pp[d] = nn[d] + h->lo[d] + h->hi[d];
+    }
+    h->px = pp[0];
+    h->py = pp[1];
+    h->pz = pp[2];
+    h->pn = (long long)h->px * h->py * h->pz;
+  }
+  if (h->pn >= (1LL << 31)) {
     delete h;
     return fail(GP_ERR_UNSUPPORTED, "grids are limited to fewer than 2^31 cells");
   }
@@ -323,6 +515,16 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
                                                : (grid->xend[d] - grid->xbeg[d]) / nn;
     if (!(h->dx[d] > 0.0)) h->dx[d] = 1.0;
   }
+  // Cartesian face areas in the reference's operation order
+  if (h->ndim == 2) {
+    h->A[0] = 1.0 * h->dx[1];
+    h->A[1] = h->dx[0] * 1.0;
+    h->A[2] = 0.0;
+  } else {
+    h->A[0] = 1.0 * h->dx[1] * h->dx[2];
+    h->A[1] = h->dx[0] * 1.0 * h->dx[2];
+    h->A[2] = h->dx[0] * h->dx[1] * 1.0;
+  }
   h->stream = (cudaStream_t)stream;
   h->mixed = scheme->precision == GP_MIXED;
   h->key = gp::SchemeKey{scheme->physics, grid->ndim, scheme->riemann, scheme->ct_emf,
@@ -330,14 +532,14 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
                                                                     : scheme->limiter};
   // pencil segment for the marching sweeps: enough threads to fill 148 SMs
   {
-    long long cols = (long long)h->nx * (h->ndim == 3 ? h->nz : 1);
-    int nd = h->ny;
+    long long cols = (long long)h->px * (h->ndim == 3 ? h->pz : 1);
+    int nd = h->py;
     int seg = 64;
     while (seg > 4 && cols * ((nd + seg - 1) / seg) < 148LL * 1024) seg /= 2;
     h->seg = seg;
   }
-  const size_t cell = sizeof(double) * h->n;
-  const size_t ctb = (h->mixed ? sizeof(float) : sizeof(double)) * h->n;
+  const size_t cell = sizeof(double) * h->pn;
+  const size_t ctb = (h->mixed ? sizeof(float) : sizeof(double)) * h->pn;
   bool ok = true;
   auto alloc = [&](void** p, size_t b) {
     if (ok && cudaMalloc(p, b) != cudaSuccess) ok = false;
@@ -346,7 +548,7 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   alloc((void**)&h->U[1], cell * h->nvar);
   alloc((void**)&h->V, cell * h->nvar);
   // flux differences, inverse-dt terms, UCT data and EMFs: float in the mixed form
-  const size_t fcell = (h->mixed ? sizeof(float) : sizeof(double)) * h->n;
+  const size_t fcell = (h->mixed ? sizeof(float) : sizeof(double)) * h->pn;
   alloc((void**)&h->dU, fcell * h->nvar * 3);
   alloc((void**)&h->Cdt, fcell * 3);
   if (scheme->physics != GP_HD) {
@@ -370,7 +572,18 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   cudaMemsetAsync(h->dU, 0, fcell * h->nvar * 3, h->stream);
   cudaMemsetAsync(h->Cdt, 0, fcell * 3, h->stream);
   h->bcur = 0;
-  h->launches_per_step = 2 * gp::stage_launch_count(h->key) + 1;
+  {
+    int fills = 0;
+    for (int side = 0; side < 2 * h->ndim; side++) fills += 2 * (h->padded && ((h->outflow >> side) & 1u));
+    h->launches_per_step = 2 * (gp::stage_launch_count(h->key) + fills) + 1;
+  }
+  if (h->padded) {  // padding cells start finite
+    cudaMemsetAsync(h->V, 0, cell * h->nvar, h->stream);
+    cudaMemsetAsync(h->U[0], 0, cell * h->nvar, h->stream);
+    cudaMemsetAsync(h->U[1], 0, cell * h->nvar, h->stream);
+    for (int b = 0; b < 3; b++)
+      for (int d = 0; d < h->ndim; d++) cudaMemsetAsync(h->Bs[b][d], 0, cell, h->stream);
+  }
   *out = h;
   return GP_OK;
 }
@@ -403,41 +616,82 @@ static void ref_dims(const gp_handle* h, int stag, int* s, int* o) {
   }
 }
 
+// a padded grid's reference layout must have the scheme's ghost depth
+static int check_ref_ghosts(gp_handle* h) {
+  if (!h->padded) return GP_OK;
+  const int S = h->lo[0] > h->lo[1] ? (h->lo[0] > h->lo[2] ? h->lo[0] : h->lo[2])
+                                    : (h->lo[1] > h->lo[2] ? h->lo[1] : h->lo[2]);
+  if (h->ng != S)
+    return fail(GP_ERR_UNSUPPORTED, "reference layout with outflow needs nghost = %d", S);
+  return GP_OK;
+}
+
 static int upload_one(gp_handle* h, int layout, const double* src, double* dst, int nvar,
                       int stag) {
   const size_t nb = sizeof(double) * h->n * nvar;
-  if (layout == GP_LAYOUT_INTERIOR) {
+  if (layout == GP_LAYOUT_INTERIOR && !h->padded) {
     CUDA_TRY(cudaMemcpyAsync(dst, src, nb, cudaMemcpyHostToDevice, h->stream));
     return GP_OK;
   }
   int s[3], o[3];
-  ref_dims(h, stag, s, o);
+  if (layout == GP_LAYOUT_INTERIOR) {
+    s[0] = h->nx; s[1] = h->ny; s[2] = h->nz;
+    o[0] = o[1] = o[2] = 0;
+  } else {
+    int rc = check_ref_ghosts(h);
+    if (rc) return rc;
+    ref_dims(h, stag, s, o);
+  }
   size_t tot = sizeof(double) * (size_t)s[0] * s[1] * s[2] * nvar;
   int rc = ensure_stage(h, tot);
   if (rc) return rc;
   CUDA_TRY(cudaMemcpyAsync(h->stage_buf, src, tot, cudaMemcpyHostToDevice, h->stream));
-  long long work = h->n * nvar;
+  Pad p = pad_of(h);
+  // a face field of a padded direction also has the high-side boundary face
+  const bool extra = stag >= 0 && h->padded && h->lo[stag] > 0;
+  if (extra && layout == GP_LAYOUT_REFERENCE) {
+    if (stag == 0) p.nx += 1;
+    if (stag == 1) p.ny += 1;
+    if (stag == 2) p.nz += 1;
+  }
+  long long work = (long long)p.nx * p.ny * p.nz * nvar;
   gather_kernel<<<(unsigned)((work + 255) / 256), 256, 0, h->stream>>>(
-      h->stage_buf, dst, nvar, s[0], s[1], s[2], o[0], o[1], o[2], h->nx, h->ny, h->nz);
+      h->stage_buf, dst, nvar, s[0], s[1], s[2], o[0], o[1], o[2], p);
   CUDA_TRY(cudaGetLastError());
+  if (extra && layout == GP_LAYOUT_INTERIOR) {
+    const int P[3] = {h->px, h->py, h->pz};
+    const int a = (stag == 0) ? 1 : 0, b = (stag == 2) ? 1 : 2;
+    const long long nt = (long long)P[a] * P[b];
+    wrap_face_kernel<<<(unsigned)((nt + 127) / 128), 128, 0, h->stream>>>(dst, pad_of(h), stag);
+    CUDA_TRY(cudaGetLastError());
+  }
   return GP_OK;
 }
 
+// `cons` marks the conserved array: its ghost zones are not part of a padded
+// grid's state, so they are given the outflow copy of the domain.
 static int download_one(gp_handle* h, int layout, const double* src, double* dst, int nvar,
-                        int stag) {
+                        int stag, bool cons = false) {
   const size_t nb = sizeof(double) * h->n * nvar;
-  if (layout == GP_LAYOUT_INTERIOR) {
+  if (layout == GP_LAYOUT_INTERIOR && !h->padded) {
     CUDA_TRY(cudaMemcpyAsync(dst, src, nb, cudaMemcpyDeviceToHost, h->stream));
     return GP_OK;
   }
   int s[3], o[3];
-  ref_dims(h, stag, s, o);
+  if (layout == GP_LAYOUT_INTERIOR) {
+    s[0] = h->nx; s[1] = h->ny; s[2] = h->nz;
+    o[0] = o[1] = o[2] = 0;
+  } else {
+    int rc = check_ref_ghosts(h);
+    if (rc) return rc;
+    ref_dims(h, stag, s, o);
+  }
   long long tot = (long long)s[0] * s[1] * s[2] * nvar;
   int rc = ensure_stage(h, sizeof(double) * tot);
   if (rc) return rc;
   scatter_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, h->stream>>>(
-      src, h->stage_buf, nvar, s[0], s[1], s[2], o[0], o[1], o[2], h->nx, h->ny, h->nz,
-      h->outflow);
+      src, h->stage_buf, nvar, s[0], s[1], s[2], o[0], o[1], o[2], pad_of(h), h->outflow,
+      cons ? 0 : 1);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaMemcpyAsync(dst, h->stage_buf, sizeof(double) * tot, cudaMemcpyDeviceToHost,
                            h->stream));
@@ -454,7 +708,7 @@ int gp_upload_state(gp_handle* h, int layout, const double* Uc, const double* Vc
   if (Uc) {
     rc = upload_one(h, layout, Uc, h->U[0], h->nvar, -1);
   } else {
-    rc = gp::launch_prim2cons(h->scheme.physics, h->V, h->U[0], h->n, h->scheme.gamma,
+    rc = gp::launch_prim2cons(h->scheme.physics, h->V, h->U[0], h->pn, h->scheme.gamma,
                               h->stream);
     if (rc) return fail(GP_ERR_UNSUPPORTED, "prim2cons not built for this physics");
   }
@@ -475,7 +729,9 @@ int gp_download_state(gp_handle* h, int layout, double* Uc, double* Vc, double* 
                       double* Vs1, double* Vs2) {
   if (!h) return fail(GP_ERR_INVALID, "null handle");
   int rc;
-  if (Uc && (rc = download_one(h, layout, h->U[0], Uc, h->nvar, -1))) return rc;
+  // ghost zones of the current state, as Boundary() would fill them
+  if (h->padded && layout == GP_LAYOUT_REFERENCE) fill_outflow(h, h->Bs[h->bcur]);
+  if (Uc && (rc = download_one(h, layout, h->U[0], Uc, h->nvar, -1, true))) return rc;
   if (Vc && (rc = download_one(h, layout, h->V, Vc, h->nvar, -1))) return rc;
   if (h->scheme.physics != GP_HD) {
     double* vs[3] = {Vs0, Vs1, Vs2};
@@ -540,6 +796,8 @@ int gp_advance_steps(gp_handle* h, int nsteps, double* dt, double* dt_hist, gp_s
 
 int gp_device_state(gp_handle* h, double** Uc, double** Vc, double** Vs) {
   if (!h) return fail(GP_ERR_INVALID, "null handle");
+  if (h->padded)
+    return fail(GP_ERR_UNSUPPORTED, "the state of a grid with outflow sides is padded");
   if (Uc) *Uc = h->U[0];
   if (Vc) *Vc = h->V;
   if (Vs)

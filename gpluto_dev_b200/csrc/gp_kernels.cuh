@@ -27,13 +27,29 @@
 
 namespace gp {
 
+constexpr int kNoLimit = 0x3fffffff;
+
 struct Grid3 {
   int nx, ny, nz;
   long long n;  // nx*ny*nz
-  // outflow sides: bit 2d = low side of direction d, bit 2d+1 = high side;
-  // every other side is periodic
+  // outflow sides handled by index clamping (HD): bit 2d = low side of
+  // direction d, bit 2d+1 = high side; every other side wraps
   unsigned outflow = 0u;
+  // Grids padded with ghost cells (outflow with constrained transport):
+  // the cells [ilo, ihi] are the domain; [glo, ghi] the cells whose faces
+  // the reference's sweeps also solve (domain plus its ghost zone).  Only
+  // those contribute error bits, and only the domain the CFL maximum.
+  int ilo[3] = {0, 0, 0}, ihi[3] = {kNoLimit, kNoLimit, kNoLimit};
+  int glo[3] = {0, 0, 0}, ghi[3] = {kNoLimit, kNoLimit, kNoLimit};
 };
+
+// whether the face f (along d) of the pencil at transverse cells (ta, tb) is
+// one the reference solves: ta, tb inside the ghosted box, f a domain face
+__device__ __forceinline__ bool face_counts(const Grid3& g, int d, int f, int a, int ta, int b,
+                                            int tb) {
+  return f >= g.ilo[d] && f <= g.ihi[d] + 1 && ta >= g.glo[a] && ta <= g.ghi[a] &&
+         tb >= g.glo[b] && tb <= g.ghi[b];
+}
 
 template <typename CTT>
 struct StageArgs {
@@ -313,10 +329,12 @@ __device__ __forceinline__ void sweep_x_row_ppm(const StageArgs<CTT>& a, const G
       vR[BX1] = Bn;
     }
     CTFace<R> ct;
-    cm = riemann<PHYS, RS, CT, 0>(vL, vR, F, gamma, Bn, ct, err);
+    uint32_t fe = 0;
+    cm = riemann<PHYS, RS, CT, 0>(vL, vR, F, gamma, Bn, ct, fe);
 #pragma unroll
     for (int nv = 0; nv < NV; nv++)
-      if (act && rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) err |= ERR_NAN | ERR_QUIT;
+      if (act && rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) fe |= ERR_NAN | ERR_QUIT;
+    if (face_counts(g, 0, f, 1, row % g.ny, 2, row / g.ny)) err |= fe;
     if constexpr (PHYS != PHYS_HD) {
       if (act) store_ct(a, 0, rb + f, ct);
     }
@@ -458,10 +476,12 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
       vR[BX1] = Bn;
     }
     CTFace<R> ct;
-    cm = riemann<PHYS, RS, CT, 0>(vL, vR, F, gamma, Bn, ct, err);
+    uint32_t fe = 0;
+    cm = riemann<PHYS, RS, CT, 0>(vL, vR, F, gamma, Bn, ct, fe);
 #pragma unroll
     for (int nv = 0; nv < NV; nv++)
-      if (act && rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) err |= ERR_NAN | ERR_QUIT;
+      if (act && rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) fe |= ERR_NAN | ERR_QUIT;
+    if (face_counts(g, 0, f, 1, row % g.ny, 2, row / g.ny)) err |= fe;
     if constexpr (PHYS != PHYS_HD) {
       if (act) store_ct(a, 0, rb + f, ct);
     }
@@ -593,10 +613,12 @@ __device__ __forceinline__ void sweep_m_col_ppm(const StageArgs<CTT>& a, const G
         vR[BX1 + DIR] = Bn;
       }
       CTFace<R> ct;
-      R cm = riemann<PHYS, RS, CT, DIR>(vL, vR, F, gamma, Bn, ct, err);
+      uint32_t fe = 0;
+      R cm = riemann<PHYS, RS, CT, DIR>(vL, vR, F, gamma, Bn, ct, fe);
 #pragma unroll
       for (int nv = 0; nv < NV; nv++)
-        if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) err |= ERR_NAN | ERR_QUIT;
+        if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) fe |= ERR_NAN | ERR_QUIT;
+      if (face_counts(g, DIR, m, 0, i, DIR == 1 ? 2 : 1, t)) err |= fe;
       if constexpr (PHYS != PHYS_HD) {
         if (m < m1) store_ct(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
       }
@@ -685,10 +707,12 @@ __device__ __forceinline__ void sweep_m_col(const StageArgs<CTT>& a, const Grid3
         vR[BX1 + DIR] = Bn;
       }
       CTFace<R> ct;
-      R cm = riemann<PHYS, RS, CT, DIR>(vL, vR, F, gamma, Bn, ct, err);
+      uint32_t fe = 0;
+      R cm = riemann<PHYS, RS, CT, DIR>(vL, vR, F, gamma, Bn, ct, fe);
 #pragma unroll
       for (int nv = 0; nv < NV; nv++)
-        if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) err |= ERR_NAN | ERR_QUIT;
+        if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) fe |= ERR_NAN | ERR_QUIT;
+      if (face_counts(g, DIR, m, 0, i, DIR == 1 ? 2 : 1, t)) err |= fe;
       if constexpr (PHYS != PHYS_HD) {
         if (m < m1) store_ct(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
       }
@@ -940,6 +964,14 @@ __device__ __forceinline__ double finish_cell(const StageArgs<CTT>& a, const Gri
 #pragma unroll
     for (int nv = 0; nv < NV; nv++)
       if (isnan(u[nv])) err |= ERR_NAN | ERR_QUIT;
+    bool dom = true;  // a domain cell (not padding)
+    if constexpr (PHYS != PHYS_HD) {
+      const int i = (int)(c % g.nx);
+      const int j = (int)((c / g.nx) % g.ny);
+      const int k = (int)(c / ((long long)g.nx * g.ny));
+      dom = i >= g.ilo[0] && i <= g.ihi[0] && j >= g.ilo[1] && j <= g.ihi[1] && k >= g.ilo[2] &&
+            k <= g.ihi[2];
+    }
     uint32_t le;
     if constexpr (PHYS == PHYS_MHD) le = mhd_cons2prim(u, v, a.gamma, a.small_rho, a.small_prs);
     else if constexpr (PHYS == PHYS_RMHD)
@@ -951,6 +983,10 @@ __device__ __forceinline__ double finish_cell(const StageArgs<CTT>& a, const Gri
     for (int nv = 0; nv < NV; nv++) {
       a.Uout[nv * n + c] = u[nv];
       a.Vout[nv * n + c] = v[nv];
+    }
+    if (!dom) {
+      err = 0;
+      cdt = 0.0;
     }
     if (err) atomicOr(a.err, err);
   }

@@ -57,6 +57,12 @@ template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM>
 static void run_stage(const StageArgs<CTT>& a, const GridDims& gd, int seg, cudaStream_t s,
                       cudaEvent_t* ev) {
   Grid3 g{gd.nx, gd.ny, gd.nz, gd.n, gd.outflow};
+  for (int d = 0; d < 3; d++) {
+    g.ilo[d] = gd.ilo[d];
+    g.ihi[d] = gd.ihi[d];
+    g.glo[d] = gd.glo[d];
+    g.ghi[d] = gd.ghi[d];
+  }
   int kidx = 0;
   auto pre = [&]() { if (ev) cudaEventRecord(ev[2 * kidx], s); };
   auto post = [&]() { if (ev) cudaEventRecord(ev[2 * kidx + 1], s); kidx++; };

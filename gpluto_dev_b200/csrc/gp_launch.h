@@ -32,6 +32,9 @@ struct GridDims {
   int nx, ny, nz;
   long long n;
   unsigned outflow = 0u;  // bit 2d / 2d+1: low / high side of direction d is outflow
+  // domain and ghosted-box cell ranges of a padded grid (see Grid3)
+  int ilo[3] = {0, 0, 0}, ihi[3] = {0x3fffffff, 0x3fffffff, 0x3fffffff};
+  int glo[3] = {0, 0, 0}, ghi[3] = {0x3fffffff, 0x3fffffff, 0x3fffffff};
 };
 
 struct SchemeKey {

@@ -31,8 +31,6 @@ def make_solver(st, limiter, solver, ct, cfl=0.4, cfl_max_var=1.1, precision=api
 @pytest.mark.parametrize("name", [n for n in gu.names() if not n.startswith("rmhd")])
 def test_gpu_matches_reference_fixture_bitwise(name):
     g = gu.Golden(name)
-    if g.outflow and g.physics != api.HD:
-        pytest.skip("outflow with constrained transport is not built on the GPU yet")
     s = make_solver(g.ic, g.limiter, g.solver, g.ct, g.cfl, g.cfl_max_var, outflow=g.outflow)
     dt_after, hist, out = s.run(g.nsteps, g.first_dt)
     V, U, Bs = s.download()
@@ -107,6 +105,54 @@ def test_gpu_outflow_matches_oracle_bitwise(case):
     np.testing.assert_array_equal(hist, ohist[:-1])
     np.testing.assert_array_equal(V, Vo)
     np.testing.assert_array_equal(U, Uo)
+
+
+CT_OUTFLOW_CASES = [
+    # (generator, kwargs, limiter, solver, ct, outflow mask, nsteps)
+    (ics.mhd2d_turbulence, dict(n=(33, 20), seed=57), "mc", "hlld", "uct_hlld", 0b0011, 12),
+    (ics.mhd2d_turbulence, dict(n=(24, 30), seed=58), "ppm", "hlld", "uct_hlld", 0b1111, 10),
+    (ics.mhd3d_turbulence, dict(n=(12, 10, 9), seed=59), "mc", "hlld", "uct_hlld", 0b111111, 6),
+    (ics.mhd3d_turbulence, dict(n=(16, 12, 10), seed=60), "vl", "hll", "uct_hll", 0b110000, 6),
+    (ics.mhd3d_blast, dict(n=(20, 18, 16), seed=61, radius=0.2), "mc", "hlld", "uct_hlld",
+     0b001100, 6),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CT_OUTFLOW_CASES)))
+def test_gpu_ct_outflow_matches_oracle_bitwise(case):
+    """Outflow with constrained transport: padded ghost zones filled before
+    every stage (copies, div-free normal faces, re-averaged ghost B)."""
+    gen, kw, lim, rs, ct, ob, nsteps = CT_OUTFLOW_CASES[case]
+    st = gen(**kw)
+    o = orc.Oracle(st, limiter=lim, solver=rs, ct=ct, outflow=ob)
+    ohist, oerr = o.run(nsteps, 1e-4)
+    Vo, Uo, Bo = o.state()
+    s = make_solver(st, lim, rs, ct, outflow=ob)
+    dt_after, hist, out = s.run(nsteps, 1e-4)
+    V, U, Bs = s.download()
+    assert out.err_bits == oerr
+    np.testing.assert_array_equal(hist, ohist[:-1])
+    np.testing.assert_array_equal(V, Vo)
+    np.testing.assert_array_equal(U, Uo)
+    for a, b in zip(Bs, Bo):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_ct_outflow_reference_layout_needs_the_scheme_ghost_depth():
+    st = ics.mhd2d_turbulence(n=(20, 16), seed=62)
+    s = make_solver(st, "mc", "hlld", "uct_hlld", outflow=0b0011)
+    cshape, fshapes = s.reference_shapes()          # nghost 2 = PLM ghost depth
+    Vr = np.empty(cshape)
+    Br = [np.empty(f) for f in fshapes]
+    api._check(api.lib().gp_download_state(s._h, api.LAYOUT_REFERENCE, None, api._dp(Vr),
+                                           api._dp(Br[0]), api._dp(Br[1]), None))
+    V, _, Bs = s.download()
+    np.testing.assert_array_equal(Vr[:, :, 2:-2, 2:-2], V)
+    np.testing.assert_array_equal(Br[0][:, 2:-2, 2:-3], Bs[0])
+    sp = api.Solver(2, (20, 16), api.Scheme(physics=api.MHD, limiter="ppm"), outflow=0b0011)
+    with pytest.raises(api.GPError) as ei:                # PPM needs nghost 3
+        sp.upload(st.V, None, st.Bs, layout=api.LAYOUT_REFERENCE)
+    assert ei.value.code == -2
 
 
 def test_outflow_reference_layout_ghosts_copy_the_boundary_cells():

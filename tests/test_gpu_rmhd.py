@@ -53,8 +53,6 @@ def test_rmhd_fp64_matches_reference_fixture(name):
     floors 1e-12 / 1e-11) and lose at most 1% more cells beyond 1e-10.
     The dt sequence must agree to 1e-12."""
     g = gu.Golden(name)
-    if g.outflow:
-        pytest.skip("outflow with constrained transport is not built on the GPU yet")
     spread = []
     try:
         for nudge in (1, -1):
