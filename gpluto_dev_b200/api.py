@@ -187,7 +187,10 @@ class Solver:
             self._h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:   # interpreter shutdown: the library may already be gone
+            pass
 
     # -- state transfer ---------------------------------------------------
     def upload(self, V, U=None, Bs=None, layout=LAYOUT_INTERIOR):

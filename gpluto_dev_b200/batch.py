@@ -114,7 +114,10 @@ class Batch:
             self._h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:   # interpreter shutdown: the library may already be gone
+            pass
 
     def add(self, st: "ics.PrimState", scheme: api.Scheme, dt0: float, nsteps: int,
             shape: TileShape | None = None) -> int:

@@ -334,7 +334,7 @@ __device__ __forceinline__ void sweep_x_row_ppm(const StageArgs<CTT>& a, const G
 #pragma unroll
     for (int nv = 0; nv < NV; nv++)
       if (act && rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) fe |= ERR_NAN | ERR_QUIT;
-    if (face_counts(g, 0, f, 1, row % g.ny, 2, row / g.ny)) err |= fe;
+    if (fe && face_counts(g, 0, f, 1, row % g.ny, 2, row / g.ny)) err |= fe;
     if constexpr (PHYS != PHYS_HD) {
       if (act) store_ct(a, 0, rb + f, ct);
     }
@@ -481,7 +481,7 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
 #pragma unroll
     for (int nv = 0; nv < NV; nv++)
       if (act && rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) fe |= ERR_NAN | ERR_QUIT;
-    if (face_counts(g, 0, f, 1, row % g.ny, 2, row / g.ny)) err |= fe;
+    if (fe && face_counts(g, 0, f, 1, row % g.ny, 2, row / g.ny)) err |= fe;
     if constexpr (PHYS != PHYS_HD) {
       if (act) store_ct(a, 0, rb + f, ct);
     }
@@ -618,7 +618,7 @@ __device__ __forceinline__ void sweep_m_col_ppm(const StageArgs<CTT>& a, const G
 #pragma unroll
       for (int nv = 0; nv < NV; nv++)
         if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) fe |= ERR_NAN | ERR_QUIT;
-      if (face_counts(g, DIR, m, 0, i, DIR == 1 ? 2 : 1, t)) err |= fe;
+      if (fe && face_counts(g, DIR, m, 0, i, DIR == 1 ? 2 : 1, t)) err |= fe;
       if constexpr (PHYS != PHYS_HD) {
         if (m < m1) store_ct(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
       }
@@ -712,7 +712,7 @@ __device__ __forceinline__ void sweep_m_col(const StageArgs<CTT>& a, const Grid3
 #pragma unroll
       for (int nv = 0; nv < NV; nv++)
         if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) fe |= ERR_NAN | ERR_QUIT;
-      if (face_counts(g, DIR, m, 0, i, DIR == 1 ? 2 : 1, t)) err |= fe;
+      if (fe && face_counts(g, DIR, m, 0, i, DIR == 1 ? 2 : 1, t)) err |= fe;
       if constexpr (PHYS != PHYS_HD) {
         if (m < m1) store_ct(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
       }
@@ -966,11 +966,13 @@ __device__ __forceinline__ double finish_cell(const StageArgs<CTT>& a, const Gri
       if (isnan(u[nv])) err |= ERR_NAN | ERR_QUIT;
     bool dom = true;  // a domain cell (not padding)
     if constexpr (PHYS != PHYS_HD) {
-      const int i = (int)(c % g.nx);
-      const int j = (int)((c / g.nx) % g.ny);
-      const int k = (int)(c / ((long long)g.nx * g.ny));
-      dom = i >= g.ilo[0] && i <= g.ihi[0] && j >= g.ilo[1] && j <= g.ihi[1] && k >= g.ilo[2] &&
-            k <= g.ihi[2];
+      if (g.ihi[0] != kNoLimit || g.ihi[1] != kNoLimit || g.ihi[2] != kNoLimit) {
+        const int i = (int)(c % g.nx);
+        const int j = (int)((c / g.nx) % g.ny);
+        const int k = (int)(c / ((long long)g.nx * g.ny));
+        dom = i >= g.ilo[0] && i <= g.ihi[0] && j >= g.ilo[1] && j <= g.ihi[1] &&
+              k >= g.ilo[2] && k <= g.ihi[2];
+      }
     }
     uint32_t le;
     if constexpr (PHYS == PHYS_MHD) le = mhd_cons2prim(u, v, a.gamma, a.small_rho, a.small_prs);

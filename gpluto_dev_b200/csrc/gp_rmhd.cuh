@@ -92,8 +92,9 @@ __device__ __forceinline__ void cubic_solve(double b, double c, double d, double
   arg = GP_MAX(-1.0, arg);
   arg = GP_MIN(1.0, arg);
   double theta = acos(arg) * one_3;
-  double cs = cos(theta);
-  double sn = sqrt3 * sin(theta);
+  double sn, cs;
+  sincos(theta, &sn, &cs);  // one range reduction for both
+  sn = sqrt3 * sn;
   double p = -b * one_3;
   z[0] = -sQ * (cs + sn) + p;
   z[1] = -sQ * (cs - sn) + p;
@@ -110,8 +111,9 @@ __device__ __forceinline__ void cubic_solve(float b, float c, float d, float* z)
   arg = GP_MAX(-1.0f, arg);
   arg = GP_MIN(1.0f, arg);
   float theta = acosf(arg) * one_3;
-  float cs = cosf(theta);
-  float sn = sqrt3 * sinf(theta);
+  float sn, cs;
+  sincosf(theta, &sn, &cs);
+  sn = sqrt3 * sn;
   float p = -b * one_3;
   z[0] = -sQ * (cs + sn) + p;
   z[1] = -sQ * (cs - sn) + p;
@@ -416,8 +418,37 @@ __device__ __forceinline__ int hlld_riemann_state(RState<R>& P, R p, R Bx, int s
 // fails the star solution (HLL fallback), which is deterministic.
 template <int DIR, typename R>
 __device__ __forceinline__ R hlld_fstar(RState<R>& PaL, RState<R>& PaR, R p, R Bx, R& Sc) {
-  const int okL = hlld_riemann_state<DIR>(PaL, p, Bx, -1);
-  const int okR = hlld_riemann_state<DIR>(PaR, p, Bx, 1);
+  // both sides through one inlined copy of the state builder: inputs (S,
+  // R) in, outputs (w, v, B_t, K, sw) back; a failed side keeps its
+  // previous outputs, as a direct call would
+  int okL = 0, okR = 0;
+#pragma unroll 1
+  for (int s = 0; s < 2; s++) {
+    RState<R> T;
+    T.S = s ? PaR.S : PaL.S;
+#pragma unroll
+    for (int nv = 0; nv < 8; nv++) T.Rr[nv] = s ? PaR.Rr[nv] : PaL.Rr[nv];
+    T.w = s ? PaR.w : PaL.w;
+    T.vx = s ? PaR.vx : PaL.vx;
+    T.vy = s ? PaR.vy : PaL.vy;
+    T.vz = s ? PaR.vz : PaL.vz;
+    T.By = s ? PaR.By : PaL.By;
+    T.Bz = s ? PaR.Bz : PaL.Bz;
+    T.sw = s ? PaR.sw : PaL.sw;
+    T.Kx = s ? PaR.Kx : PaL.Kx;
+    T.Ky = s ? PaR.Ky : PaL.Ky;
+    T.Kz = s ? PaR.Kz : PaL.Kz;
+    T.K2 = s ? PaR.K2 : PaL.K2;
+    const int ok = hlld_riemann_state<DIR>(T, p, Bx, s ? 1 : -1);
+    if (s) okR = ok; else okL = ok;
+    if (s) {
+      PaR.w = T.w; PaR.vx = T.vx; PaR.vy = T.vy; PaR.vz = T.vz; PaR.By = T.By; PaR.Bz = T.Bz;
+      PaR.sw = T.sw; PaR.Kx = T.Kx; PaR.Ky = T.Ky; PaR.Kz = T.Kz; PaR.K2 = T.K2;
+    } else {
+      PaL.w = T.w; PaL.vx = T.vx; PaL.vy = T.vy; PaL.vz = T.vz; PaL.By = T.By; PaL.Bz = T.Bz;
+      PaL.sw = T.sw; PaL.Kx = T.Kx; PaL.Ky = T.Ky; PaL.Kz = T.Kz; PaL.K2 = T.K2;
+    }
+  }
   R dK = PaR.Kx - PaL.Kx + R(1.e-12);
   R Bxc = Bx * dK;
   R Byc = PaR.By * (PaR.Kx - PaR.vx) - PaL.By * (PaL.Kx - PaL.vx) + Bx * (PaR.vy - PaL.vy);
@@ -461,13 +492,12 @@ __device__ __forceinline__ void hlld_astate(RState<R>& P, R p, R Bx) {
   ua[MXb] = (ua[7] + p) * P.vz - vB * ua[BXb];
 }
 
-// Src/RMHD/hlld.cpp:776-858
+// Src/RMHD/hlld.cpp:776-858; PaL.u and PaR.u hold the Alfven states
+// (hlld_astate) on entry
 template <int DIR, typename R>
 __device__ __forceinline__ void hlld_cstate(RState<R>& PaL, RState<R>& PaR, R p, R Bx, R* Uc) {
   constexpr int MXn = MX1 + DIR, MXt = MX1 + (DIR + 1) % 3, MXb = MX1 + (DIR + 2) % 3;
   constexpr int BXn = BX1 + DIR, BXt = BX1 + (DIR + 1) % 3, BXb = BX1 + (DIR + 2) % 3;
-  hlld_astate<DIR>(PaL, p, Bx);
-  hlld_astate<DIR>(PaR, p, Bx);
   R dK = (PaR.Kx - PaL.Kx) + R(1.e-12);
   R Byc = PaR.By * (PaR.Kx - PaR.vx) - PaL.By * (PaL.Kx - PaL.vx) + Bx * (PaR.vy - PaL.vy);
   R Bzc = PaR.Bz * (PaR.Kx - PaR.vx) - PaL.Bz * (PaL.Kx - PaL.vx) + Bx * (PaR.vz - PaL.vz);
@@ -532,11 +562,20 @@ __device__ __forceinline__ R rmhd_riemann(const R* vl, const R* vr, R* flux, R g
   rmhd_flux<DIR>(vl, ul, hl, fl, pl);
   rmhd_flux<DIR>(vr, ur, hr, fr, pr);
   {
-    R sl_min, sl_max, sr_min, sr_max;
-    rmhd_signal_speed<DIR>(vl, a2L, hl, sl_min, sl_max);
-    rmhd_signal_speed<DIR>(vr, a2R, hr, sr_min, sr_max);
-    Sl = GP_MIN(sl_min, sr_min);
-    Sr = GP_MAX(sl_max, sr_max);
+    // one inlined copy of the quartic for both states: the left state on
+    // the first pass, the right on the second
+    R cmn[2], cmx[2];
+#pragma unroll 1
+    for (int s = 0; s < 2; s++) {
+      R q[8];
+#pragma unroll
+      for (int nv = 0; nv < 8; nv++) q[nv] = s ? vr[nv] : vl[nv];
+      R sm, sx;
+      rmhd_signal_speed<DIR>(q, s ? a2R : a2L, s ? hr : hl, sm, sx);
+      if (s) { cmn[1] = sm; cmx[1] = sx; } else { cmn[0] = sm; cmx[0] = sx; }
+    }
+    Sl = GP_MIN(cmn[0], cmn[1]);
+    Sr = GP_MAX(cmx[0], cmx[1]);
   }
   const R cmax = GP_MAX(rabs(Sl), rabs(Sr));
   if constexpr (RS != RS_HLLD) {  // Src/RMHD/hll.cpp:180-202
@@ -594,36 +633,41 @@ __device__ __forceinline__ R rmhd_riemann(const R* vl, const R* vr, R* flux, R g
       }
       p0 = (R)hlld_total_pressure(vh);
     }
-    f0 = hlld_fstar<DIR>(PaL, PaR, p0, Bx, Sc);
-    if (isnan((double)f0) || PaL.fail) switch_to_hll = 1;
-    if (rabs(f0) > R(1.e-12) && !switch_to_hll) {
-      p = R(1.025) * p0;
-      f = f0;
-      for (int k1 = 1; k1 < 20; k1++) {  // bounded secant iteration (MAX_ITER 20)
-        f = hlld_fstar<DIR>(PaL, PaR, p, Bx, Sc);
-        if (f != f || PaL.fail || (k1 > 7) || (rabs(f) > rabs(f0) && k1 > 4)) {
-          switch_to_hll = 1;
-          break;
-        }
-        R dp = (p - p0) / (f - f0) * f;
-        p0 = p;
+    // Secant iteration on the total pressure (MAX_ITER 20).  Pass 0 is the
+    // initial guess p0 and pass k1 >= 1 the k1-th iterate, so the star-state
+    // evaluation has one inlined copy.
+    p = p0;
+#pragma unroll 1
+    for (int k1 = 0; k1 < 20; k1++) {
+      f = hlld_fstar<DIR>(PaL, PaR, p, Bx, Sc);
+      if (k1 == 0) {
         f0 = f;
-        p -= dp;
-        if (p < R(0)) p = R(1.e-6);
-        if (rabs(dp) < R(1.e-5) * p || rabs(f) < R(1.e-6)) break;
+        if (isnan((double)f0) || PaL.fail) switch_to_hll = 1;
+        if (!(rabs(f0) > R(1.e-12) && !switch_to_hll)) break;  // p stays p0
+        p = R(1.025) * p0;
+        continue;
       }
-    } else {
-      p = p0;
+      if (f != f || PaL.fail || (k1 > 7) || (rabs(f) > rabs(f0) && k1 > 4)) {
+        switch_to_hll = 1;
+        break;
+      }
+      R dp = (p - p0) / (f - f0) * f;
+      p0 = p;
+      f0 = f;
+      p -= dp;
+      if (p < R(0)) p = R(1.e-6);
+      if (rabs(dp) < R(1.e-5) * p || rabs(f) < R(1.e-6)) break;
     }
     if (PaL.fail) switch_to_hll = 1;
     if (!switch_to_hll) {
+      // both Alfven states (each depends only on its own side), one copy each
+      hlld_astate<DIR>(PaL, p, Bx);
+      hlld_astate<DIR>(PaR, p, Bx);
       if (PaL.Sa >= R(-1.e-6)) {
-        hlld_astate<DIR>(PaL, p, Bx);
         PaL.u[7] -= PaL.u[RHO];
 #pragma unroll
         for (int nv = 0; nv < 8; nv++) flux[nv] = fl[nv] + Sl * (PaL.u[nv] - ul[nv]);
       } else if (PaR.Sa <= R(1.e-6)) {
-        hlld_astate<DIR>(PaR, p, Bx);
         PaR.u[7] -= PaR.u[RHO];
 #pragma unroll
         for (int nv = 0; nv < 8; nv++) flux[nv] = fr[nv] + Sr * (PaR.u[nv] - ur[nv]);
