@@ -887,30 +887,179 @@ __global__ void __launch_bounds__(256, 4) emf_kernel(StageArgs<CTT> a, Grid3 g) 
   emf_cell<NDIM, LIM, R, CTT>(a, g, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+// 3-D edge EMFs of the mixed form (FP32 operands), one thread per (i, j)
+// column marching k over a segment of `sz` planes; blocks of 32 x 8 columns.
+// Same operands and operation order as emf_cell: the z-stencils (Bs_x and
+// Bs_y with their velocities along z) roll through a 4-plane register
+// window, and the face coefficients of a cell are loaded once and kept for
+// the next plane's k-1 neighbour, so the loads that remain (x and y stencils
+// of the current plane) fall in the block's 32 x 8 tile and its halo.
+constexpr int EMF_TX = 32, EMF_TY = 8, EMF_SEGMENT = 16;
+
+template <typename R, typename CTT>
+__device__ __forceinline__ void coef_load(const StageArgs<CTT>& a, int d, int f, R* c) {
+#pragma unroll
+  for (int q = 0; q < 4; q++) c[q] = (R)a.ct[d][2 + q][f];
+}
+
+template <typename R>
+__device__ __forceinline__ void coef_pair(const R* f1, const R* f2, R& aL, R& aR, R& dL,
+                                          R& dR) {
+  aL = R(0.5) * (f1[0] + f2[0]);
+  aR = R(0.5) * (f1[1] + f2[1]);
+  dL = R(0.5) * (f1[2] + f2[2]);
+  dR = R(0.5) * (f1[3] + f2[3]);
+}
+
+template <int LIM, typename R, typename CTT>
+__global__ void __launch_bounds__(EMF_TX * EMF_TY, 3)
+    emf_march_kernel(StageArgs<CTT> a, Grid3 g, int sz) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int i = blockIdx.x * EMF_TX + threadIdx.x;
+  const int j = blockIdx.y * EMF_TY + threadIdx.y;
+  if (i >= nx || j >= ny) return;
+  const int k0 = blockIdx.z * sz, k1 = min(k0 + sz, nz);
+  const int nxy = nx * ny;
+  int X[4], Y[4];
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    X[m] = wrapi(i - 2 + m, nx);
+    Y[m] = nx * wrapi(j - 2 + m, ny);
+  }
+  const int cxy = X[2] + Y[2];
+  // z window: plane k-2+m in slot m
+  R zb0[4], zq0[4], zb1[4], zq1[4];
+#pragma unroll
+  for (int m = 0; m < 3; m++) {
+    const int e = cxy + nxy * wrapi(k0 - 2 + m, nz);
+    zb0[m] = (R)a.Bs[0][e];
+    zq0[m] = (R)a.ct[0][1][e];
+    zb1[m] = (R)a.Bs[1][e];
+    zq1[m] = (R)a.ct[1][0][e];
+  }
+  R c0m[4], c1m[4];  // face coefficients of directions 0 and 1 at (i, j, k-1)
+  {
+    const int e = cxy + nxy * wrapi(k0 - 1, nz);
+    coef_load<R>(a, 0, e, c0m);
+    coef_load<R>(a, 1, e, c1m);
+  }
+  R b[4], q[4], f1[4], aL, aR, dL, dR, avg, phi;
+  for (int k = k0; k < k1; k++) {
+    const int Zk = nxy * k;
+    const int c = cxy + Zk;
+    {
+      const int e = cxy + nxy * wrapi(k + 1, nz);
+      zb0[3] = (R)a.Bs[0][e];
+      zq0[3] = (R)a.ct[0][1][e];
+      zb1[3] = (R)a.Bs[1][e];
+      zq1[3] = (R)a.ct[1][0][e];
+    }
+    // The six half-edge terms grouped by the face coefficients they share
+    // (each EMF still sums its own two terms in emf_cell's order), so that
+    // one set of cell coefficients is live at a time.
+    R Ez, Ey, Ex, cc[4];
+    coef_load<R>(a, 0, c, cc);
+    {  // Ez, first term: Bs_y along x
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        const int e = X[m] + Y[2] + Zk;
+        b[m] = (R)a.Bs[1][e];
+        q[m] = (R)a.ct[1][1][e];
+      }
+      coef_load<R>(a, 0, X[2] + Y[1] + Zk, f1);
+      coef_pair(f1, cc, aL, aR, dL, dR);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      Ez = avg + phi;
+    }
+    {  // Ey, first term: Bs_z along x
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        const int e = X[m] + Y[2] + Zk;
+        b[m] = (R)a.Bs[2][e];
+        q[m] = (R)a.ct[2][0][e];
+      }
+      coef_pair(c0m, cc, aL, aR, dL, dR);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      Ey = avg - phi;
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) c0m[m] = cc[m];
+    coef_load<R>(a, 1, c, cc);
+    {  // Ez, second term: Bs_x along y
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        const int e = X[2] + Y[m] + Zk;
+        b[m] = (R)a.Bs[0][e];
+        q[m] = (R)a.ct[0][0][e];
+      }
+      coef_load<R>(a, 1, X[1] + Y[2] + Zk, f1);
+      coef_pair(f1, cc, aL, aR, dL, dR);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      Ez += avg - phi;
+    }
+    {  // Ex, first term: Bs_z along y
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        const int e = X[2] + Y[m] + Zk;
+        b[m] = (R)a.Bs[2][e];
+        q[m] = (R)a.ct[2][1][e];
+      }
+      coef_pair(c1m, cc, aL, aR, dL, dR);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      Ex = avg + phi;
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) c1m[m] = cc[m];
+    coef_load<R>(a, 2, c, cc);
+    {  // Ey, second term: Bs_x along z (window)
+      coef_load<R>(a, 2, X[1] + Y[2] + Zk, f1);
+      coef_pair(f1, cc, aL, aR, dL, dR);
+      uct_terms<LIM>(zb0, zq0, aL, aR, dL, dR, avg, phi);
+      Ey += avg + phi;
+    }
+    {  // Ex, second term: Bs_y along z (window)
+      coef_load<R>(a, 2, X[2] + Y[1] + Zk, f1);
+      coef_pair(f1, cc, aL, aR, dL, dR);
+      uct_terms<LIM>(zb1, zq1, aL, aR, dL, dR, avg, phi);
+      Ex += avg - phi;
+    }
+    a.Ee[2][c] = (CTT)Ez;
+    a.Ee[1][c] = (CTT)Ey;
+    a.Ee[0][c] = (CTT)Ex;
+#pragma unroll
+    for (int m = 0; m < 3; m++) {
+      zb0[m] = zb0[m + 1];
+      zq0[m] = zq0[m + 1];
+      zb1[m] = zb1[m + 1];
+      zq1[m] = zq1[m + 1];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------
 // Stage finish: CT update (Src/MHD/CT/ct_update.cpp:181-423), face RK
 // combine (Src/rk_step.cpp:378-385, 536-552), cell-centred average
 // (Src/MHD/CT/ct_field_average.cpp:175-200), con2prim
 // (Src/mappers3D.cpp:104-194) -- all FP64.
 // ---------------------------------------------------------------------
+// -(curl E)·dt/dx of face d of the cell at offsets (X[x], Y[y], Z[z]) (the
+// wrapped offsets are formed once by the caller)
 template <int NDIM, typename CTT>
-__device__ __forceinline__ double face_rs(const StageArgs<CTT>& a, const Grid3& g, int d,
-                                          int i, int j, int k) {
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  auto id = [&](int ii, int jj, int kk) -> long long {
-    return wrapi(ii, nx) + (long long)nx * (wrapi(jj, ny) + (long long)ny * wrapi(kk, nz));
+__device__ __forceinline__ double face_rs_at(const StageArgs<CTT>& a, int d, const int* X,
+                                             const int* Y, const int* Z, int x, int y, int z) {
+  auto E = [&](int q, int ox, int oy, int oz) -> double {
+    return (double)a.Ee[q][X[x + ox] + Y[y + oy] + Z[z + oz]];
   };
-  auto E = [&](int q, int ii, int jj, int kk) -> double { return (double)a.Ee[q][id(ii, jj, kk)]; };
   double curlE;
   if (d == 0) {
-    curlE = 0.0 + a.dtdx[1] * (E(2, i, j + 1, k) - E(2, i, j, k));
-    if (NDIM == 3) curlE = curlE - a.dtdx[2] * (E(1, i, j, k + 1) - E(1, i, j, k));
+    curlE = 0.0 + a.dtdx[1] * (E(2, 0, 1, 0) - E(2, 0, 0, 0));
+    if (NDIM == 3) curlE = curlE - a.dtdx[2] * (E(1, 0, 0, 1) - E(1, 0, 0, 0));
   } else if (d == 1) {
-    curlE = -a.dtdx[0] * (E(2, i + 1, j, k) - E(2, i, j, k));
-    if (NDIM == 3) curlE = curlE + a.dtdx[2] * (E(0, i, j, k + 1) - E(0, i, j, k));
+    curlE = -a.dtdx[0] * (E(2, 1, 0, 0) - E(2, 0, 0, 0));
+    if (NDIM == 3) curlE = curlE + a.dtdx[2] * (E(0, 0, 0, 1) - E(0, 0, 0, 0));
   } else {
-    curlE = a.dtdx[0] * (E(1, i + 1, j, k) - E(1, i, j, k)) -
-            a.dtdx[1] * (E(0, i, j + 1, k) - E(0, i, j, k));
+    curlE = a.dtdx[0] * (E(1, 1, 0, 0) - E(1, 0, 0, 0)) -
+            a.dtdx[1] * (E(0, 0, 1, 0) - E(0, 0, 0, 0));
   }
   return -curlE;
 }
@@ -945,17 +1094,24 @@ __device__ __forceinline__ double finish_cell(const StageArgs<CTT>& a, const Gri
     cdt = (double)a.Cdt[c] + (double)a.Cdt[n + c];
     if (NDIM == 3) cdt = cdt + (double)a.Cdt[2 * n + c];
     if constexpr (PHYS != PHYS_HD) {
-      const int nx = g.nx, ny = g.ny, nz = g.nz;
-      const int i = (int)(c % nx);
-      const int j = (int)((c / nx) % ny);
-      const int k = (int)(c / ((long long)nx * ny));
+      // 32-bit wrapped offsets of the index and its two successors along
+      // each direction, formed once (grids hold fewer than 2^31 cells)
+      const int nx = g.nx, ny = g.ny, nz = g.nz, nxy = nx * ny;
+      const int ci = (int)c;
+      const int i = ci % nx, j = (ci / nx) % ny, k = ci / nxy;
+      int X[3], Y[3], Z[3];
+#pragma unroll
+      for (int m = 0; m < 3; m++) {
+        X[m] = wrapi(i + m, nx);
+        Y[m] = nx * wrapi(j + m, ny);
+        Z[m] = NDIM == 3 ? nxy * wrapi(k + m, nz) : 0;
+      }
 #pragma unroll
       for (int d = 0; d < NDIM; d++) {
         const int di = (d == 0), dj = (d == 1), dk = (d == 2);
-        const long long fr = wrapi(i + di, nx) +
-                             (long long)nx * (wrapi(j + dj, ny) + (long long)ny * wrapi(k + dk, nz));
-        double bl = face_new(a, d, c, face_rs<NDIM>(a, g, d, i, j, k));
-        double br = face_new(a, d, fr, face_rs<NDIM>(a, g, d, i + di, j + dj, k + dk));
+        const double bl = face_new(a, d, c, face_rs_at<NDIM>(a, d, X, Y, Z, 0, 0, 0));
+        const double br = face_new(a, d, (long long)(X[di] + Y[dj] + Z[dk]),
+                                   face_rs_at<NDIM>(a, d, X, Y, Z, di, dj, dk));
         a.Bsout[d][c] = bl;
         u[BX1 + d] = 0.5 * (bl + br);
       }

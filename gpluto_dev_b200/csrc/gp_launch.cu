@@ -91,7 +91,14 @@ static void run_stage(const StageArgs<CTT>& a, const GridDims& gd, int seg, cuda
   const unsigned nb = (unsigned)((gd.n + 255) / 256);
   if constexpr (PHYS != PHYS_HD) {
     pre();
-    emf_kernel<NDIM, LIM, RT, CTT><<<nb, 256, 0, s>>>(a, g);
+    if constexpr (NDIM == 3 && sizeof(RT) == 4) {  // mixed form: z-marching EMF
+      const int sz = EMF_SEGMENT;
+      dim3 grid((gd.nx + EMF_TX - 1) / EMF_TX, (gd.ny + EMF_TY - 1) / EMF_TY,
+                (gd.nz + sz - 1) / sz);
+      emf_march_kernel<LIM, RT, CTT><<<grid, dim3(EMF_TX, EMF_TY), 0, s>>>(a, g, sz);
+    } else {
+      emf_kernel<NDIM, LIM, RT, CTT><<<nb, 256, 0, s>>>(a, g);
+    }
     post();
   }
   pre();
