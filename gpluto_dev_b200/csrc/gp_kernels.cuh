@@ -93,11 +93,6 @@ __device__ __forceinline__ void load_cell(const double* __restrict__ V, long lon
   for (int nv = 0; nv < NV; nv++) v[nv] = (R)__ldg(V + nv * n + c);
 }
 
-__device__ __forceinline__ void atomic_max_pos(unsigned long long* addr, double v) {
-  // non-negative doubles order like their bit patterns
-  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
-}
-
 // Asynchronous global->shared copies (cp.async, per thread, 8 bytes): the
 // sweeps stage the next stencil cell while the current face is solved, so the
 // prefetch costs no registers.  Each thread reads back only what it staged.
@@ -1151,22 +1146,52 @@ __device__ __forceinline__ double finish_cell(const StageArgs<CTT>& a, const Gri
   return cdt;
 }
 
-// Stage-1 CFL maximum (Src/update_stage.cpp:422-435, getMax 446-461): warp
-// maximum, then one atomic per warp.  All 32 lanes must call it.
+// Stage-1 CFL maximum (Src/update_stage.cpp:422-435, getMax 446-461) on the
+// bit patterns of the non-negative inverse time steps, which order like the
+// values.  The stored maximum only grows, so an atomic whose value does not exceed a
+// (possibly older) read of it cannot change it and is skipped: the result
+// is the same, and the contended atomics on the one address drop from one
+// per warp to a handful per launch.
+__device__ __forceinline__ void max_bits_if_larger(unsigned long long* bits,
+                                                   unsigned long long v) {
+  if (v > __ldcg(bits)) atomicMax(bits, v);
+}
+
+// Warp maximum, then at most one atomic per warp.  All 32 lanes must call it.
 __device__ __forceinline__ void warp_invdt_max(unsigned long long* bits, double cdt, int lane) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const double other = __shfl_xor_sync(0xffffffffu, cdt, o);
     cdt = GP_MAX(cdt, other);
   }
-  if (lane == 0) atomic_max_pos(bits, cdt);
+  if (lane == 0) max_bits_if_larger(bits, (unsigned long long)__double_as_longlong(cdt));
+}
+
+// Warp maxima, then their largest bit pattern (the order atomicMax applies)
+// over the block, then at most one atomic per block.  Every thread of the
+// block must call it.
+__device__ __forceinline__ void block_invdt_max(unsigned long long* bits, double cdt) {
+  __shared__ unsigned long long wmax[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double other = __shfl_xor_sync(0xffffffffu, cdt, o);
+    cdt = GP_MAX(cdt, other);
+  }
+  if (lane == 0) wmax[w] = (unsigned long long)__double_as_longlong(cdt);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long m = wmax[0];
+    for (int q = 1; q < (int)(blockDim.x >> 5); q++) m = m > wmax[q] ? m : wmax[q];
+    max_bits_if_larger(bits, m);
+  }
 }
 
 template <int PHYS, int NV, int NDIM, typename CTT>
 __global__ void __launch_bounds__(256) finish_kernel(StageArgs<CTT> a, Grid3 g) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const double cdt = finish_cell<PHYS, NV, NDIM, CTT>(a, g, c);
-  if (a.stage == 1) warp_invdt_max(a.invdt_bits, cdt, threadIdx.x & 31);
+  if (a.stage == 1) block_invdt_max(a.invdt_bits, cdt);
 }
 
 // Start-up primitive -> conservative map (Src/startup.cpp:542-566).
