@@ -175,14 +175,26 @@ template <int PHYS, int NV, int NDIM, typename R, typename CTT>
 __device__ __forceinline__ void cell_update(const StageArgs<CTT>& a, long long n,
                                             long long c, const R* Fl, const R* Fr,
                                             R cml, R cmr, int dir) {
-  const double dtdx = a.dtdx[dir];
   CTT* du = a.dU + (long long)dir * NV * n;
+  if constexpr (sizeof(R) == sizeof(double)) {
+    const double dtdx = a.dtdx[dir];
 #pragma unroll
-  for (int nv = 0; nv < NV; nv++) {
-    if (!rhs_var<PHYS, NDIM>(nv)) continue;
-    du[nv * n + c] = (CTT)(-dtdx * ((double)Fr[nv] - (double)Fl[nv]));
+    for (int nv = 0; nv < NV; nv++) {
+      if (!rhs_var<PHYS, NDIM>(nv)) continue;
+      du[nv * n + c] = (CTT)(-dtdx * ((double)Fr[nv] - (double)Fl[nv]));
+    }
+    a.Cdt[(long long)dir * n + c] = (CTT)(0.5 * ((double)cml + (double)cmr) / a.dx[dir]);
+  } else {
+    // mixed form: the stored difference is FP32, so it is formed in FP32
+    // (no widening and narrowing conversions on the XU pipe)
+    const R dtdx = (R)a.dtdx[dir];
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      if (!rhs_var<PHYS, NDIM>(nv)) continue;
+      du[nv * n + c] = (CTT)(-dtdx * (Fr[nv] - Fl[nv]));
+    }
+    a.Cdt[(long long)dir * n + c] = (CTT)(R(0.5) * (cml + cmr) / (R)a.dx[dir]);
   }
-  a.Cdt[(long long)dir * n + c] = (CTT)(0.5 * ((double)cml + (double)cmr) / a.dx[dir]);
 }
 
 template <typename R, typename CTT>
@@ -328,7 +340,7 @@ __device__ __forceinline__ void sweep_x_row_ppm(const StageArgs<CTT>& a, const G
     cm = riemann<PHYS, RS, CT, 0>(vL, vR, F, gamma, Bn, ct, fe);
 #pragma unroll
     for (int nv = 0; nv < NV; nv++)
-      if (act && rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) fe |= ERR_NAN | ERR_QUIT;
+      if (act && rhs_var<PHYS, NDIM>(nv) && isnan(F[nv])) fe |= ERR_NAN | ERR_QUIT;
     if (fe && face_counts(g, 0, f, 1, row % g.ny, 2, row / g.ny)) err |= fe;
     if constexpr (PHYS != PHYS_HD) {
       if (act) store_ct(a, 0, rb + f, ct);
@@ -475,7 +487,7 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
     cm = riemann<PHYS, RS, CT, 0>(vL, vR, F, gamma, Bn, ct, fe);
 #pragma unroll
     for (int nv = 0; nv < NV; nv++)
-      if (act && rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) fe |= ERR_NAN | ERR_QUIT;
+      if (act && rhs_var<PHYS, NDIM>(nv) && isnan(F[nv])) fe |= ERR_NAN | ERR_QUIT;
     if (fe && face_counts(g, 0, f, 1, row % g.ny, 2, row / g.ny)) err |= fe;
     if constexpr (PHYS != PHYS_HD) {
       if (act) store_ct(a, 0, rb + f, ct);
@@ -612,7 +624,7 @@ __device__ __forceinline__ void sweep_m_col_ppm(const StageArgs<CTT>& a, const G
       R cm = riemann<PHYS, RS, CT, DIR>(vL, vR, F, gamma, Bn, ct, fe);
 #pragma unroll
       for (int nv = 0; nv < NV; nv++)
-        if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) fe |= ERR_NAN | ERR_QUIT;
+        if (rhs_var<PHYS, NDIM>(nv) && isnan(F[nv])) fe |= ERR_NAN | ERR_QUIT;
       if (fe && face_counts(g, DIR, m, 0, i, DIR == 1 ? 2 : 1, t)) err |= fe;
       if constexpr (PHYS != PHYS_HD) {
         if (m < m1) store_ct(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
@@ -706,7 +718,7 @@ __device__ __forceinline__ void sweep_m_col(const StageArgs<CTT>& a, const Grid3
       R cm = riemann<PHYS, RS, CT, DIR>(vL, vR, F, gamma, Bn, ct, fe);
 #pragma unroll
       for (int nv = 0; nv < NV; nv++)
-        if (rhs_var<PHYS, NDIM>(nv) && isnan((double)F[nv])) fe |= ERR_NAN | ERR_QUIT;
+        if (rhs_var<PHYS, NDIM>(nv) && isnan(F[nv])) fe |= ERR_NAN | ERR_QUIT;
       if (fe && face_counts(g, DIR, m, 0, i, DIR == 1 ? 2 : 1, t)) err |= fe;
       if constexpr (PHYS != PHYS_HD) {
         if (m < m1) store_ct(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);

@@ -92,7 +92,12 @@ static void run_stage(const StageArgs<CTT>& a, const GridDims& gd, int seg, cuda
   if constexpr (PHYS != PHYS_HD) {
     pre();
     if constexpr (NDIM == 3 && sizeof(RT) == 4) {  // mixed form: z-marching EMF
-      const int sz = EMF_SEGMENT;
+      // the longest segment (<= EMF_SEGMENT planes) that still gives about
+      // four waves of blocks over 148 SMs (3 blocks per SM)
+      const long long cols = (long long)((gd.nx + EMF_TX - 1) / EMF_TX) *
+                             ((gd.ny + EMF_TY - 1) / EMF_TY);
+      int sz = EMF_SEGMENT;
+      while (sz > 4 && cols * ((gd.nz + sz - 1) / sz) < 148LL * 3 * 4) sz /= 2;
       dim3 grid((gd.nx + EMF_TX - 1) / EMF_TX, (gd.ny + EMF_TY - 1) / EMF_TY,
                 (gd.nz + sz - 1) / sz);
       emf_march_kernel<LIM, RT, CTT><<<grid, dim3(EMF_TX, EMF_TY), 0, s>>>(a, g, sz);
