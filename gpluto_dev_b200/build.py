@@ -23,9 +23,15 @@ LIB = os.path.join(OUT, "libgpluto_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 BASE = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 
+# The mixed form's FP32 arithmetic (reconstruction, Riemann fluxes, UCT
+# EMFs) uses the approximate FP32 divide and square root and flushes FP32
+# denormals: it is issue-bound, and these halve the instructions of every
+# FP32 division.  These flags touch single precision only, so the FP64
+# accumulation, CT update and con2prim of that form stay IEEE.
+MIXED_FP32 = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
 UNITS = [
     ("gp_launch_fp64.o", "gp_launch.cu", ["-DGP_MIXED=0", "-fmad=false"]),
-    ("gp_launch_mixed.o", "gp_launch.cu", ["-DGP_MIXED=1", "-fmad=true"]),
+    ("gp_launch_mixed.o", "gp_launch.cu", ["-DGP_MIXED=1", *MIXED_FP32]),
     ("gp_api.o", "gp_api.cu", ["-fmad=false"]),
     ("gp_noalloc.o", "gp_noalloc.cu", ["-fmad=false"]),
 ]
@@ -37,9 +43,9 @@ SWEEP_RDC = ["-rdc=true", "-maxrregcount=168", "-DGP_BATCH_PART=0"]
 CELL_RDC = ["-rdc=true", "-maxrregcount=64", "-DGP_BATCH_PART=1"]
 RDC_UNITS = [
     ("gp_batch_sweeps_fp64.o", "gp_batch_tiles.cu", ["-DGP_MIXED=0", "-fmad=false", *SWEEP_RDC]),
-    ("gp_batch_sweeps_mixed.o", "gp_batch_tiles.cu", ["-DGP_MIXED=1", "-fmad=true", *SWEEP_RDC]),
+    ("gp_batch_sweeps_mixed.o", "gp_batch_tiles.cu", ["-DGP_MIXED=1", *MIXED_FP32, *SWEEP_RDC]),
     ("gp_batch_cells_fp64.o", "gp_batch_tiles.cu", ["-DGP_MIXED=0", "-fmad=false", *CELL_RDC]),
-    ("gp_batch_cells_mixed.o", "gp_batch_tiles.cu", ["-DGP_MIXED=1", "-fmad=true", *CELL_RDC]),
+    ("gp_batch_cells_mixed.o", "gp_batch_tiles.cu", ["-DGP_MIXED=1", *MIXED_FP32, *CELL_RDC]),
     ("gp_batch.o", "gp_batch.cu", ["-fmad=false", "-rdc=true"]),
 ]
 DLINK = "gp_batch_dlink.o"
@@ -54,7 +60,8 @@ def nvcc() -> str:
 
 def _deps() -> list:
     return [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [
-        os.path.join(os.path.dirname(HERE), "include", "gpluto_b200.h")]
+        os.path.join(os.path.dirname(HERE), "include", "gpluto_b200.h"),
+        os.path.abspath(__file__)]  # the flags live here
 
 
 def build(verbose: bool = False, jobs: int = 3) -> str:
