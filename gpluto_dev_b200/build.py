@@ -25,8 +25,8 @@ BASE = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed
 
 # The mixed form's FP32 arithmetic (reconstruction, Riemann fluxes, UCT
 # EMFs) uses the approximate FP32 divide and square root and flushes FP32
-# denormals: it is issue-bound, and these halve the instructions of every
-# FP32 division.  These flags touch single precision only, so the FP64
+# denormals: its sweeps are issue-bound, and these cut their instruction
+# count by about a fifth.  These flags touch single precision only, so the FP64
 # accumulation, CT update and con2prim of that form stay IEEE.
 MIXED_FP32 = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
 UNITS = [

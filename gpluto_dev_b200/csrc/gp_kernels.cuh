@@ -186,7 +186,7 @@ __device__ __forceinline__ void cell_update(const StageArgs<CTT>& a, long long n
     a.Cdt[(long long)dir * n + c] = (CTT)(0.5 * ((double)cml + (double)cmr) / a.dx[dir]);
   } else {
     // mixed form: the stored difference is FP32, so it is formed in FP32
-    // (no widening and narrowing conversions on the XU pipe)
+    // (no widening and narrowing conversions, no FP64 division)
     const R dtdx = (R)a.dtdx[dir];
 #pragma unroll
     for (int nv = 0; nv < NV; nv++) {
