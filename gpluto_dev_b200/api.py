@@ -23,7 +23,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("GPLUTO_B200_LIB") or os.path.join(_HERE, "_build",
                                                              "libgpluto_b200.so")
 
-GP_OK, GP_ERR_INVALID, GP_ERR_QUIT, GP_ERR_NO_DEVICE = 0, -1, -5, -6
+GP_OK, GP_ERR_INVALID, GP_ERR_QUIT, GP_ERR_NO_DEVICE, GP_ERR_IO = 0, -1, -5, -6, -7
 HD, MHD, RMHD = 0, 1, 2
 # "ppm" selects RECONSTRUCTION PARABOLIC (the limiter then plays no part)
 LIMITERS = {"flat": 0, "minmod": 1, "vl": 2, "vanleer": 2, "mc": 3, "ppm": 3}
@@ -87,6 +87,11 @@ def lib():
         L.gp_kernel_name.restype = ctypes.c_char_p
         L.gp_kernel_name.argtypes = [P, ctypes.c_int]
         L.gp_last_error.restype = ctypes.c_char_p
+        L.gp_write_dbl.argtypes = [P, ctypes.c_char_p, ctypes.c_int, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_int]
+        L.gp_read_dbl.argtypes = [P, ctypes.c_char_p, ctypes.c_int, D, D,
+                                  ctypes.POINTER(ctypes.c_int)]
+        L.gp_data_minmax.argtypes = [P, D, D, D]
         _lib = L
     return _lib
 
@@ -257,6 +262,28 @@ class Solver:
         res = [(lib().gp_kernel_name(self._h, q).decode(), 1 + q // per, float(buf[q]))
                for q in range(nk.value)]
         return res, d.value
+
+    # -- output, restart, diagnostics (reference formats) ------------------
+    def write_dbl(self, dir: str, nfile: int, t: float, dt: float, nstep: int):
+        """WriteData (DBL, single_file) + RestartDump: data.NNNN.dbl, dbl.out,
+        restart.out in ``dir`` (Src/write_data.cpp:35-503,
+        Src/restart.cpp:423-458)."""
+        _check(lib().gp_write_dbl(self._h, os.fsencode(dir), nfile, t, dt, nstep))
+
+    def read_dbl(self, dir: str, nrestart: int):
+        """RestartFromFile for a .dbl output (Src/restart.cpp:34-411): loads
+        output #nrestart and returns (t, dt, nstep) of its restart record."""
+        t, dt, ns = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        _check(lib().gp_read_dbl(self._h, os.fsencode(dir), nrestart, ctypes.byref(t),
+                                 ctypes.byref(dt), ctypes.byref(ns)))
+        return t.value, dt.value, ns.value
+
+    def minmax(self):
+        """DataMinMax (Src/main.cpp:752-900): (vmin, vmax, mach_max)."""
+        vmin, vmax = np.zeros(self.nvar), np.zeros(self.nvar)
+        mach = ctypes.c_double()
+        _check(lib().gp_data_minmax(self._h, _dp(vmin), _dp(vmax), ctypes.byref(mach)))
+        return vmin, vmax, mach.value
 
     def device_pointers(self):
         u, v = ctypes.c_void_p(), ctypes.c_void_p()

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "../../include/gpluto_b200.h"
 #include "gp_launch.h"
@@ -841,6 +842,344 @@ const char* gp_kernel_name(const gp_handle* h, int idx) {
   if (!h) return "?";
   const int per = gp::stage_launch_count(h->key);
   return gp::stage_kernel_name(h->key, idx % per);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Output, restart and the min/max diagnostic in the reference's formats.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kDblOutput = 1;          // DBL_OUTPUT, Src/gpluto.hpp:139
+constexpr int kMaxOutputTypes = 16;    // Src/gpluto.hpp:184
+constexpr int kMaxRestartParams = 12;  // Src/gpluto.hpp:186
+
+// One record of restart.out (Src/structs.hpp:382-390); the reference prints
+// sizeof(Restart) = 256 on x86-64.
+struct RestartRecord {
+  double t;
+  double dt;
+  double param[kMaxRestartParams];
+  int nstep;
+  int nfile[kMaxOutputTypes];
+  int nfileParticles[kMaxOutputTypes];
+  char fill[10];
+};
+static_assert(sizeof(RestartRecord) == 256, "restart.out record layout");
+
+bool little_endian() {
+  const unsigned one = 1u;
+  unsigned char b;
+  std::memcpy(&b, &one, 1);
+  return b == 1;
+}
+
+// output variable names in NVAR order (Src/set_var_names.cpp:20-42)
+const char* var_name(int physics, int nv) {
+  static const char* mhd[8] = {"rho", "vx1", "vx2", "vx3", "Bx1", "Bx2", "Bx3", "prs"};
+  static const char* hd[5] = {"rho", "vx1", "vx2", "vx3", "prs"};
+  return physics == GP_HD ? hd[nv] : mhd[nv];
+}
+
+// interior extents of output variable `stag` (-1: cell centred), with the
+// one extra face along a staggered field's own direction
+// (Src/bin_io.cpp:309-330)
+void out_dims(const gp_handle* h, int stag, int* m) {
+  const int n[3] = {h->nx, h->ny, h->nz};
+  for (int d = 0; d < 3; d++) m[d] = n[d] + (stag == d ? 1 : 0);
+}
+
+void swap4(int* x) {
+  unsigned char b[4];
+  std::memcpy(b, x, 4);
+  const unsigned char r[4] = {b[3], b[2], b[1], b[0]};
+  std::memcpy(x, r, 4);
+}
+
+void swap8(double* x, size_t n) {
+  for (size_t q = 0; q < n; q++) {
+    unsigned char b[8];
+    std::memcpy(b, x + q, 8);
+    for (int e = 0; e < 4; e++) {
+      unsigned char t = b[e];
+      b[e] = b[7 - e];
+      b[7 - e] = t;
+    }
+    std::memcpy(x + q, b, 8);
+  }
+}
+
+// DataMinMax (Src/main.cpp:752-900) over the domain cells of V: per variable
+// minimum and maximum, and the largest max(|v_x|,|v_y|,|v_z|)/sqrt(p/rho),
+// with the reference's MAX/MIN (Src/macros.hpp:191-194).  Grid-stride
+// partials per block, then one block over the partials.
+constexpr int kMinMaxThreads = 256;
+constexpr int kMinMaxBlocks = 592;  // 148 SMs x 4
+
+__device__ __forceinline__ double ref_max(double a, double b) { return a >= b ? a : b; }
+__device__ __forceinline__ double ref_min(double a, double b) { return a <= b ? a : b; }
+
+__global__ void __launch_bounds__(kMinMaxThreads) minmax_partial_kernel(
+    const double* __restrict__ V, int nvar, int prs, Pad p, double* __restrict__ part) {
+  __shared__ double red[kMinMaxThreads];
+  double mn[8], mx[8], mach = 0.0;
+  for (int nv = 0; nv < 8; nv++) {
+    mx[nv] = -1e18;
+    mn[nv] = 1e18;
+  }
+  const long long ncell = (long long)p.nx * p.ny * p.nz;
+  const long long pn = (long long)p.px * p.py * p.pz;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % p.nx), j = (int)((c / p.nx) % p.ny);
+    const int k = (int)(c / ((long long)p.nx * p.ny));
+    const long long q = (i + p.lx) + (long long)p.px * ((j + p.ly) + (long long)p.py * (k + p.lz));
+    double v[8];
+    for (int nv = 0; nv < nvar; nv++) v[nv] = V[nv * pn + q];
+    double cs = v[prs] / v[0];
+    cs = sqrt(cs);
+    const double mi = fabs(v[1]) / cs, mj = fabs(v[2]) / cs, mk = fabs(v[3]) / cs;
+    double lm = ref_max(mi, mj);
+    lm = ref_max(lm, mk);
+    mach = ref_max(mach, lm);
+    for (int nv = 0; nv < nvar; nv++) {
+      mx[nv] = ref_max(mx[nv], v[nv]);
+      mn[nv] = ref_min(mn[nv], v[nv]);
+    }
+  }
+  const int nq = 2 * nvar + 1;
+  for (int qv = 0; qv < nq; qv++) {
+    const bool is_min = qv >= nvar && qv < 2 * nvar;
+    red[threadIdx.x] = qv < nvar ? mx[qv] : (is_min ? mn[qv - nvar] : mach);
+    __syncthreads();
+    for (int s = kMinMaxThreads / 2; s > 0; s >>= 1) {
+      if ((int)threadIdx.x < s)
+        red[threadIdx.x] = is_min ? ref_min(red[threadIdx.x], red[threadIdx.x + s])
+                                  : ref_max(red[threadIdx.x], red[threadIdx.x + s]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(long long)blockIdx.x * nq + qv] = red[0];
+    __syncthreads();
+  }
+}
+
+__global__ void minmax_final_kernel(const double* __restrict__ part, int nparts, int nvar,
+                                    double* __restrict__ out) {
+  const int nq = 2 * nvar + 1;
+  const int qv = threadIdx.x;
+  if (qv >= nq) return;
+  const bool is_min = qv >= nvar && qv < 2 * nvar;
+  double r = part[qv];
+  for (int b = 1; b < nparts; b++)
+    r = is_min ? ref_min(r, part[(long long)b * nq + qv]) : ref_max(r, part[(long long)b * nq + qv]);
+  out[qv] = r;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gp_data_minmax(gp_handle* h, double* vmin, double* vmax, double* mach_max) {
+  if (!h || !vmin || !vmax) return fail(GP_ERR_INVALID, "null handle or output");
+  const int nq = 2 * h->nvar + 1;
+  double* part = nullptr;
+  CUDA_TRY(cudaMallocAsync((void**)&part, sizeof(double) * (kMinMaxBlocks + 1) * nq, h->stream));
+  const int prs = h->nvar - 1;  // PRS is the last variable (HD 4, MHD/RMHD 7)
+  minmax_partial_kernel<<<kMinMaxBlocks, kMinMaxThreads, 0, h->stream>>>(h->V, h->nvar, prs,
+                                                                         pad_of(h), part);
+  minmax_final_kernel<<<1, 32, 0, h->stream>>>(part, kMinMaxBlocks, h->nvar,
+                                               part + (size_t)kMinMaxBlocks * nq);
+  double res[17];
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(res, part + (size_t)kMinMaxBlocks * nq, sizeof(double) * nq,
+                        cudaMemcpyDeviceToHost, h->stream);
+  cudaFreeAsync(part, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return fail(GP_ERR_CUDA, "gp_data_minmax: %s", cudaGetErrorString(e));
+  for (int nv = 0; nv < h->nvar; nv++) {
+    vmax[nv] = res[nv];
+    vmin[nv] = res[h->nvar + nv];
+  }
+  if (mach_max) *mach_max = res[2 * h->nvar];
+  return GP_OK;
+}
+
+int gp_write_dbl(gp_handle* h, const char* dir, int nfile, double t, double dt, int nstep) {
+  if (!h || !dir || nfile < 0) return fail(GP_ERR_INVALID, "null handle/dir or nfile < 0");
+  const bool mhd = h->scheme.physics != GP_HD;
+  // current state in the reference layout (ghost zones as Boundary() fills them)
+  int s[3], o[3];
+  ref_dims(h, -1, s, o);
+  std::vector<double> V((size_t)s[0] * s[1] * s[2] * h->nvar);
+  std::vector<double> B[3];
+  for (int d = 0; mhd && d < h->ndim; d++) {
+    int fs[3], fo[3];
+    ref_dims(h, d, fs, fo);
+    B[d].resize((size_t)fs[0] * fs[1] * fs[2]);
+  }
+  int rc = gp_download_state(h, GP_LAYOUT_REFERENCE, nullptr, V.data(),
+                             B[0].empty() ? nullptr : B[0].data(),
+                             B[1].empty() ? nullptr : B[1].data(),
+                             B[2].empty() ? nullptr : B[2].data());
+  if (rc) return rc;
+  // data.NNNN.dbl, single_file mode: the interior of every output variable
+  // in turn (Src/write_data.cpp:131-160, FillOutputBuffer 563-601)
+  char fname[1024];
+  snprintf(fname, sizeof(fname), "%s/data.%04d.dbl", dir, nfile);
+  FILE* f = fopen(fname, "wb");
+  if (!f) return fail(GP_ERR_IO, "cannot write %s", fname);
+  std::vector<double> buf;
+  auto dump = [&](const double* src, const int* sext, int stag) -> bool {
+    int m[3];
+    out_dims(h, stag, m);
+    buf.resize((size_t)m[0] * m[1] * m[2]);
+    size_t q = 0;
+    for (int k = 0; k < m[2]; k++)
+      for (int j = 0; j < m[1]; j++)
+        for (int i = 0; i < m[0]; i++)
+          buf[q++] = src[(i + o[0]) + (size_t)sext[0] * ((j + o[1]) + (size_t)sext[1] * (k + o[2]))];
+    return fwrite(buf.data(), sizeof(double), buf.size(), f) == buf.size();
+  };
+  bool ok = true;
+  const size_t ncell = (size_t)s[0] * s[1] * s[2];
+  for (int nv = 0; ok && nv < h->nvar; nv++) ok = dump(V.data() + nv * ncell, s, -1);
+  for (int d = 0; ok && mhd && d < h->ndim; d++) {
+    int fs[3], fo[3];
+    ref_dims(h, d, fs, fo);
+    ok = dump(B[d].data(), fs, d);
+  }
+  if (fclose(f) != 0 || !ok) return fail(GP_ERR_IO, "short write to %s", fname);
+  // dbl.out: line nfile, written over whatever follows line nfile-1
+  // (Src/write_data.cpp:474-503)
+  snprintf(fname, sizeof(fname), "%s/dbl.out", dir);
+  FILE* fo_ = fopen(fname, nfile == 0 ? "w" : "r+");
+  if (!fo_) return fail(GP_ERR_IO, "cannot open %s", fname);
+  char sline[512];
+  for (int q = 0; q < nfile; q++)
+    if (!fgets(sline, sizeof(sline), fo_)) {
+      fclose(fo_);
+      return fail(GP_ERR_IO, "%s has fewer than %d lines", fname, nfile);
+    }
+  fseek(fo_, ftell(fo_), SEEK_SET);
+  fprintf(fo_, "%d %12.6e %12.6e %d ", nfile, t, dt, nstep);
+  fprintf(fo_, "single_file ");
+  fprintf(fo_, little_endian() ? "little " : "big ");
+  for (int nv = 0; nv < h->nvar; nv++) fprintf(fo_, "%s ", var_name(h->scheme.physics, nv));
+  for (int d = 0; mhd && d < h->ndim; d++) fprintf(fo_, "Bx%ds ", d + 1);
+  fprintf(fo_, "\n");
+  if (fclose(fo_) != 0) return fail(GP_ERR_IO, "cannot write %s", fname);
+  // restart.out: record nfile (RestartDump, Src/restart.cpp:423-458)
+  RestartRecord r;
+  std::memset(&r, 0, sizeof(r));
+  r.t = t;
+  r.dt = dt;
+  r.nstep = nstep;
+  for (int q = 0; q < kMaxOutputTypes; q++) r.nfile[q] = r.nfileParticles[q] = -1;
+  r.nfile[kDblOutput] = nfile;
+  snprintf(fname, sizeof(fname), "%s/restart.out", dir);
+  FILE* fr = fopen(fname, nfile == 0 ? "wb" : "r+b");
+  if (!fr && nfile > 0) fr = fopen(fname, "wb");
+  if (!fr) return fail(GP_ERR_IO, "cannot open %s", fname);
+  fseek(fr, (long)nfile * (long)sizeof(RestartRecord), SEEK_SET);
+  ok = fwrite(&r, sizeof(r), 1, fr) == 1;
+  if (fclose(fr) != 0 || !ok) return fail(GP_ERR_IO, "cannot write %s", fname);
+  return GP_OK;
+}
+
+int gp_read_dbl(gp_handle* h, const char* dir, int nrestart, double* t, double* dt,
+                int* nstep) {
+  if (!h || !dir || nrestart < 0) return fail(GP_ERR_INVALID, "null handle/dir or nrestart < 0");
+  const bool mhd = h->scheme.physics != GP_HD;
+  // 1. dbl.out line nrestart: mode and byte order (Src/restart.cpp:67-104)
+  char fname[1024], sline[1024], mode[64] = "", endian[64] = "";
+  snprintf(fname, sizeof(fname), "%s/dbl.out", dir);
+  FILE* f = fopen(fname, "r");
+  if (!f) return fail(GP_ERR_IO, "cannot find %s", fname);
+  int line = 0, found = 0;
+  while (fgets(sline, sizeof(sline), f)) {
+    if (line++ == nrestart) {
+      int a, c;
+      double x, y;
+      found = sscanf(sline, "%d %lf %lf %d %63s %63s", &a, &x, &y, &c, mode, endian) == 6;
+      break;
+    }
+  }
+  fclose(f);
+  if (!found) return fail(GP_ERR_IO, "output #%d does not exist in %s", nrestart, fname);
+  if (std::strcmp(mode, "single_file") != 0)
+    return fail(GP_ERR_UNSUPPORTED, "only single_file dbl output is read (found %s)", mode);
+  const bool swap = (std::strcmp(endian, "big") == 0) == little_endian();
+  // 2. restart.out: the record whose DBL file number is nrestart
+  //    (RestartGet, Src/restart.cpp:331-411)
+  snprintf(fname, sizeof(fname), "%s/restart.out", dir);
+  f = fopen(fname, "rb");
+  if (!f) return fail(GP_ERR_IO, "cannot find %s", fname);
+  RestartRecord r;
+  found = 0;
+  while (fread(&r, sizeof(r), 1, f) == 1) {
+    int nf = r.nfile[kDblOutput];
+    if (swap) swap4(&nf);
+    if (nf == nrestart) {
+      found = 1;
+      break;
+    }
+  }
+  fclose(f);
+  if (!found) return fail(GP_ERR_IO, "no record of output #%d in %s", nrestart, fname);
+  if (swap) {
+    swap8(&r.t, 1);
+    swap8(&r.dt, 1);
+    swap4(&r.nstep);
+  }
+  // 3. data.NNNN.dbl into the reference layout; ghost zones take the
+  //    nearest interior value (they are refilled before every stage)
+  snprintf(fname, sizeof(fname), "%s/data.%04d.dbl", dir, nrestart);
+  f = fopen(fname, "rb");
+  if (!f) return fail(GP_ERR_IO, "cannot find %s", fname);
+  int s[3], o[3];
+  ref_dims(h, -1, s, o);
+  const size_t ncell = (size_t)s[0] * s[1] * s[2];
+  std::vector<double> V(ncell * h->nvar), B[3];
+  std::vector<double> buf;
+  bool ok = true;
+  auto load = [&](double* dst, const int* sext, int stag) -> bool {
+    int m[3];
+    out_dims(h, stag, m);
+    buf.resize((size_t)m[0] * m[1] * m[2]);
+    if (fread(buf.data(), sizeof(double), buf.size(), f) != buf.size()) return false;
+    if (swap) swap8(buf.data(), buf.size());
+    for (int k = 0; k < sext[2]; k++)
+      for (int j = 0; j < sext[1]; j++)
+        for (int i = 0; i < sext[0]; i++) {
+          const int ii = i - o[0] < 0 ? 0 : (i - o[0] >= m[0] ? m[0] - 1 : i - o[0]);
+          const int jj = j - o[1] < 0 ? 0 : (j - o[1] >= m[1] ? m[1] - 1 : j - o[1]);
+          const int kk = k - o[2] < 0 ? 0 : (k - o[2] >= m[2] ? m[2] - 1 : k - o[2]);
+          dst[i + (size_t)sext[0] * (j + (size_t)sext[1] * k)] =
+              buf[ii + (size_t)m[0] * (jj + (size_t)m[1] * kk)];
+        }
+    return true;
+  };
+  for (int nv = 0; ok && nv < h->nvar; nv++) ok = load(V.data() + nv * ncell, s, -1);
+  for (int d = 0; ok && mhd && d < h->ndim; d++) {
+    int fs[3], fo[3];
+    ref_dims(h, d, fs, fo);
+    B[d].resize((size_t)fs[0] * fs[1] * fs[2]);
+    ok = load(B[d].data(), fs, d);
+  }
+  fclose(f);
+  if (!ok) return fail(GP_ERR_IO, "%s is shorter than this grid's output", fname);
+  // 4. upload; Uc = PrimToCons(Vc) on the device (Src/restart.cpp:276-283)
+  int rc = gp_upload_state(h, GP_LAYOUT_REFERENCE, nullptr, V.data(),
+                           B[0].empty() ? nullptr : B[0].data(),
+                           B[1].empty() ? nullptr : B[1].data(),
+                           B[2].empty() ? nullptr : B[2].data());
+  if (rc) return rc;
+  if (t) *t = r.t;
+  if (dt) *dt = r.dt;
+  if (nstep) *nstep = r.nstep;
+  return GP_OK;
 }
 
 }  // extern "C"

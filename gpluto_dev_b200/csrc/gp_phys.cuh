@@ -43,8 +43,8 @@ template <> __device__ __forceinline__ float rsqrt_(float x) { return sqrtf(x); 
 template <typename R> __device__ __forceinline__ R rabs(R x) { return fabs(x); }
 template <> __device__ __forceinline__ float rabs(float x) { return fabsf(x); }
 
-#define GP_MAX(a, b) ((a) >= (b) ? (a) : (b))      // Src/macros.hpp:188
-#define GP_MIN(a, b) ((a) <= (b) ? (a) : (b))      // Src/macros.hpp:191
+#define GP_MAX(a, b) ((a) >= (b) ? (a) : (b))      // Src/macros.hpp:191
+#define GP_MIN(a, b) ((a) <= (b) ? (a) : (b))      // Src/macros.hpp:194
 
 // ---------------------------------------------------------------------
 // PLM slope limiters on a uniform Cartesian grid,

@@ -44,7 +44,8 @@ enum gp_status {
   GP_ERR_CUDA = -3,         /* CUDA runtime error (see gp_last_error) */
   GP_ERR_NOMEM = -4,        /* device allocation failed */
   GP_ERR_QUIT = -5,         /* a kernel raised ERR_QUIT (the reference would QuitPLUTO) */
-  GP_ERR_NO_DEVICE = -6     /* no CUDA device: this library has no CPU path */
+  GP_ERR_NO_DEVICE = -6,    /* no CUDA device: this library has no CPU path */
+  GP_ERR_IO = -7            /* an output or restart file is missing, short or unwritable */
 };
 
 /* PHYSICS (definitions.hpp) */
@@ -147,6 +148,35 @@ int gp_profile_steps(gp_handle *h, int nsteps, double *dt, float *kernel_ms, int
                      int *nkernels);
 /* Name of launch q of a step (as ordered by gp_profile_steps). */
 const char *gp_kernel_name(const gp_handle *h, int q);
+
+/* ---- output and restart in the reference's .dbl format ------------------
+   Replace WriteData for DBL_OUTPUT in single_file mode
+   (Src/write_data.cpp:35-160, 474-503), RestartDump
+   (Src/restart.cpp:423-458) and RestartFromFile/RestartGet
+   (Src/restart.cpp:34-283, 331-411), so that a run on the device and a run
+   of the reference can restart from each other's files.
+
+   gp_write_dbl: writes <dir>/data.<nfile %04d>.dbl (the interior of rho,
+   vx1..vx3, [Bx1..Bx3,] prs, then the staggered Bx1s..Bx<ndim>s with one
+   extra face along their own direction, doubles, x fastest), line nfile of
+   <dir>/dbl.out ("nfile t dt nstep single_file little|big names...") and
+   record nfile of <dir>/restart.out (256-byte Restart records).  t, dt and
+   nstep are the caller's time, the dt of the next step and the step count.
+
+   gp_read_dbl: loads output #nrestart written by either program: Vc and the
+   staggered fields from the data file (byte order from dbl.out), Uc =
+   PrimToCons(Vc) on the device, and returns the record's t, dt (the next
+   step's dt) and nstep.  Errors: GP_ERR_IO for a missing or short file,
+   GP_ERR_UNSUPPORTED for multiple_files output. */
+int gp_write_dbl(gp_handle *h, const char *dir, int nfile, double t, double dt, int nstep);
+int gp_read_dbl(gp_handle *h, const char *dir, int nrestart, double *t, double *dt,
+                int *nstep);
+
+/* DataMinMax (Src/main.cpp:752-900) on the device: per variable minimum and
+   maximum of the primitive state over the domain cells (vmin, vmax: nvar
+   values each, in NVAR order) and the largest Mach number
+   max(|vx1|,|vx2|,|vx3|)/sqrt(prs/rho) (mach_max may be NULL). */
+int gp_data_minmax(gp_handle *h, double *vmin, double *vmax, double *mach_max);
 
 /* Limits of gp_advance_step_noalloc: the largest grid it accepts (cells) and
    the doubles of device scratch it keeps per cell. */

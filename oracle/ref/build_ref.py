@@ -244,6 +244,33 @@ def run_ref(binary: str, ic_path: str, nsteps: int, dump_path: str,
     return read_dump(dump_path)
 
 
+def run_ref_io(binary: str, ic_path: str, every: int, nsteps: int, workdir: str,
+               restart: int | None = None, dump_path: str | None = None,
+               timeout: float | None = None) -> RefDump | None:
+    """Run the reference with .dbl output every ``every`` steps into ``workdir``
+    (data.NNNN.dbl, dbl.out, restart.out), optionally restarting from output
+    #``restart`` found there; stop at step ``nsteps`` and return the state
+    dumped at that step (or None without ``dump_path``)."""
+    binary = os.path.abspath(binary)
+    ini = open(os.path.join(os.path.dirname(binary), "pluto.ini")).read()
+    ini = ini.replace("dbl       -1.0  -1   single_file",
+                      f"dbl       -1.0  {every}   single_file\noutput_dir {workdir}")
+    ip = os.path.join(workdir, "pluto.ini")
+    with open(ip, "w") as f:
+        f.write(ini)
+    env = dict(os.environ, GPLUTO_FTZ_DAZ="0", GP_IC_FILE=os.path.abspath(ic_path),
+               GP_DUMP_STEP=str(nsteps), GP_DUMP_FILE=os.path.abspath(dump_path or
+                                                                     os.path.join(workdir, "x.dump")))
+    cmd = [binary, "-i", ip, "-maxsteps", str(nsteps)]
+    if restart is not None:
+        cmd += ["-restart", str(restart)]
+    out = subprocess.run(cmd, cwd=workdir, env=env, capture_output=True, text=True,
+                         timeout=timeout)
+    if out.returncode != 0:
+        raise RuntimeError(f"reference run failed (rc={out.returncode}):\n{out.stdout[-3000:]}")
+    return read_dump(dump_path) if dump_path else None
+
+
 if __name__ == "__main__":
     cfg = RefConfig(name=sys.argv[1] if len(sys.argv) > 1 else "mhd2d_mc_hlld")
     print(build(cfg, quiet=False))

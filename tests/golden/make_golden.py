@@ -9,6 +9,10 @@ sources compiled in place), writes a seeded initial condition made by
 gpluto_dev_b200/ics.py, runs N steps with FTZ/DAZ off, and stores the
 initial primitive state, the face fields and the reference's final
 Vc/Uc/Vs plus its dt history as ``<name>.npz`` next to this script.
+The output/restart cases (``IO_CASES``, stored under ``io/``) also run the
+reference with .dbl output every few steps and keep its data.0000.dbl,
+data.0001.dbl, dbl.out and restart.out, then restart the reference from
+output #1 and store the state it reaches.
 The fixtures are small so that they can be committed; the GPU box never
 needs the reference tree.
 """
@@ -118,6 +122,55 @@ CASES = {
 }
 
 
+# Output/restart cases: .dbl output every `every` steps, then a restart of
+# the reference from output #1 run to step `nsteps`.
+# name: (generator, kwargs, RefConfig kwargs, every, nsteps)
+IO_CASES = {
+    "io_mhd2d_dbl": (ics.mhd2d_turbulence, dict(n=(24, 16), seed=21),
+                     dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",
+                          ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4), 4, 8),
+    "io_mhd3d_outflowx_dbl": (ics.mhd3d_turbulence, dict(n=(12, 10, 8), seed=22),
+                              dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                   ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4,
+                                   bc=("outflow", "periodic", "periodic")), 3, 6),
+    "io_hd2d_dbl": (ics.hd_turbulence, dict(n=(20, 12), seed=23),
+                    dict(physics="HD", ndim=2, limiter="MC_LIM", solver="hllc",
+                         cfl=0.4, first_dt=1e-4), 3, 6),
+}
+
+
+def make_io(name: str) -> str:
+    """Reference .dbl files of outputs #0 and #1, dbl.out, restart.out, and the
+    reference's own restart from #1 run to step nsteps."""
+    gen, kw, rc, every, nsteps = IO_CASES[name]
+    st = gen(**kw)
+    if rc["ndim"] == 2 and st.ndim == 3:
+        st = _as2d(st)
+    cfg = br.RefConfig(name=ref_cfg_name(rc), n=st.shape, **rc)
+    binary = br.build(cfg)
+    with tempfile.TemporaryDirectory() as tmp:
+        icp = os.path.join(tmp, "ic.bin")
+        ics.write_ic(icp, st)
+        br.run_ref_io(binary, icp, every, every + 1, tmp)
+        files = {f: open(os.path.join(tmp, f), "rb").read()
+                 for f in ("data.0000.dbl", "data.0001.dbl", "dbl.out", "restart.out")}
+        d = br.run_ref_io(binary, icp, every, nsteps, tmp, restart=1,
+                          dump_path=os.path.join(tmp, "rst.dump"))
+    os.makedirs(os.path.join(HERE, "io"), exist_ok=True)
+    out = os.path.join(HERE, "io", f"{name}.npz")
+    u8 = lambda b: np.frombuffer(b, np.uint8)
+    np.savez_compressed(
+        out, physics=st.physics, ndim=st.ndim, shape=np.array(st.shape), gamma=st.gamma,
+        V0=st.V, Bs0=np.array(st.Bs) if st.Bs else np.zeros(0),
+        dbl0=u8(files["data.0000.dbl"]), dbl1=u8(files["data.0001.dbl"]),
+        dbl_out=u8(files["dbl.out"]), restart_out=u8(files["restart.out"]),
+        rst_V=d.V, rst_U=d.U, rst_Bs=np.array(d.Bs) if d.Bs else np.zeros(0), rst_dt=d.dt,
+        every=every, nsteps=nsteps, limiter=rc["limiter"], solver=rc["solver"],
+        ct=rc.get("ct_emf", "none"), cfl=rc["cfl"], cfl_max_var=1.1, first_dt=rc["first_dt"],
+        reconstruction=rc.get("reconstruction", "LINEAR"), outflow=outflow_mask(rc))
+    return out
+
+
 def ref_cfg_name(rc: dict) -> str:
     lim = "ppm" if rc.get("reconstruction") == "PARABOLIC" else rc["limiter"]
     return "{physics}{ndim}d_{lim}_{solver}_{ct}".format(
@@ -168,7 +221,7 @@ def make(name: str) -> str:
 
 
 if __name__ == "__main__":
-    names = sys.argv[1:] or list(CASES)
+    names = sys.argv[1:] or list(CASES) + list(IO_CASES)
     for nm in names:
-        p = make(nm)
+        p = make_io(nm) if nm in IO_CASES else make(nm)
         print(f"{nm}: {os.path.getsize(p)/1024:.0f} KiB")
