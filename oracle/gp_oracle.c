@@ -735,6 +735,52 @@ static void Boundary(orc_t *o) {
       }
       continue;
     }
+    if (((o->c.reflect | o->c.eqtsym) >> side) & 1) {
+      /* ReflectiveBoundary with the signs of FlipSign
+         (Src/boundary.cpp:203-216, 838-900, 931-1060): ghost cell m copies
+         its mirror image i0 - m; REFLECTIVE (and AXISYMMETRIC, the same in
+         Cartesian geometry) flips v_n and B_n, EQTSYMMETRIC flips v_n, B_t
+         and B_b.  Normal faces mirror across the boundary face (which keeps
+         its value), tangential faces like the cells, one face wider. */
+      int eqt = (o->c.eqtsym >> side) & 1;
+      double vsign[8];
+      int i0 = beg ? 2*o->beg[d] - 1 : 2*o->end[d] + 1;
+      for (nv = 0; nv < o->nvar; nv++) vsign[nv] = 1.0;
+      vsign[VX1 + d] = -1.0;
+      if (isMHD) {
+        if (eqt) { vsign[BX1 + (d+1)%3] = -1.0; vsign[BX1 + (d+2)%3] = -1.0; }
+        else     vsign[BX1 + d] = -1.0;
+      }
+      for (nv = 0; nv < o->nvar; nv++)
+        for (k = lo[2]; k <= hi[2]; k++)
+        for (j = lo[1]; j <= hi[1]; j++)
+        for (i = lo[0]; i <= hi[0]; i++) {
+          int s[3] = {i, j, k}; s[d] = i0 - s[d];
+          *VC(o, o->Vc, nv, i, j, k) = vsign[nv] * *VC(o, o->Vc, nv, s[0], s[1], s[2]);
+        }
+      if (isMHD) {
+        int c;
+        for (c = 0; c < o->c.ndim; c++) {
+          int h[3] = {hi[0], hi[1], hi[2]};
+          if (c != d) h[c] += 1;
+          for (k = lo[2]; k <= h[2]; k++)
+          for (j = lo[1]; j <= h[1]; j++)
+          for (i = lo[0]; i <= h[0]; i++) {
+            int t[3] = {i, j, k}, s[3] = {i, j, k};
+            if (c == d) {
+              if (beg) s[d] = i0 - t[d] + 1;         /* face m from face i0-m+1 */
+              else   { t[d] += 1; s[d] = i0 - i*(d==0) - j*(d==1) - k*(d==2); }
+            } else {
+              s[d] = i0 - t[d];
+            }
+            o->Vs[c][SI(o,c,t[0],t[1],t[2])] = vsign[BX1 + c] * o->Vs[c][SI(o,c,s[0],s[1],s[2])];
+          }
+        }
+        /* Src/boundary.cpp:260-307: ghost cell B from faces, copied to Vc */
+        AverageStaggered(o, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], 1);
+      }
+      continue;
+    }
     for (nv = 0; nv < o->nvar; nv++)
       for (k = lo[2]; k <= hi[2]; k++)
       for (j = lo[1]; j <= hi[1]; j++)

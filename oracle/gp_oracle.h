@@ -19,7 +19,9 @@ typedef struct {
   double gamma;
   double dx[3];
   double cfl, cfl_max_var;
-  int outflow;   /* bit 2d / 2d+1: low / high side of direction d is OUTFLOW (HD) */
+  int outflow;   /* bit 2d / 2d+1: low / high side of direction d is OUTFLOW */
+  int reflect;   /* same bits: REFLECTIVE (or AXISYMMETRIC, identical in Cartesian) */
+  int eqtsym;    /* same bits: EQTSYMMETRIC */
 } orc_cfg;
 
 void    *orc_create(const orc_cfg *cfg);

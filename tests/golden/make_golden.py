@@ -119,6 +119,35 @@ CASES = {
                                dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
                                     ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
                                     reconstruction="PARABOLIC"), 8),
+    # reflective and equatorially symmetric sides (ReflectiveBoundary)
+    "mhd2d_mc_hlld_ucthlld_reflectx": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=71),
+                                       dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",
+                                            ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4,
+                                            bc=("reflective", "periodic", "periodic")), 12),
+    "mhd2d_mc_hlld_ucthlld_reflectx_outflowy": (
+        ics.mhd2d_turbulence, dict(n=(24, 20), seed=77),
+        dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld", ct_emf="UCT_HLLD", cfl=0.4,
+             first_dt=1e-4, bc=("reflective", "outflow", "periodic")), 12),
+    "mhd2d_vl_hll_ucthll_eqtsymy": (ics.mhd2d_turbulence, dict(n=(20, 24), seed=73),
+                                    dict(physics="MHD", ndim=2, limiter="VANLEER_LIM", solver="hll",
+                                         ct_emf="UCT_HLL", cfl=0.4, first_dt=1e-4,
+                                         bc=("periodic", "eqtsymmetric", "periodic")), 12),
+    "mhd3d_blast_mc_hlld_reflect": (ics.mhd3d_blast, dict(n=(14, 12, 10), seed=72, radius=0.25),
+                                    dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                         ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4,
+                                         bc=("reflective", "reflective", "reflective")), 8),
+    "hd2d_mc_hllc_reflect": (ics.hd_turbulence, dict(n=(22, 18), seed=74),
+                             dict(physics="HD", ndim=2, limiter="MC_LIM", solver="hllc", cfl=0.4,
+                                  first_dt=1e-4, bc=("reflective", "reflective", "periodic")), 12),
+    "hd3d_ppm_hllc_reflectz": (ics.hd_turbulence, dict(n=(12, 10, 9), seed=75),
+                               dict(physics="HD", ndim=3, limiter="MC_LIM", solver="hllc", cfl=0.4,
+                                    first_dt=1e-4, reconstruction="PARABOLIC",
+                                    bc=("periodic", "periodic", "reflective")), 8),
+    "rmhd3d_mc_hlld_ucthll_reflectx": (ics.rmhd3d_turbulence, dict(n=(10, 8, 8), seed=76,
+                                                                   lorentz_max=3.0),
+                                       dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                            ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
+                                            bc=("reflective", "periodic", "periodic")), 6),
 }
 
 
@@ -186,13 +215,17 @@ def _as2d(st):
     return ics.PrimState(st.physics, 2, (st.shape[0], st.shape[1], 1), st.gamma, V, Bs)
 
 
-def outflow_mask(rc: dict) -> int:
-    """Bits 2d and 2d+1 set for each direction d with outflow sides."""
+def side_mask(rc: dict, kinds=("outflow",)) -> int:
+    """Bits 2d and 2d+1 set for each direction d whose sides are of `kinds`."""
     m = 0
     for d, t in enumerate(rc.get("bc", ("periodic",) * 3)):
-        if t == "outflow" and d < rc["ndim"]:
+        if t in kinds and d < rc["ndim"]:
             m |= 3 << (2 * d)
     return m
+
+
+def outflow_mask(rc: dict) -> int:
+    return side_mask(rc, ("outflow",))
 
 
 def make(name: str) -> str:
@@ -216,7 +249,9 @@ def make(name: str) -> str:
         V=d.V, U=d.U, Bs=np.array(d.Bs) if d.Bs else np.zeros(0), dt=d.dt, nsteps=nsteps,
         limiter=rc["limiter"], solver=rc["solver"], ct=rc.get("ct_emf", "none"),
         cfl=rc["cfl"], cfl_max_var=1.1, first_dt=rc["first_dt"],
-        reconstruction=rc.get("reconstruction", "LINEAR"), outflow=outflow_mask(rc))
+        reconstruction=rc.get("reconstruction", "LINEAR"), outflow=outflow_mask(rc),
+        reflect=side_mask(rc, ("reflective", "axisymmetric")),
+        eqtsym=side_mask(rc, ("eqtsymmetric",)))
     return out
 
 

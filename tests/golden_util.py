@@ -41,5 +41,9 @@ class Golden:
         self.first_dt = float(z["first_dt"])
         self.reconstruction = str(z["reconstruction"]) if "reconstruction" in z else "LINEAR"
         self.outflow = int(z["outflow"]) if "outflow" in z else 0
+        self.reflect = int(z["reflect"]) if "reflect" in z else 0
+        self.eqtsym = int(z["eqtsym"]) if "eqtsym" in z else 0
+        # side types as keyword arguments of the oracle and of api.Solver
+        self.bc = dict(outflow=self.outflow, reflect=self.reflect, eqtsym=self.eqtsym)
         if self.reconstruction == "PARABOLIC":
             self.limiter = "ppm"
