@@ -24,6 +24,7 @@ LIB_PATH = os.environ.get("GPLUTO_B200_LIB") or os.path.join(_HERE, "_build",
                                                              "libgpluto_b200.so")
 
 GP_OK, GP_ERR_INVALID, GP_ERR_QUIT, GP_ERR_NO_DEVICE, GP_ERR_IO = 0, -1, -5, -6, -7
+BC_PERIODIC, BC_OUTFLOW, BC_REFLECTIVE, BC_AXISYMMETRIC, BC_EQTSYMMETRIC = 0, 1, 2, 3, 4
 HD, MHD, RMHD = 0, 1, 2
 # "ppm" selects RECONSTRUCTION PARABOLIC (the limiter then plays no part)
 LIMITERS = {"flat": 0, "minmod": 1, "vl": 2, "vanleer": 2, "mc": 3, "ppm": 3}
@@ -154,9 +155,11 @@ class Solver:
     """Device-resident state of one grid and its Godunov step."""
 
     def __init__(self, ndim: int, shape, scheme: Scheme, xbeg=(0.0, 0.0, 0.0),
-                 xend=(1.0, 1.0, 1.0), nghost: int = 2, stream=None, outflow: int = 0):
-        """``outflow``: bit 2d (2d+1) makes the low (high) side of direction d
-        an OUTFLOW boundary; other sides are periodic."""
+                 xend=(1.0, 1.0, 1.0), nghost: int = 2, stream=None, outflow: int = 0,
+                 reflect: int = 0, eqtsym: int = 0):
+        """Side masks: bit 2d (2d+1) of ``outflow`` / ``reflect`` / ``eqtsym``
+        makes the low (high) side of direction d an OUTFLOW / REFLECTIVE /
+        EQTSYMMETRIC boundary; other sides are periodic."""
         g = GpGridDesc()
         g.ndim = ndim
         nx, ny, nz = (tuple(shape) + (1, 1, 1))[:3]
@@ -164,9 +167,17 @@ class Solver:
         g.nghost = nghost
         for d in range(3):
             g.xbeg[d], g.xend[d] = xbeg[d], xend[d]
-            g.lbound[d] = (outflow >> (2 * d)) & 1
-            g.rbound[d] = (outflow >> (2 * d + 1)) & 1
-        self.outflow = outflow
+            for e, attr in ((0, "lbound"), (1, "rbound")):
+                bit = 2 * d + e
+                t = BC_PERIODIC
+                if (outflow >> bit) & 1:
+                    t = BC_OUTFLOW
+                elif (reflect >> bit) & 1:
+                    t = BC_REFLECTIVE
+                elif (eqtsym >> bit) & 1:
+                    t = BC_EQTSYMMETRIC
+                getattr(g, attr)[d] = t
+        self.outflow, self.reflect, self.eqtsym = outflow, reflect, eqtsym
         self.ndim, self.shape = ndim, (nx, ny, nz if ndim == 3 else 1)
         self.scheme = scheme
         self.nvar = 5 if scheme.physics == HD else 8

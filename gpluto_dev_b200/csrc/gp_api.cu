@@ -174,8 +174,32 @@ __device__ __forceinline__ SideGeom side_geom(const Pad& p, int d) {
   return s;
 }
 
+// cell-centred B of the side's ghost cells at transverse position (ta, tb)
+// from the faces around each (Src/MHD/CT/ct_field_average.cpp:175-200)
+__device__ void ghost_average(const SideGeom& s, double* V, double* const* B, int ndim, int ta,
+                              int tb, int beg) {
+  const int d = s.d, a = s.a, b = s.b;
+  const int L = s.L[d], N = s.N[d], P = s.P[d];
+  const int g0 = beg ? 0 : L + N, g1 = beg ? L - 1 : P - 1;
+  for (int g = g0; g <= g1; g++) {
+    const long long c = s.idx(g, ta, tb);
+    for (int e = 0; e < ndim; e++) {
+      long long cn;
+      if (e == d) {
+        if (g + 1 >= P) continue;  // the extra padding cell: not a reference ghost
+        cn = s.idx(g + 1, ta, tb);
+      } else if (e == a) {
+        cn = s.idx(g, (ta + 1) % s.P[a], tb);
+      } else {
+        cn = s.idx(g, ta, (tb + 1) % s.P[b]);
+      }
+      V[(kBX1 + e) * s.pn + c] = 0.5 * (B[e][c] + B[e][cn]);
+    }
+  }
+}
+
 __global__ void outflow_copy_kernel(double* __restrict__ V, int nvar, double* B0, double* B1,
-                                    double* B2, int ndim, Pad p, int d, int beg) {
+                                    double* B2, int nb, Pad p, int d, int beg) {
   const SideGeom s = side_geom(p, d);
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)s.P[s.a] * s.P[s.b]) return;
@@ -187,7 +211,7 @@ __global__ void outflow_copy_kernel(double* __restrict__ V, int nvar, double* B0
   for (int g = g0; g <= g1; g++) {
     const long long c = s.idx(g, ta, tb);
     for (int nv = 0; nv < nvar; nv++) V[nv * s.pn + c] = V[nv * s.pn + c0];
-    for (int e = 0; e < ndim; e++)
+    for (int e = 0; e < nb; e++)
       if (e != d) B[e][c] = B[e][c0];
   }
 }
@@ -218,22 +242,58 @@ __global__ void outflow_march_kernel(double* __restrict__ V, double* B0, double*
     for (int m = L + N; m + 1 < P; m++)
       B[d][s.idx(m + 1, ta, tb)] = (A[d] * B[d][s.idx(m, ta, tb)] - (dB(a, m) + dB(b, m))) / A[d];
   }
-  const int g0 = beg ? 0 : L + N, g1 = beg ? L - 1 : P - 1;
+  ghost_average(s, V, B, ndim, ta, tb, beg);
+}
+
+// Mirrored side of a padded grid (ReflectiveBoundary with the signs of
+// FlipSign, Src/boundary.cpp:838-1060): ghost cell g copies its mirror image
+// across the boundary face times the variable's sign (bit nv of `flip`
+// set: -1); the normal staggered field mirrors across the boundary face,
+// which keeps its value; tangential faces mirror like the cells.  The extra
+// high-side padding cell (not a reference ghost) repeats the last ghost.
+__global__ void reflect_copy_kernel(double* __restrict__ V, int nvar, double* B0, double* B1,
+                                    double* B2, int nb, Pad p, int d, int beg, unsigned flip) {
+  const SideGeom s = side_geom(p, d);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)s.P[s.a] * s.P[s.b]) return;
+  const int ta = (int)(t % s.P[s.a]), tb = (int)(t / s.P[s.a]);
+  const int L = s.L[d], N = s.N[d], P = s.P[d];
+  double* B[3] = {B0, B1, B2};
+  auto sgn = [&](int nv) -> double { return ((flip >> nv) & 1u) ? -1.0 : 1.0; };
+  const int g0 = beg ? 0 : L + N, g1 = beg ? L - 1 : L + N + L - 1;   // reference ghosts
+  const int i0 = beg ? 2 * L - 1 : 2 * (L + N - 1) + 1;              // mirror of g: i0 - g
   for (int g = g0; g <= g1; g++) {
-    const long long c = s.idx(g, ta, tb);
-    for (int e = 0; e < ndim; e++) {
-      long long cn;
-      if (e == d) {
-        if (g + 1 >= P) continue;  // the extra padding cell: not a reference ghost
-        cn = s.idx(g + 1, ta, tb);
-      } else if (e == a) {
-        cn = s.idx(g, (ta + 1) % s.P[a], tb);
+    const long long c = s.idx(g, ta, tb), cm = s.idx(i0 - g, ta, tb);
+    for (int nv = 0; nv < nvar; nv++) V[nv * s.pn + c] = sgn(nv) * V[nv * s.pn + cm];
+    for (int e = 0; e < nb; e++) {
+      const double se = sgn(kBX1 + e);
+      if (e != d) {
+        B[e][c] = se * B[e][cm];
+      } else if (beg) {
+        B[e][c] = se * B[e][s.idx(i0 - g + 1, ta, tb)];        // face g from face i0-g+1
       } else {
-        cn = s.idx(g, ta, (tb + 1) % s.P[b]);
+        B[e][s.idx(g + 1, ta, tb)] = se * B[e][cm];             // face g+1 from face i0-g
       }
-      V[(kBX1 + e) * s.pn + c] = 0.5 * (B[e][c] + B[e][cn]);
     }
   }
+  if (!beg && P - 1 > g1) {  // the extra padding cell: finite copies of the last ghost
+    const long long c = s.idx(P - 1, ta, tb), cl = s.idx(g1, ta, tb);
+    for (int nv = 0; nv < nvar; nv++) V[nv * s.pn + c] = V[nv * s.pn + cl];
+    for (int e = 0; e < nb; e++)
+      if (e != d) B[e][c] = B[e][cl];
+  }
+}
+
+// Ghost cells' B from their faces (Src/boundary.cpp:260-307), after the
+// side's faces are all set: its own launch, since it reads the tangential
+// faces of the neighbouring positions.
+__global__ void ghost_average_kernel(double* __restrict__ V, double* B0, double* B1, double* B2,
+                                     int ndim, Pad p, int d, int beg) {
+  const SideGeom s = side_geom(p, d);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)s.P[s.a] * s.P[s.b]) return;
+  double* B[3] = {B0, B1, B2};
+  ghost_average(s, V, B, ndim, (int)(t % s.P[s.a]), (int)(t / s.P[s.a]), beg);
 }
 
 bool uniform(const double* dx, int n) {
@@ -272,6 +332,8 @@ struct gp_handle {
   size_t stage_bytes;
   int launches_per_step;
   unsigned outflow;      // outflow sides (bit 2d low, 2d+1 high)
+  unsigned reflect;      // reflective (or axisymmetric) sides, same bits
+  unsigned eqtsym;       // equatorially symmetric sides, same bits
   // Outflow with constrained transport pads the outflow directions with
   // ghost cells filled before every stage (S = ghost cells of the scheme,
   // plus one on the high side so that the outermost ghost's faces exist).
@@ -321,21 +383,39 @@ gp::GridDims grid_dims(const gp_handle* h) {
   return g;
 }
 
-// ghost zones of the outflow sides of a padded grid, sides in the
-// reference's order (Src/boundary.cpp:144-190)
-void fill_outflow(gp_handle* h, double* const* Bs) {
+// ghost zones of the non-periodic sides of a padded grid, sides in the
+// reference's order (Src/boundary.cpp:144-310)
+void fill_boundaries(gp_handle* h, double* const* Bs) {
   const Pad p = pad_of(h);
   const int P[3] = {h->px, h->py, h->pz};
+  const int nb = h->scheme.physics == GP_HD ? 0 : h->ndim;  // staggered components
   for (int side = 0; side < 2 * h->ndim; side++) {
-    if (!((h->outflow >> side) & 1u)) continue;
+    const unsigned bit = 1u << side;
+    if (!((h->outflow | h->reflect | h->eqtsym) & bit)) continue;
     const int d = side / 2, beg = side % 2 == 0;
     const int a = (d == 0) ? 1 : 0, b = (d == 2) ? 1 : 2;
     const long long nt = (long long)P[a] * P[b];
-    const unsigned nb = (unsigned)((nt + 127) / 128);
-    outflow_copy_kernel<<<nb, 128, 0, h->stream>>>(h->V, h->nvar, Bs[0], Bs[1], Bs[2], h->ndim,
-                                                   p, d, beg);
-    outflow_march_kernel<<<nb, 128, 0, h->stream>>>(h->V, Bs[0], Bs[1], Bs[2], h->ndim, p, d,
-                                                    beg, h->A[0], h->A[1], h->A[2]);
+    const unsigned nblk = (unsigned)((nt + 127) / 128);
+    if (h->outflow & bit) {
+      outflow_copy_kernel<<<nblk, 128, 0, h->stream>>>(h->V, h->nvar, Bs[0], Bs[1], Bs[2], nb,
+                                                       p, d, beg);
+      if (nb)
+        outflow_march_kernel<<<nblk, 128, 0, h->stream>>>(h->V, Bs[0], Bs[1], Bs[2], h->ndim, p,
+                                                          d, beg, h->A[0], h->A[1], h->A[2]);
+      continue;
+    }
+    // FlipSign (Src/boundary.cpp:838-920): v_n always; B_n for REFLECTIVE
+    // (and AXISYMMETRIC), B_t and B_b for EQTSYMMETRIC
+    unsigned flip = 1u << (1 + d);                                    // VX1 + d
+    if (nb) {
+      if (h->eqtsym & bit) flip |= (1u << (kBX1 + (d + 1) % 3)) | (1u << (kBX1 + (d + 2) % 3));
+      else flip |= 1u << (kBX1 + d);
+    }
+    reflect_copy_kernel<<<nblk, 128, 0, h->stream>>>(h->V, h->nvar, Bs[0], Bs[1], Bs[2], nb, p,
+                                                     d, beg, flip);
+    if (nb)
+      ghost_average_kernel<<<nblk, 128, 0, h->stream>>>(h->V, Bs[0], Bs[1], Bs[2], h->ndim, p, d,
+                                                        beg);
   }
 }
 
@@ -365,7 +445,7 @@ int enqueue_step(gp_handle* h, double* hist, int slot, cudaEvent_t* ev = nullptr
                     : gp::launch_stage_fp64(sd, g, h->key, h->seg, h->stream, e);
   };
   // stage 1: (U^n, B^n) -> (U1, B1)
-  if (h->padded) fill_outflow(h, h->Bs[b0]);
+  if (h->padded) fill_boundaries(h, h->Bs[b0]);
   d.stage = 1;
   d.V = h->V;
   d.Vout = h->V;
@@ -379,7 +459,7 @@ int enqueue_step(gp_handle* h, double* hist, int slot, cudaEvent_t* ev = nullptr
   }
   if (launch(d) != 0) return fail(GP_ERR_UNSUPPORTED, "scheme not compiled");
   // stage 2: (U^n, U1, B^n, B1) -> (U^{n+1} in place of U^n, B^{n+1})
-  if (h->padded) fill_outflow(h, h->Bs[b1]);
+  if (h->padded) fill_boundaries(h, h->Bs[b1]);
   d.stage = 2;
   d.Uc = h->U[1];
   d.Uout = h->U[0];
@@ -448,9 +528,11 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
     if (d < grid->ndim) {
       if (grid->nint[d] < 2) return fail(GP_ERR_INVALID, "nint[%d] < 2", d);
       const int lb = grid->lbound[d], rb = grid->rbound[d];
-      if ((lb != GP_BC_PERIODIC && lb != GP_BC_OUTFLOW) ||
-          (rb != GP_BC_PERIODIC && rb != GP_BC_OUTFLOW))
-        return fail(GP_ERR_UNSUPPORTED, "boundary types are periodic or outflow");
+      if (lb < GP_BC_PERIODIC || lb > GP_BC_EQTSYMMETRIC || rb < GP_BC_PERIODIC ||
+          rb > GP_BC_EQTSYMMETRIC)
+        return fail(GP_ERR_UNSUPPORTED,
+                    "boundary types are periodic, outflow, reflective, axisymmetric or "
+                    "eqtsymmetric");
       if ((lb == GP_BC_PERIODIC) != (rb == GP_BC_PERIODIC))
         return fail(GP_ERR_INVALID, "a periodic direction needs both sides periodic");
 
@@ -484,17 +566,28 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   h->nz = grid->ndim == 3 ? grid->nint[2] : 1;
   h->n = (long long)h->nx * h->ny * h->nz;
   for (int d = 0; d < grid->ndim; d++) {
-    if (grid->lbound[d] == GP_BC_OUTFLOW) h->outflow |= 1u << (2 * d);
-    if (grid->rbound[d] == GP_BC_OUTFLOW) h->outflow |= 1u << (2 * d + 1);
+    const int t[2] = {grid->lbound[d], grid->rbound[d]};
+    for (int e = 0; e < 2; e++) {
+      const unsigned bit = 1u << (2 * d + e);
+      if (t[e] == GP_BC_OUTFLOW) h->outflow |= bit;
+      // AXISYMMETRIC flips the same components as REFLECTIVE in Cartesian
+      // geometry (FlipSign, Src/boundary.cpp:838-920)
+      if (t[e] == GP_BC_REFLECTIVE || t[e] == GP_BC_AXISYMMETRIC) h->reflect |= bit;
+      if (t[e] == GP_BC_EQTSYMMETRIC) h->eqtsym |= bit;
+    }
   }
-  // outflow with constrained transport: pad the outflow directions
-  h->padded = h->outflow != 0 && scheme->physics != GP_HD;
+  // Non-periodic directions are padded with stored ghost cells filled before
+  // every stage: with constrained transport (the staggered field's ghost
+  // faces), and for mirrored sides of every physics.  HD outflow alone keeps
+  // the clamped ghost index of the sweeps.
+  const unsigned nonper = h->outflow | h->reflect | h->eqtsym;
+  h->padded = (h->reflect | h->eqtsym) != 0 || (h->outflow != 0 && scheme->physics != GP_HD);
   {
     const int S = scheme->reconstruction == GP_REC_PARABOLIC ? 3 : 2;
     const int nn[3] = {h->nx, h->ny, h->nz};
     int pp[3];
     for (int d = 0; d < 3; d++) {
-      const bool pd = h->padded && d < grid->ndim && ((h->outflow >> (2 * d)) & 3u);
+      const bool pd = h->padded && d < grid->ndim && ((nonper >> (2 * d)) & 3u);
       h->lo[d] = pd ? S : 0;
       h->hi[d] = pd ? S + 1 : 0;
       pp[d] = nn[d] + h->lo[d] + h->hi[d];
@@ -575,14 +668,15 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   h->bcur = 0;
   {
     int fills = 0;
-    for (int side = 0; side < 2 * h->ndim; side++) fills += 2 * (h->padded && ((h->outflow >> side) & 1u));
+    for (int side = 0; side < 2 * h->ndim; side++)
+      if (h->padded && ((nonper >> side) & 1u)) fills += scheme->physics == GP_HD ? 1 : 2;
     h->launches_per_step = 2 * (gp::stage_launch_count(h->key) + fills) + 1;
   }
   if (h->padded) {  // padding cells start finite
     cudaMemsetAsync(h->V, 0, cell * h->nvar, h->stream);
     cudaMemsetAsync(h->U[0], 0, cell * h->nvar, h->stream);
     cudaMemsetAsync(h->U[1], 0, cell * h->nvar, h->stream);
-    for (int b = 0; b < 3; b++)
+    for (int b = 0; b < 3 && scheme->physics != GP_HD; b++)
       for (int d = 0; d < h->ndim; d++) cudaMemsetAsync(h->Bs[b][d], 0, cell, h->stream);
   }
   *out = h;
@@ -731,7 +825,7 @@ int gp_download_state(gp_handle* h, int layout, double* Uc, double* Vc, double* 
   if (!h) return fail(GP_ERR_INVALID, "null handle");
   int rc;
   // ghost zones of the current state, as Boundary() would fill them
-  if (h->padded && layout == GP_LAYOUT_REFERENCE) fill_outflow(h, h->Bs[h->bcur]);
+  if (h->padded && layout == GP_LAYOUT_REFERENCE) fill_boundaries(h, h->Bs[h->bcur]);
   if (Uc && (rc = download_one(h, layout, h->U[0], Uc, h->nvar, -1, true))) return rc;
   if (Vc && (rc = download_one(h, layout, h->V, Vc, h->nvar, -1))) return rc;
   if (h->scheme.physics != GP_HD) {

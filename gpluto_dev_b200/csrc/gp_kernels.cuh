@@ -1128,14 +1128,12 @@ __device__ __forceinline__ double finish_cell(const StageArgs<CTT>& a, const Gri
     for (int nv = 0; nv < NV; nv++)
       if (isnan(u[nv])) err |= ERR_NAN | ERR_QUIT;
     bool dom = true;  // a domain cell (not padding)
-    if constexpr (PHYS != PHYS_HD) {
-      if (g.ihi[0] != kNoLimit || g.ihi[1] != kNoLimit || g.ihi[2] != kNoLimit) {
-        const int i = (int)(c % g.nx);
-        const int j = (int)((c / g.nx) % g.ny);
-        const int k = (int)(c / ((long long)g.nx * g.ny));
-        dom = i >= g.ilo[0] && i <= g.ihi[0] && j >= g.ilo[1] && j <= g.ihi[1] &&
-              k >= g.ilo[2] && k <= g.ihi[2];
-      }
+    if (g.ihi[0] != kNoLimit || g.ihi[1] != kNoLimit || g.ihi[2] != kNoLimit) {
+      const int i = (int)(c % g.nx);
+      const int j = (int)((c / g.nx) % g.ny);
+      const int k = (int)(c / ((long long)g.nx * g.ny));
+      dom = i >= g.ilo[0] && i <= g.ihi[0] && j >= g.ilo[1] && j <= g.ihi[1] &&
+            k >= g.ilo[2] && k <= g.ihi[2];
     }
     uint32_t le;
     if constexpr (PHYS == PHYS_MHD) le = mhd_cons2prim(u, v, a.gamma, a.small_rho, a.small_prs);

@@ -58,7 +58,8 @@ enum { GP_RS_HLL = 0, GP_RS_HLLC = 1, GP_RS_HLLD = 2 };
 enum { GP_CT_UCT_HLL = 0, GP_CT_UCT_HLLD = 1 };
 /* [Boundary] types (Src/boundary.cpp): periodic, or outflow (zero-gradient
    ghost copy, OutflowBoundary Src/boundary.cpp:677-780; built for HD) */
-enum { GP_BC_PERIODIC = 0, GP_BC_OUTFLOW = 1 };
+enum { GP_BC_PERIODIC = 0, GP_BC_OUTFLOW = 1, GP_BC_REFLECTIVE = 2, GP_BC_AXISYMMETRIC = 3,
+       GP_BC_EQTSYMMETRIC = 4 };
 /* RECONSTRUCTION (definitions.hpp): LINEAR (PLM with LIMITER) or PARABOLIC
    (PPM, Src/States/ppm_states.cpp) */
 enum { GP_REC_LINEAR = 0, GP_REC_PARABOLIC = 1 };

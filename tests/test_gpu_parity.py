@@ -22,16 +22,16 @@ def rel_linf(a, b):
 
 
 def make_solver(st, limiter, solver, ct, cfl=0.4, cfl_max_var=1.1, precision=api.FP64,
-                outflow=0):
+                outflow=0, reflect=0, eqtsym=0):
     sch = api.Scheme(physics=st.physics, limiter=limiter, riemann=solver, ct_emf=ct,
                      precision=precision, gamma=st.gamma, cfl=cfl, cfl_max_var=cfl_max_var)
-    return api.Solver.from_state(st, sch, outflow=outflow)
+    return api.Solver.from_state(st, sch, outflow=outflow, reflect=reflect, eqtsym=eqtsym)
 
 
 @pytest.mark.parametrize("name", [n for n in gu.names() if not n.startswith("rmhd")])
 def test_gpu_matches_reference_fixture_bitwise(name):
     g = gu.Golden(name)
-    s = make_solver(g.ic, g.limiter, g.solver, g.ct, g.cfl, g.cfl_max_var, outflow=g.outflow)
+    s = make_solver(g.ic, g.limiter, g.solver, g.ct, g.cfl, g.cfl_max_var, **g.bc)
     dt_after, hist, out = s.run(g.nsteps, g.first_dt)
     V, U, Bs = s.download()
     assert out.err_bits & api.ERR_QUIT == 0
@@ -128,6 +128,48 @@ def test_gpu_ct_outflow_matches_oracle_bitwise(case):
     ohist, oerr = o.run(nsteps, 1e-4)
     Vo, Uo, Bo = o.state()
     s = make_solver(st, lim, rs, ct, outflow=ob)
+    dt_after, hist, out = s.run(nsteps, 1e-4)
+    V, U, Bs = s.download()
+    assert out.err_bits == oerr
+    np.testing.assert_array_equal(hist, ohist[:-1])
+    np.testing.assert_array_equal(V, Vo)
+    np.testing.assert_array_equal(U, Uo)
+    for a, b in zip(Bs, Bo):
+        np.testing.assert_array_equal(a, b)
+
+
+MIRROR_CASES = [
+    # (generator, kwargs, limiter, solver, ct, dict of side masks, nsteps): odd
+    # sizes, mirrored sides alone, with outflow, all sides, HD PPM
+    (ics.mhd2d_turbulence, dict(n=(33, 21), seed=81), "mc", "hlld", "uct_hlld",
+     dict(reflect=0b0011), 10),
+    (ics.mhd2d_turbulence, dict(n=(20, 27), seed=82), "ppm", "hlld", "uct_hlld",
+     dict(reflect=0b0001, outflow=0b0010, eqtsym=0b1100), 10),
+    (ics.mhd3d_turbulence, dict(n=(11, 10, 9), seed=83), "mc", "hlld", "uct_hlld",
+     dict(reflect=0b110011, eqtsym=0b001100), 6),
+    (ics.mhd3d_blast, dict(n=(16, 14, 12), seed=84, radius=0.25), "vl", "hll", "uct_hll",
+     dict(reflect=0b111111), 6),
+    (ics.hd_turbulence, dict(n=(13, 11, 9), seed=85), "ppm", "hllc", "uct_hll",
+     dict(reflect=0b110000, outflow=0b000011), 8),
+    (ics.hd_turbulence, dict(n=(31, 17), seed=86), "mc", "hll", "uct_hll",
+     dict(reflect=0b1111), 12),
+]
+
+
+@pytest.mark.parametrize("case", range(len(MIRROR_CASES)))
+def test_gpu_mirrored_sides_match_oracle_bitwise(case):
+    """Reflective / eqtsymmetric sides (mixed with outflow and periodic ones):
+    padded ghost zones filled before every stage by mirror copies with the
+    reference's signs, then the ghost cells' B averaged from their faces."""
+    gen, kw, lim, rs, ct, bc, nsteps = MIRROR_CASES[case]
+    st = gen(**kw)
+    kwo = dict(limiter=lim, solver=rs, **bc)
+    if st.physics != ics.PHYS_HD:
+        kwo["ct"] = ct
+    o = orc.Oracle(st, **kwo)
+    ohist, oerr = o.run(nsteps, 1e-4)
+    Vo, Uo, Bo = o.state()
+    s = make_solver(st, lim, rs, ct, **bc)
     dt_after, hist, out = s.run(nsteps, 1e-4)
     V, U, Bs = s.download()
     assert out.err_bits == oerr
