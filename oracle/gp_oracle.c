@@ -1125,7 +1125,31 @@ static void ConsToPrim3D(orc_t *o) {
   }
 }
 
-/* Src/rk_step.cpp:88-593 (RK2 branch) */
+/* U = w0 U0 + w1 U + wr Rc and the same for the faces, then the cell-centred
+   B from the faces (Src/rk_step.cpp:509-552) */
+static void Combine(orc_t *o, double w0, double w1, double wr) {
+  const int ndim = o->c.ndim, nvar = o->nvar;
+  int i, j, k, nv, d;
+  for (nv = 0; nv < nvar; nv++)
+    for (k = o->beg[2]; k <= o->end[2]; k++)
+    for (j = o->beg[1]; j <= o->end[1]; j++)
+    for (i = o->beg[0]; i <= o->end[0]; i++) {
+      double *u = VC(o, o->Uc, nv, i, j, k);
+      *u = w0*(*VC(o, o->U0, nv, i, j, k)) + w1*(*u) + wr*(*VC(o, o->Rc, nv, i, j, k));
+    }
+  if (o->c.physics != ORC_HD) {
+    for (k = o->beg[2]; k <= o->end[2] + (ndim == 3); k++)
+    for (j = o->beg[1]; j <= o->end[1] + 1; j++)
+    for (i = o->beg[0]; i <= o->end[0] + 1; i++)
+      for (d = 0; d < ndim; d++) {
+        long s = SI(o, d, i, j, k);
+        o->Vs[d][s] = w0*o->Bs0[d][s] + w1*o->Vs[d][s] + wr*o->Rs[d][s];
+      }
+    AverageStaggered(o, o->beg[0], o->end[0], o->beg[1], o->end[1], o->beg[2], o->end[2], 0);
+  }
+}
+
+/* Src/rk_step.cpp:88-743 (RK2 and RK3 branches) */
 double orc_step(void *h, double dt, uint32_t *err_out) {
   orc_t *o = (orc_t *)h;
   const int ndim = o->c.ndim, nvar = o->nvar;
@@ -1157,25 +1181,20 @@ double orc_step(void *h, double dt, uint32_t *err_out) {
   }
   ConsToPrim3D(o);
 
-  /* stage 2 */
-  Boundary(o);
-  UpdateStage(o, dt, 2);
-  for (nv = 0; nv < nvar; nv++)
-    for (k = o->beg[2]; k <= o->end[2]; k++)
-    for (j = o->beg[1]; j <= o->end[1]; j++)
-    for (i = o->beg[0]; i <= o->end[0]; i++) {
-      double *u = VC(o, o->Uc, nv, i, j, k);
-      *u = 0.5*(*VC(o, o->U0, nv, i, j, k)) + 0.5*(*u) + 0.5*(*VC(o, o->Rc, nv, i, j, k));
-    }
-  if (isMHD) {
-    for (k = o->beg[2]; k <= o->end[2] + (ndim == 3); k++)
-    for (j = o->beg[1]; j <= o->end[1] + 1; j++)
-    for (i = o->beg[0]; i <= o->end[0] + 1; i++)
-      for (d = 0; d < ndim; d++) {
-        long s = SI(o, d, i, j, k);
-        o->Vs[d][s] = 0.5*o->Bs0[d][s] + 0.5*o->Vs[d][s] + 0.5*o->Rs[d][s];
-      }
-    AverageStaggered(o, o->beg[0], o->end[0], o->beg[1], o->end[1], o->beg[2], o->end[2], 0);
+  /* stage 2 (RK2: 1/2, 1/2, 1/2; RK3: 3/4, 1/4, 1/4) and RK3's stage 3
+     (1/3, 2/3, 2/3): Src/rk_step.cpp:30-61, 509-552, 681-727 */
+  if (o->c.rk == 3) {
+    Boundary(o);
+    UpdateStage(o, dt, 2);
+    Combine(o, 0.75, 0.25, 0.25);
+    ConsToPrim3D(o);
+    Boundary(o);
+    UpdateStage(o, dt, 3);
+    Combine(o, (1.0/3.0), (2.0/3.0), (2.0/3.0));
+  } else {
+    Boundary(o);
+    UpdateStage(o, dt, 2);
+    Combine(o, 0.5, 0.5, 0.5);
   }
   ConsToPrim3D(o);
   if (err_out) *err_out = o->err;

@@ -22,6 +22,7 @@ typedef struct {
   int outflow;   /* bit 2d / 2d+1: low / high side of direction d is OUTFLOW */
   int reflect;   /* same bits: REFLECTIVE (or AXISYMMETRIC, identical in Cartesian) */
   int eqtsym;    /* same bits: EQTSYMMETRIC */
+  int rk;        /* TIME_STEPPING: 2 (RK2, also for 0) or 3 (RK3) */
 } orc_cfg;
 
 void    *orc_create(const orc_cfg *cfg);

@@ -27,7 +27,7 @@ class OrcCfg(ctypes.Structure):
                 ("gamma", ctypes.c_double), ("dx", ctypes.c_double * 3),
                 ("cfl", ctypes.c_double), ("cfl_max_var", ctypes.c_double),
                 ("outflow", ctypes.c_int), ("reflect", ctypes.c_int),
-                ("eqtsym", ctypes.c_int)]
+                ("eqtsym", ctypes.c_int), ("rk", ctypes.c_int)]
 
 
 def build() -> str:
@@ -91,7 +91,7 @@ class Oracle:
     """One grid advanced by the CPU restatement."""
 
     def __init__(self, state, limiter="mc", solver="hlld", ct="uct_hlld",
-                 cfl=0.4, cfl_max_var=1.1, outflow=0, reflect=0, eqtsym=0):
+                 cfl=0.4, cfl_max_var=1.1, outflow=0, reflect=0, eqtsym=0, rk=2):
         nx, ny, nz = state.shape
         c = OrcCfg()
         c.physics, c.ndim = state.physics, state.ndim
@@ -102,6 +102,7 @@ class Oracle:
             c.dx[d] = (state.xend[d] - state.xbeg[d]) / state.shape[d]
         c.cfl, c.cfl_max_var = cfl, cfl_max_var
         c.outflow, c.reflect, c.eqtsym = outflow, reflect, eqtsym
+        c.rk = rk
         self.cfg = c
         self.shape = (nx, ny, nz)
         self.physics, self.ndim, self.nvar = state.physics, state.ndim, state.nvar

@@ -148,6 +148,26 @@ CASES = {
                                        dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
                                             ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
                                             bc=("reflective", "periodic", "periodic")), 6),
+    # RK3 time stepping (TIME_STEPPING RK3)
+    "mhd2d_mc_hlld_ucthlld_rk3": (ics.mhd2d_turbulence, dict(n=(28, 24), seed=91),
+                                  dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",
+                                       ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4, rk="RK3"), 12),
+    "mhd3d_mc_hlld_ucthlld_rk3": (ics.mhd3d_turbulence, dict(n=(12, 10, 8), seed=92),
+                                  dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                       ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4, rk="RK3"), 8),
+    "mhd2d_ppm_hlld_ucthlld_outflow_rk3": (
+        ics.mhd2d_turbulence, dict(n=(24, 22), seed=93),
+        dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld", ct_emf="UCT_HLLD", cfl=0.4,
+             first_dt=1e-4, reconstruction="PARABOLIC", rk="RK3",
+             bc=("outflow", "outflow", "periodic")), 10),
+    "hd2d_ppm_hllc_reflect_rk3": (ics.hd_turbulence, dict(n=(26, 20), seed=94),
+                                  dict(physics="HD", ndim=2, limiter="MC_LIM", solver="hllc",
+                                       cfl=0.4, first_dt=1e-4, reconstruction="PARABOLIC",
+                                       rk="RK3", bc=("reflective", "periodic", "periodic")), 12),
+    "rmhd3d_mc_hlld_ucthll_rk3": (ics.rmhd3d_turbulence, dict(n=(10, 8, 8), seed=95,
+                                                              lorentz_max=5.0),
+                                  dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                       ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4, rk="RK3"), 6),
 }
 
 
@@ -202,8 +222,9 @@ def make_io(name: str) -> str:
 
 def ref_cfg_name(rc: dict) -> str:
     lim = "ppm" if rc.get("reconstruction") == "PARABOLIC" else rc["limiter"]
+    rk = "_rk3" if rc.get("rk") == "RK3" else ""
     return "{physics}{ndim}d_{lim}_{solver}_{ct}".format(
-        ct=rc.get("ct_emf", "none"), lim=lim, **rc).lower()
+        ct=rc.get("ct_emf", "none"), lim=lim, **rc).lower() + rk
 
 
 def _as2d(st):
@@ -251,7 +272,7 @@ def make(name: str) -> str:
         cfl=rc["cfl"], cfl_max_var=1.1, first_dt=rc["first_dt"],
         reconstruction=rc.get("reconstruction", "LINEAR"), outflow=outflow_mask(rc),
         reflect=side_mask(rc, ("reflective", "axisymmetric")),
-        eqtsym=side_mask(rc, ("eqtsymmetric",)))
+        eqtsym=side_mask(rc, ("eqtsymmetric",)), rk=3 if rc.get("rk") == "RK3" else 2)
     return out
 
 

@@ -45,5 +45,6 @@ class Golden:
         self.eqtsym = int(z["eqtsym"]) if "eqtsym" in z else 0
         # side types as keyword arguments of the oracle and of api.Solver
         self.bc = dict(outflow=self.outflow, reflect=self.reflect, eqtsym=self.eqtsym)
+        self.rk = int(z["rk"]) if "rk" in z else 2
         if self.reconstruction == "PARABOLIC":
             self.limiter = "ppm"

@@ -16,7 +16,7 @@ import oracle as orc
 def test_oracle_matches_reference_bitwise(name):
     g = gu.Golden(name)
     o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct,
-                   cfl=g.cfl, cfl_max_var=g.cfl_max_var, **g.bc)
+                   cfl=g.cfl, cfl_max_var=g.cfl_max_var, **g.bc, rk=g.rk)
     hist, err = o.run(g.nsteps, g.first_dt)
     V, U, Bs = o.state()
     assert err & (1 << 15) == 0, f"oracle raised ERR_QUIT ({err:#x})"
@@ -29,7 +29,7 @@ def test_oracle_matches_reference_bitwise(name):
 
 def test_oracle_divb_roundoff():
     g = gu.Golden("mhd3d_mc_hlld_ucthlld")
-    o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct, **g.bc)
+    o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct, **g.bc, rk=g.rk)
     o.run(g.nsteps, g.first_dt)
     _, _, Bs = o.state()
     nx, ny, nz = g.shape
@@ -41,7 +41,7 @@ def test_oracle_divb_roundoff():
 
 def _run_state(g):
     o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct, cfl=g.cfl,
-                   **g.bc)
+                   **g.bc, rk=g.rk)
     o.run(g.nsteps, g.first_dt)
     return o.state()[1]
 
