@@ -129,6 +129,7 @@ class Scheme:
     cfl_max_var: float = 1.1
     small_rho: float = 1e-12
     small_prs: float = 1e-12
+    rk: int = 2                # TIME_STEPPING: 2 (RK2) or 3 (RK3)
 
     def to_c(self) -> GpScheme:
         s = GpScheme()
@@ -137,7 +138,7 @@ class Scheme:
         s.reconstruction = 1 if self.limiter == "ppm" else 0
         s.riemann = SOLVERS[self.riemann]
         s.ct_emf = CT_AVG[self.ct_emf]
-        s.rk_stages = 2
+        s.rk_stages = self.rk
         s.precision = self.precision
         s.gamma, s.cfl, s.cfl_max_var = self.gamma, self.cfl, self.cfl_max_var
         s.small_rho, s.small_prs = self.small_rho, self.small_prs
@@ -269,7 +270,7 @@ class Solver:
         nk = ctypes.c_int(0)
         d = ctypes.c_double(dt)
         _check(lib().gp_profile_steps(self._h, nsteps, ctypes.byref(d), buf, 64, ctypes.byref(nk)))
-        per = nk.value // 2
+        per = nk.value // self.scheme.rk
         res = [(lib().gp_kernel_name(self._h, q).decode(), 1 + q // per, float(buf[q]))
                for q in range(nk.value)]
         return res, d.value

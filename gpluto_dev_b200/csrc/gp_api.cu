@@ -458,22 +458,56 @@ int enqueue_step(gp_handle* h, double* hist, int slot, cudaEvent_t* ev = nullptr
     d.Bsout[q] = mhd ? h->Bs[b1][q] : nullptr;
   }
   if (launch(d) != 0) return fail(GP_ERR_UNSUPPORTED, "scheme not compiled");
-  // stage 2: (U^n, U1, B^n, B1) -> (U^{n+1} in place of U^n, B^{n+1})
-  if (h->padded) fill_boundaries(h, h->Bs[b1]);
-  d.stage = 2;
-  d.Uc = h->U[1];
-  d.Uout = h->U[0];
-  for (int q = 0; q < 3; q++) {
-    d.Bs[q] = mhd ? h->Bs[b1][q] : nullptr;
-    d.Bs0[q] = mhd ? h->Bs[b0][q] : nullptr;
-    d.Bsout[q] = mhd ? h->Bs[b2][q] : nullptr;
+  if (h->scheme.rk_stages == 3) {
+    // RK3 stage 2: (U^n, U1, B^n, B1) -> (U2 in place of U1, B2); stage 3:
+    // (U^n, U2, B^n, B2) -> (U^{n+1} in place of U^n, B^{n+1} in B1's buffer).
+    // The finish reads only its own cell's U and its neighbours' input faces,
+    // so cells update in place and faces rotate (Src/rk_step.cpp:30-61)
+    if (h->padded) fill_boundaries(h, h->Bs[b1]);
+    d.stage = 2;
+    d.w0 = 0.75;
+    d.w1 = 0.25;
+    d.wr = 0.25;
+    d.Uc = h->U[1];
+    d.Uout = h->U[1];
+    for (int q = 0; q < 3; q++) {
+      d.Bs[q] = mhd ? h->Bs[b1][q] : nullptr;
+      d.Bs0[q] = mhd ? h->Bs[b0][q] : nullptr;
+      d.Bsout[q] = mhd ? h->Bs[b2][q] : nullptr;
+    }
+    if (launch(d) != 0) return fail(GP_ERR_UNSUPPORTED, "scheme not compiled");
+    if (h->padded) fill_boundaries(h, h->Bs[b2]);
+    d.stage = 3;
+    d.w0 = 1.0 / 3.0;
+    d.w1 = 2.0 / 3.0;
+    d.wr = 2.0 / 3.0;
+    d.Uc = h->U[1];
+    d.Uout = h->U[0];
+    for (int q = 0; q < 3; q++) {
+      d.Bs[q] = mhd ? h->Bs[b2][q] : nullptr;
+      d.Bs0[q] = mhd ? h->Bs[b0][q] : nullptr;
+      d.Bsout[q] = mhd ? h->Bs[b1][q] : nullptr;
+    }
+    if (launch(d) != 0) return fail(GP_ERR_UNSUPPORTED, "scheme not compiled");
+  } else {
+    // stage 2: (U^n, U1, B^n, B1) -> (U^{n+1} in place of U^n, B^{n+1})
+    if (h->padded) fill_boundaries(h, h->Bs[b1]);
+    d.stage = 2;
+    d.w0 = d.w1 = d.wr = 0.5;
+    d.Uc = h->U[1];
+    d.Uout = h->U[0];
+    for (int q = 0; q < 3; q++) {
+      d.Bs[q] = mhd ? h->Bs[b1][q] : nullptr;
+      d.Bs0[q] = mhd ? h->Bs[b0][q] : nullptr;
+      d.Bsout[q] = mhd ? h->Bs[b2][q] : nullptr;
+    }
+    if (launch(d) != 0) return fail(GP_ERR_UNSUPPORTED, "scheme not compiled");
   }
-  if (launch(d) != 0) return fail(GP_ERR_UNSUPPORTED, "scheme not compiled");
   dt_update_kernel<<<1, 1, 0, h->stream>>>(h->sc, (double)h->ndim, h->scheme.cfl,
                                           h->scheme.cfl_max_var, h->dx[0], h->dx[1], h->dx[2],
                                           hist, slot);
   CUDA_TRY(cudaGetLastError());
-  h->bcur = b2;
+  h->bcur = h->scheme.rk_stages == 3 ? b1 : b2;
   return GP_OK;
 }
 
@@ -521,7 +555,8 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   if (scheme->physics == GP_RMHD && (scheme->riemann == GP_RS_HLLC || scheme->ct_emf != GP_CT_UCT_HLL))
     return fail(GP_ERR_UNSUPPORTED, "RMHD is built with HLLD/HLL and UCT_HLL "
                 "(the reference RMHD HLLD stores no UCT_HLLD data, Src/RMHD/hlld.cpp:526-537)");
-  if (scheme->rk_stages != 2) return fail(GP_ERR_UNSUPPORTED, "only RK2 is built");
+  if (scheme->rk_stages != 2 && scheme->rk_stages != 3)
+    return fail(GP_ERR_UNSUPPORTED, "TIME_STEPPING RK2 and RK3 are built");
   if (scheme->precision != GP_FP64 && scheme->precision != GP_MIXED)
     return fail(GP_ERR_INVALID, "bad precision");
   for (int d = 0; d < 3; d++) {
@@ -670,7 +705,7 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
     int fills = 0;
     for (int side = 0; side < 2 * h->ndim; side++)
       if (h->padded && ((nonper >> side) & 1u)) fills += scheme->physics == GP_HD ? 1 : 2;
-    h->launches_per_step = 2 * (gp::stage_launch_count(h->key) + fills) + 1;
+    h->launches_per_step = scheme->rk_stages * (gp::stage_launch_count(h->key) + fills) + 1;
   }
   if (h->padded) {  // padding cells start finite
     cudaMemsetAsync(h->V, 0, cell * h->nvar, h->stream);
@@ -905,7 +940,7 @@ int gp_launches_per_step(const gp_handle* h) { return h ? h->launches_per_step :
 int gp_profile_steps(gp_handle* h, int nsteps, double* dt, float* kernel_ms, int cap,
                      int* nkernels) {
   if (!h || !dt || !kernel_ms || !nkernels) return fail(GP_ERR_INVALID, "null argument");
-  const int nk = 2 * gp::stage_launch_count(h->key);
+  const int nk = h->scheme.rk_stages * gp::stage_launch_count(h->key);
   *nkernels = nk;
   if (cap < nk) return fail(GP_ERR_INVALID, "kernel_ms needs %d entries", nk);
   for (int q = 0; q < nk; q++) kernel_ms[q] = 0.f;

@@ -566,6 +566,7 @@ int gp_batch_add(gp_batch* b, const gp_grid_desc* grid, const gp_scheme* scheme,
       a.small_rho = scheme->small_rho;
       a.small_prs = scheme->small_prs;
       a.stage = stage;
+      a.w0 = a.w1 = a.wr = 0.5;  // RK2 combine of stage 2 (Src/rk_step.cpp:30-35)
       a.invdt_bits = &sc->invdt_bits;
       a.err = &sc->err;
     }

@@ -68,7 +68,9 @@ struct StageArgs {
   const double* dtdx;     // dt/dx_d (3 values in device memory, set per step)
   double dx[3];
   double gamma, small_rho, small_prs;
-  int stage;              // 1 or 2 (RK2)
+  int stage;              // 1, 2 (RK2, RK3) or 3 (RK3)
+  double w0, w1, wr;      // combine weights of stages >= 2: U = w0 U^n + w1 U_c + wr R
+                          // (Src/rk_step.cpp:30-61)
   unsigned long long* invdt_bits;  // max over cells of Cdt (stage 1)
   uint32_t* err;          // OR of error bits
 };
@@ -1076,7 +1078,7 @@ __device__ __forceinline__ double face_new(const StageArgs<CTT>& a, int d, long 
                                            double rs) {
   double bc = a.Bs[d][f];
   if (a.stage == 1) return bc + rs;
-  return 0.5 * a.Bs0[d][f] + 0.5 * bc + 0.5 * rs;
+  return a.w0 * a.Bs0[d][f] + a.w1 * bc + a.wr * rs;
 }
 
 // Stage finish of cell c; returns its inverse-dt sum (0 outside the grid).
@@ -1096,7 +1098,7 @@ __device__ __forceinline__ double finish_cell(const StageArgs<CTT>& a, const Gri
       if (NDIM == 3) Rc = Rc + (double)a.dU[(2 * NV + nv) * n + c];
       const double u0 = a.U0[nv * n + c];
       if (a.stage == 1) u[nv] = u0 + Rc;
-      else u[nv] = 0.5 * u0 + 0.5 * a.Uc[nv * n + c] + 0.5 * Rc;
+      else u[nv] = a.w0 * u0 + a.w1 * a.Uc[nv * n + c] + a.wr * Rc;
     }
     cdt = (double)a.Cdt[c] + (double)a.Cdt[n + c];
     if (NDIM == 3) cdt = cdt + (double)a.Cdt[2 * n + c];

@@ -48,6 +48,9 @@ static StageArgs<CTT> make_args(const StageDesc& d) {
   a.small_rho = d.small_rho;
   a.small_prs = d.small_prs;
   a.stage = d.stage;
+  a.w0 = d.w0;
+  a.w1 = d.w1;
+  a.wr = d.wr;
   a.invdt_bits = d.invdt_bits;
   a.err = d.err;
   return a;

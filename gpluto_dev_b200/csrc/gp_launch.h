@@ -24,6 +24,7 @@ struct StageDesc {
   double dx[3];
   double gamma, small_rho, small_prs;
   int stage;
+  double w0, w1, wr;   // combine weights of stages >= 2
   unsigned long long* invdt_bits;
   uint32_t* err;
 };

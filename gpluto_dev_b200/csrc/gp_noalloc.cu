@@ -176,6 +176,7 @@ extern "C" int gp_advance_step_noalloc(const gp_grid_desc* grid, const gp_scheme
   if (launch(d) != 0) return GP_ERR_UNSUPPORTED;
   // stage 2: (U, U1, B, B1) -> (U in place, B2), then B2 -> caller's B
   d.stage = 2;
+  d.w0 = d.w1 = d.wr = 0.5;  // RK2 (Src/rk_step.cpp:30-35)
   d.Uc = U1;
   d.Uout = Uc;
   for (int q = 0; q < 3; q++) {

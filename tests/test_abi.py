@@ -51,7 +51,7 @@ def test_create_rejects_bad_configs_before_touching_the_device():
     g.ndim = 2
     g.nint[0] = g.nint[1] = 16
     g.nint[2] = 1
-    s.rk_stages = 3
+    s.rk_stages = 4                       # RK4 is not built
     assert L.gp_create(ctypes.byref(g), ctypes.byref(s), None, ctypes.byref(h)) == -2
 
 

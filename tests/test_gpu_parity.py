@@ -22,16 +22,17 @@ def rel_linf(a, b):
 
 
 def make_solver(st, limiter, solver, ct, cfl=0.4, cfl_max_var=1.1, precision=api.FP64,
-                outflow=0, reflect=0, eqtsym=0):
+                outflow=0, reflect=0, eqtsym=0, rk=2):
     sch = api.Scheme(physics=st.physics, limiter=limiter, riemann=solver, ct_emf=ct,
-                     precision=precision, gamma=st.gamma, cfl=cfl, cfl_max_var=cfl_max_var)
+                     precision=precision, gamma=st.gamma, cfl=cfl, cfl_max_var=cfl_max_var,
+                     rk=rk)
     return api.Solver.from_state(st, sch, outflow=outflow, reflect=reflect, eqtsym=eqtsym)
 
 
 @pytest.mark.parametrize("name", [n for n in gu.names() if not n.startswith("rmhd")])
 def test_gpu_matches_reference_fixture_bitwise(name):
     g = gu.Golden(name)
-    s = make_solver(g.ic, g.limiter, g.solver, g.ct, g.cfl, g.cfl_max_var, **g.bc)
+    s = make_solver(g.ic, g.limiter, g.solver, g.ct, g.cfl, g.cfl_max_var, **g.bc, rk=g.rk)
     dt_after, hist, out = s.run(g.nsteps, g.first_dt)
     V, U, Bs = s.download()
     assert out.err_bits & api.ERR_QUIT == 0
@@ -170,6 +171,37 @@ def test_gpu_mirrored_sides_match_oracle_bitwise(case):
     ohist, oerr = o.run(nsteps, 1e-4)
     Vo, Uo, Bo = o.state()
     s = make_solver(st, lim, rs, ct, **bc)
+    dt_after, hist, out = s.run(nsteps, 1e-4)
+    V, U, Bs = s.download()
+    assert out.err_bits == oerr
+    np.testing.assert_array_equal(hist, ohist[:-1])
+    np.testing.assert_array_equal(V, Vo)
+    np.testing.assert_array_equal(U, Uo)
+    for a, b in zip(Bs, Bo):
+        np.testing.assert_array_equal(a, b)
+
+
+RK3_CASES = [
+    # (generator, kwargs, limiter, solver, ct, side masks, nsteps): TIME_STEPPING RK3
+    (ics.mhd3d_blast, dict(n=(17, 15, 13), seed=96, radius=0.2), "mc", "hlld", "uct_hlld",
+     dict(), 6),
+    (ics.mhd2d_turbulence, dict(n=(29, 23), seed=97), "ppm", "hlld", "uct_hlld",
+     dict(reflect=0b0011, outflow=0b1100), 8),
+    (ics.hd_turbulence, dict(n=(19, 13, 11), seed=98), "vl", "hllc", "uct_hll", dict(), 8),
+]
+
+
+@pytest.mark.parametrize("case", range(len(RK3_CASES)))
+def test_gpu_rk3_matches_oracle_bitwise(case):
+    gen, kw, lim, rs, ct, bc, nsteps = RK3_CASES[case]
+    st = gen(**kw)
+    kwo = dict(limiter=lim, solver=rs, rk=3, **bc)
+    if st.physics != ics.PHYS_HD:
+        kwo["ct"] = ct
+    o = orc.Oracle(st, **kwo)
+    ohist, oerr = o.run(nsteps, 1e-4)
+    Vo, Uo, Bo = o.state()
+    s = make_solver(st, lim, rs, ct, rk=3, **bc)
     dt_after, hist, out = s.run(nsteps, 1e-4)
     V, U, Bs = s.download()
     assert out.err_bits == oerr

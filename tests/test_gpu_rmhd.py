@@ -22,9 +22,9 @@ def rel_linf(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-def solver(st, lim, rs, cfl=0.3, precision=api.FP64, outflow=0, reflect=0, eqtsym=0):
+def solver(st, lim, rs, cfl=0.3, precision=api.FP64, outflow=0, reflect=0, eqtsym=0, rk=2):
     sch = api.Scheme(physics=api.RMHD, limiter=lim, riemann=rs, ct_emf="uct_hll",
-                     precision=precision, gamma=st.gamma, cfl=cfl)
+                     precision=precision, gamma=st.gamma, cfl=cfl, rk=rk)
     return api.Solver.from_state(st, sch, outflow=outflow, reflect=reflect, eqtsym=eqtsym)
 
 
@@ -58,7 +58,7 @@ def test_rmhd_fp64_matches_reference_fixture(name):
         for nudge in (1, -1):
             orc.set_ulp_nudge(nudge)
             o = orc.Oracle(g.ic, limiter=g.limiter, solver=g.solver, ct=g.ct, cfl=g.cfl,
-                           **g.bc)
+                           **g.bc, rk=g.rk)
             o.run(g.nsteps, g.first_dt)
             spread.append(deviation(o.state()[1], g.U))
     finally:
@@ -67,7 +67,7 @@ def test_rmhd_fp64_matches_reference_fixture(name):
     frac_ref = min(x[1] for x in spread)
     linf_ref = max(x[2] for x in spread)
 
-    s = solver(g.ic, g.limiter, g.solver, g.cfl, **g.bc)
+    s = solver(g.ic, g.limiter, g.solver, g.cfl, **g.bc, rk=g.rk)
     _, hist, out = s.run(g.nsteps, g.first_dt)
     V, U, Bs = s.download()
     assert out.err_bits & api.ERR_QUIT == 0
