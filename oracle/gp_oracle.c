@@ -24,8 +24,8 @@
 
 #include "gp_oracle.h"
 
-#define MAX(a,b)  ( (a) >= (b) ? (a) : (b) )      /* Src/macros.hpp:188 */
-#define MIN(a,b)  ( (a) <= (b) ? (a) : (b) )      /* Src/macros.hpp:191 */
+#define MAX(a,b)  ( (a) >= (b) ? (a) : (b) )      /* Src/macros.hpp:191 */
+#define MIN(a,b)  ( (a) <= (b) ? (a) : (b) )      /* Src/macros.hpp:194 */
 #define ABS_MIN(a,b)  (fabs(a) < fabs(b) ? (a):(b))   /* Src/macros.hpp:14 */
 #define MINMOD_LIMITER(a,b)  ((a)*(b) > 0.0 ? (fabs(a) < fabs(b) ? (a):(b)):0.0)
 
@@ -629,6 +629,42 @@ static void PPM_Cell(const double *v, long st, double *dvp_out, double *dvm_out)
   *dvm_out = dvm;
 }
 
+/* Monotonicity-preserving 5th-order edge value of Suresh & Huynh (1997),
+   Src/States/states.hpp:32-98 (MP5_ALPHA 4, cell averages): F points at the
+   cell, `st` is the stride between cells, sign +1 gives the right edge and
+   -1 the left edge. */
+static double MP5_Edge(const double *F, long st, int sign) {
+  const double alpha = 4.0, epsm = 1.e-12;
+  const double Fpp = F[2*sign*st], Fp = F[sign*st], F0 = F[0], Fm = F[-sign*st],
+               Fmm = F[-2*sign*st];
+  double dFp = Fp - F0, dFm = F0 - Fm;
+  double f = 2.0*Fmm - 13.0*Fm + 47.0*F0 + 27.0*Fp - 3.0*Fpp;   /* Eq. (2.1) */
+  f /= 60.0;
+  double fMP = F0 + Minmod(dFp, alpha*dFm);                      /* Eq. (2.12) */
+  if ((f - F0)*(f - fMP) <= epsm) return f;
+  double d2m = Fmm + F0 - 2.0*Fm;
+  double d2  = Fm + Fp - 2.0*F0;
+  double d2p = F0 + Fpp - 2.0*Fp;
+  double scrh1 = Minmod(4.0*d2 - d2p, 4.0*d2p - d2);
+  double scrh2 = Minmod(d2, d2p);
+  double dMMp = Minmod(scrh1, scrh2);                             /* Eq. (2.27) */
+  scrh1 = Minmod(4.0*d2m - d2, 4.0*d2 - d2m);
+  scrh2 = Minmod(d2, d2m);
+  double dMMm = Minmod(scrh1, scrh2);
+  double fUL = F0 + alpha*dFm;                                   /* Eq. (2.8) */
+  double fAV = 0.5*(F0 + Fp);                                    /* Eq. (2.16) */
+  double fMD = fAV - 0.5*dMMp;                                   /* Eq. (2.28) */
+  double fLC = 0.5*(3.0*F0 - Fm) + 4.0/3.0*dMMm;                 /* Eq. (2.29) */
+  scrh1 = MIN(F0, Fp); scrh1 = MIN(scrh1, fMD);
+  scrh2 = MIN(F0, fUL); scrh2 = MIN(scrh2, fLC);
+  double fmin = MAX(scrh1, scrh2);                               /* Eq. (2.24a) */
+  scrh1 = MAX(F0, Fp); scrh1 = MAX(scrh1, fMD);
+  scrh2 = MAX(F0, fUL); scrh2 = MAX(scrh2, fLC);
+  double fmax = MIN(scrh1, scrh2);                               /* Eq. (2.24b) */
+  f = f + Minmod(fmin - f, fmax - f);                            /* Eq. (2.26) */
+  return f;
+}
+
 /* ------------------------------------------------------------------ */
 /* boundary: Src/boundary.cpp:67-322 + PeriodicBoundary 502-675         */
 /* ------------------------------------------------------------------ */
@@ -837,6 +873,11 @@ static void Sweep(orc_t *o, int dir, double dt) {
        Src/States/ppm_states.cpp:110-164 */
     for (nv = 0; nv < nvar; nv++)
       for (i = ib-1; i <= ie+1; i++) {
+        if (o->c.limiter == ORC_LIM_MP5) {   /* Src/States/mp5_states.cpp:125-172 */
+          vL[(i+1)*nvar + nv] = MP5_Edge(v + i*nvar + nv, nvar, +1);
+          vR[i*nvar + nv]     = MP5_Edge(v + i*nvar + nv, nvar, -1);
+          continue;
+        }
         if (o->c.limiter == ORC_LIM_PPM) {
           double dvp, dvm;
           PPM_Cell(v + i*nvar + nv, nvar, &dvp, &dvm);
@@ -850,6 +891,23 @@ static void Sweep(orc_t *o, int dir, double dt) {
         vL[(i+1)*nvar + nv] = v[i*nvar + nv] + 0.5*dv;
         vR[i*nvar + nv]     = v[i*nvar + nv] - 0.5*dv;
       }
+    /* MP5: density and pressure edges that came out negative fall back to
+       minmod PLM (Src/States/mp5_states.cpp:184-213, uniform grid) */
+    if (o->c.limiter == ORC_LIM_MP5) {
+      const int qv[2] = {RHO, nvar - 1};
+      int q;
+      for (i = ib-1; i <= ie+1; i++)
+        for (q = 0; q < 2; q++) {
+          nv = qv[q];
+          if (vL[(i+1)*nvar + nv] < 0.0 || vR[i*nvar + nv] < 0.0) {
+            double dvp = (v[(i+1)*nvar + nv] - v[i*nvar + nv])*1.0;
+            double dvm = (v[i*nvar + nv] - v[(i-1)*nvar + nv])*1.0;
+            double dv = Minmod(dvp, dvm);
+            vL[(i+1)*nvar + nv] = v[i*nvar + nv] + 0.5*dv;
+            vR[i*nvar + nv]     = v[i*nvar + nv] - 0.5*dv;
+          }
+        }
+    }
     /* relativistic velocity limiter, Src/vel_limiter.hpp:13-34 (applied in
        the adjustment loop before the CT overwrite, plm_states.cpp:166) */
     if (o->c.physics == ORC_RMHD) {
@@ -914,6 +972,14 @@ static void ArrayRec(orc_t *o, int dir, int t1, int t2, int stag, const double *
     TrueIdx(dir, i, t1, t2, &ti, &tj, &tk);
     q[i] = (stag >= 0) ? o->Vs[stag][SI(o, stag, ti, tj, tk)] : Qe[EI(o, ti, tj, tk)];
   }
+  if (lim == ORC_LIM_MP5) {
+    /* MP5 branch, Src/array_reconstruct.cpp:327-384 */
+    for (i = 2; i < nd-2; i++) {
+      qL[i+1] = MP5_Edge(q + i, 1, +1);
+      qR[i]   = MP5_Edge(q + i, 1, -1);
+    }
+    return;
+  }
   if (lim == ORC_LIM_PPM) {
     /* PARABOLIC branch, Src/array_reconstruct.cpp:208-270 (uniform grid) */
     for (i = 1; i < nd-1; i++) {
@@ -950,7 +1016,9 @@ static void ComputeEMF(orc_t *o) {
   const int ndim = o->c.ndim;
   /* Src/MHD/CT/ct_emf_average.cpp:553-559: MC for B and the scheme limiter
      for velocities with linear reconstruction; parabolic for both with PPM */
-  int recV = o->c.limiter, recB = (o->c.limiter == ORC_LIM_PPM ? ORC_LIM_PPM : ORC_LIM_MC);
+  int recV = o->c.limiter,
+      recB = (o->c.limiter == ORC_LIM_PPM || o->c.limiter == ORC_LIM_MP5) ? o->c.limiter
+                                                                         : ORC_LIM_MC;
   int ib = o->beg[0], ie = o->end[0] + 1;
   int jb = o->beg[1], je = o->end[1] + 1;
   int kb = o->beg[2], ke = o->end[2] + (ndim == 3);
@@ -1290,7 +1358,8 @@ void *orc_create(const orc_cfg *cfg) {
   int d, e;
   o->c = *cfg;
   o->nvar = (cfg->physics == ORC_HD) ? 5 : 8;
-  o->ng = (cfg->limiter == ORC_LIM_PPM) ? 3 : 2;   /* Src/get_nghost.cpp:33-44 */
+  o->ng = (cfg->limiter == ORC_LIM_PPM || cfg->limiter == ORC_LIM_MP5) ? 3 : 2;
+  /* Src/get_nghost.cpp:33-44 */
   o->ncell = 1;
   for (d = 0; d < 3; d++) {
     if (d < cfg->ndim) { o->nt[d] = cfg->n[d] + 2*o->ng; o->beg[d] = o->ng; }

@@ -144,8 +144,9 @@ class RefConfig:
     def makefile(self) -> str:
         src = os.path.join(REF_ROOT, "Src")
         phys_obj, phys_dirs = _PHYS[self.physics]
-        step = [("ppm_states" if (o == "plm_states" and self.reconstruction == "PARABOLIC")
-                 else o) for o in _STEP_OBJ]
+        states = {"PARABOLIC": "ppm_states", "MP5": "mp5_states"}.get(self.reconstruction,
+                                                                    "plm_states")
+        step = [(states if o == "plm_states" else o) for o in _STEP_OBJ]
         objs = _DEFAULT_OBJ + _MATH_OBJ + step + phys_obj
         vdirs = [src, f"{src}/States", f"{src}/Math_Tools"] + [f"{src}/{d}" for d in phys_dirs]
         incs = ["-I.", f"-I{src}"] + [f"-I{src}/{d}" for d in phys_dirs] + [f"-I{src}/States", f"-I{src}/Math_Tools"]

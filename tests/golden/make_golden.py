@@ -168,6 +168,27 @@ CASES = {
                                                               lorentz_max=5.0),
                                   dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
                                        ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4, rk="RK3"), 6),
+    # MP5 reconstruction (RECONSTRUCTION MP5, 3 ghost cells)
+    "mhd2d_mp5_hlld_ucthlld": (ics.mhd2d_turbulence, dict(n=(26, 22), seed=101),
+                               dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",
+                                    ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4,
+                                    reconstruction="MP5"), 12),
+    "mhd3d_mp5_hlld_ucthlld_rk3": (ics.mhd3d_turbulence, dict(n=(12, 10, 9), seed=102),
+                                   dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                        ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4,
+                                        reconstruction="MP5", rk="RK3"), 6),
+    "mhd3d_blast_mp5_hll_ucthll_reflect": (
+        ics.mhd3d_blast, dict(n=(14, 12, 10), seed=103, radius=0.25),
+        dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="hll", ct_emf="UCT_HLL", cfl=0.4,
+             first_dt=1e-4, reconstruction="MP5", bc=("reflective", "outflow", "periodic")), 6),
+    "hd2d_mp5_hllc": (ics.hd_turbulence, dict(n=(24, 20), seed=104),
+                      dict(physics="HD", ndim=2, limiter="MC_LIM", solver="hllc", cfl=0.4,
+                           first_dt=1e-4, reconstruction="MP5"), 12),
+    "rmhd3d_mp5_hlld_ucthll": (ics.rmhd3d_turbulence, dict(n=(10, 8, 8), seed=105,
+                                                           lorentz_max=5.0),
+                               dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                    ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
+                                    reconstruction="MP5"), 6),
 }
 
 
@@ -221,7 +242,7 @@ def make_io(name: str) -> str:
 
 
 def ref_cfg_name(rc: dict) -> str:
-    lim = "ppm" if rc.get("reconstruction") == "PARABOLIC" else rc["limiter"]
+    lim = {"PARABOLIC": "ppm", "MP5": "mp5"}.get(rc.get("reconstruction"), rc["limiter"])
     rk = "_rk3" if rc.get("rk") == "RK3" else ""
     return "{physics}{ndim}d_{lim}_{solver}_{ct}".format(
         ct=rc.get("ct_emf", "none"), lim=lim, **rc).lower() + rk

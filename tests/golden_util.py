@@ -48,3 +48,5 @@ class Golden:
         self.rk = int(z["rk"]) if "rk" in z else 2
         if self.reconstruction == "PARABOLIC":
             self.limiter = "ppm"
+        elif self.reconstruction == "MP5":
+            self.limiter = "mp5"
