@@ -26,8 +26,10 @@ LIB_PATH = os.environ.get("GPLUTO_B200_LIB") or os.path.join(_HERE, "_build",
 GP_OK, GP_ERR_INVALID, GP_ERR_QUIT, GP_ERR_NO_DEVICE, GP_ERR_IO = 0, -1, -5, -6, -7
 BC_PERIODIC, BC_OUTFLOW, BC_REFLECTIVE, BC_AXISYMMETRIC, BC_EQTSYMMETRIC = 0, 1, 2, 3, 4
 HD, MHD, RMHD = 0, 1, 2
-# "ppm" selects RECONSTRUCTION PARABOLIC (the limiter then plays no part)
-LIMITERS = {"flat": 0, "minmod": 1, "vl": 2, "vanleer": 2, "mc": 3, "ppm": 3}
+# "ppm" and "mp5" select RECONSTRUCTION PARABOLIC and MP5 (the limiter then
+# plays no part)
+LIMITERS = {"flat": 0, "minmod": 1, "vl": 2, "vanleer": 2, "mc": 3, "ppm": 3, "mp5": 3}
+RECONSTRUCTION = {"ppm": 1, "mp5": 2}
 SOLVERS = {"hll": 0, "hllc": 1, "hlld": 2}
 CT_AVG = {"uct_hll": 0, "uct_hlld": 1}
 FP64, MIXED = 0, 1
@@ -135,7 +137,7 @@ class Scheme:
         s = GpScheme()
         s.physics = self.physics
         s.limiter = LIMITERS[self.limiter]
-        s.reconstruction = 1 if self.limiter == "ppm" else 0
+        s.reconstruction = RECONSTRUCTION.get(self.limiter, 0)
         s.riemann = SOLVERS[self.riemann]
         s.ct_emf = CT_AVG[self.ct_emf]
         s.rk_stages = self.rk

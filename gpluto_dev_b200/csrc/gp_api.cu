@@ -579,15 +579,16 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
     return fail(GP_ERR_UNSUPPORTED, "MHD HLLC not built");
   if (scheme->physics == GP_HD && scheme->riemann == GP_RS_HLLD)
     return fail(GP_ERR_UNSUPPORTED, "HD has no HLLD solver");
-  if (scheme->reconstruction != GP_REC_LINEAR && scheme->reconstruction != GP_REC_PARABOLIC)
+  if (scheme->reconstruction != GP_REC_LINEAR && scheme->reconstruction != GP_REC_PARABOLIC &&
+      scheme->reconstruction != GP_REC_MP5)
     return fail(GP_ERR_UNSUPPORTED, "reconstruction %d not built", scheme->reconstruction);
   if (scheme->reconstruction == GP_REC_LINEAR &&
       (scheme->limiter < GP_LIM_MINMOD || scheme->limiter > GP_LIM_MC))
     return fail(GP_ERR_UNSUPPORTED, "limiter %d not built", scheme->limiter);
-  if (scheme->reconstruction == GP_REC_PARABOLIC)
+  if (scheme->reconstruction != GP_REC_LINEAR)
     for (int d = 0; d < grid->ndim; d++)
       if (grid->nint[d] < 4)
-        return fail(GP_ERR_INVALID, "PPM needs at least 4 cells along each direction");
+        return fail(GP_ERR_INVALID, "PPM and MP5 need at least 4 cells along each direction");
   int rc = check_device();
   if (rc) return rc;
   gp_handle* h = new (std::nothrow) gp_handle;
@@ -618,7 +619,8 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   const unsigned nonper = h->outflow | h->reflect | h->eqtsym;
   h->padded = (h->reflect | h->eqtsym) != 0 || (h->outflow != 0 && scheme->physics != GP_HD);
   {
-    const int S = scheme->reconstruction == GP_REC_PARABOLIC ? 3 : 2;
+    // ghost depth of the scheme (Src/get_nghost.cpp:33-44)
+    const int S = scheme->reconstruction == GP_REC_LINEAR ? 2 : 3;
     const int nn[3] = {h->nx, h->ny, h->nz};
     int pp[3];
     for (int d = 0; d < 3; d++) {
@@ -657,7 +659,8 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   h->stream = (cudaStream_t)stream;
   h->mixed = scheme->precision == GP_MIXED;
   h->key = gp::SchemeKey{scheme->physics, grid->ndim, scheme->riemann, scheme->ct_emf,
-                         scheme->reconstruction == GP_REC_PARABOLIC ? 4 /* LIM_PPM */
+                         scheme->reconstruction == GP_REC_PARABOLIC ? 4   /* LIM_PPM */
+                         : scheme->reconstruction == GP_REC_MP5     ? 5   /* LIM_MP5 */
                                                                     : scheme->limiter};
   // pencil segment for the marching sweeps: enough threads to fill 148 SMs
   {

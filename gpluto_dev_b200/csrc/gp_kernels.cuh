@@ -219,7 +219,8 @@ __device__ __forceinline__ void store_ct(const StageArgs<CTT>& a, int dir, long 
 // (+ [2 buffers][4 warps][NV] for the second-next cell with PPM).
 template <int NV, int LIM = LIM_MC>
 constexpr int sweep_x_stage_doubles() {
-  return 2 * (2 * NV + 1) * SWEEP_THREADS + (LIM == LIM_PPM ? 2 * (SWEEP_THREADS / 32) * NV : 0);
+  return 2 * (2 * NV + 1) * SWEEP_THREADS +
+         ((LIM == LIM_PPM || LIM == LIM_MP5) ? 2 * (SWEEP_THREADS / 32) * NV : 0);
 }
 template <int NV>
 constexpr int sweep_m_stage_doubles() { return 2 * (NV + 1) * SWEEP_THREADS; }
@@ -386,6 +387,180 @@ __device__ __forceinline__ void sweep_x_row_ppm(const StageArgs<CTT>& a, const G
   if (err) atomicOr(a.err, err);
 }
 
+// MP5 adjustments of one cell's edges (Src/States/mp5_states.cpp:184-213):
+// density and pressure edges that came out negative fall back to minmod PLM
+// (qm, qp: the neighbours' density and pressure), then, for RMHD, the
+// relativistic velocity limiter.
+template <int PHYS, int NV, typename R>
+__device__ __forceinline__ void mp5_fallback(const R* w0, const R* qm, const R* qp, R* vR,
+                                             R* vLn) {
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const int nv = q ? NV - 1 : RHO;
+    if (vLn[nv] < R(0) || vR[nv] < R(0)) {
+      const R dv = minmod(qp[q] - w0[nv], w0[nv] - qm[q]);
+      vLn[nv] = w0[nv] + R(0.5) * dv;
+      vR[nv] = w0[nv] - R(0.5) * dv;
+    }
+  }
+  if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(w0, vR, vLn);
+}
+
+template <int PHYS, int NV, int NDIM, int RS, int CT, typename R, typename CTT>
+__device__ __forceinline__ void sweep_x_row_mp5(const StageArgs<CTT>& a, const Grid3& g, int row,
+                                                double* stg_, int tid) {
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr int SL = 2 * NV + 1;  // staged doubles per lane: V[f], V[f+1], Bs[f]
+  constexpr int NW = SWEEP_THREADS / 32;
+  double(*stg)[SL][SWEEP_THREADS] = reinterpret_cast<double(*)[SL][SWEEP_THREADS]>(stg_);
+  double(*stg2)[NW][NV] = reinterpret_cast<double(*)[NW][NV]>(stg_ + 2 * SL * SWEEP_THREADS);
+  const int lane = tid & 31, w = tid >> 5;
+  if (row >= g.ny * g.nz) return;  // warp-uniform
+  const int nx = g.nx;
+  const unsigned ob = g.outflow;
+  // faces solved: nx (periodic: face nx is face 0) or nx+1 (outflow high side)
+  const int nf = nx + (int)((ob >> 1) & 1u);
+  const long long n = g.n;
+  const long long rb = (long long)row * nx;
+  const R gamma = (R)a.gamma;
+
+  // carried: cells c0-1, c0-2; left state at face c0 (from cell c0-1); flux
+  // and signal speed of face c0-1
+  R pV1[NV], pV2[NV], pVLn[NV], pF[NV], pCm = R(0);
+  {
+    R q[5][NV];
+#pragma unroll
+    for (int m = 0; m < 5; m++) load_cell<NV>(a.V, n, rb + gidx(m - 3, nx, ob, 0), q[m]);
+    R vrp[NV];
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {   // cell nx-1 (stencil nx-3 .. nx+1)
+      pVLn[nv] = mp5_edge(q[0][nv], q[1][nv], q[2][nv], q[3][nv], q[4][nv]);
+      vrp[nv] = mp5_edge(q[4][nv], q[3][nv], q[2][nv], q[1][nv], q[0][nv]);
+      pV1[nv] = q[2][nv];
+      pV2[nv] = q[1][nv];
+      pF[nv] = R(0);
+    }
+    {
+      const R qm[2] = {q[1][RHO], q[1][NV - 1]}, qp[2] = {q[3][RHO], q[3][NV - 1]};
+      mp5_fallback<PHYS, NV>(q[2], qm, qp, vrp, pVLn);
+    }
+  }
+  R fF[NV], fCm = R(0);
+  R F[NV], cm = R(0);
+#pragma unroll
+  for (int nv = 0; nv < NV; nv++) { fF[nv] = R(0); F[nv] = R(0); }
+  uint32_t err = 0;
+
+  auto stage_chunk = [&](int c0, int b) {
+    const int f = c0 + lane;
+    const int fc = f < nx ? f : nx - 1;
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][nv][tid], a.V + nv * n + rb + fc);
+    if (lane == 31 || f + 1 >= nf) {
+      const int fp = gidx(fc + 1, nx, ob, 0);
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][NV + nv][tid], a.V + nv * n + rb + fp);
+    }
+    if (f < nf && (lane == 31 || f + 1 >= nf)) {  // one lane per chunk
+      const int fp2 = gidx(fc + 2, nx, ob, 0);
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) cp_async8(&stg2[b][w][nv], a.V + nv * n + rb + fp2);
+    }
+    if constexpr (PHYS != PHYS_HD) cp_async8(&stg[b][2 * NV][tid], a.Bs[0] + rb + fc);
+    cp_async_commit();
+  };
+  stage_chunk(0, 0);
+  int buf = 0;
+  for (int c0 = 0; c0 < nf; c0 += 32, buf ^= 1) {
+    const int f = c0 + lane;
+    const bool act = f < nf;
+    stage_chunk(c0 + 32 < nf ? c0 + 32 : c0, buf ^ 1);   // prefetch the next chunk
+    cp_async_wait1();
+    const bool selfp1 = (lane == 31) || (f + 1 >= nf);
+    R Vc[NV], vL[NV], vR[NV], vLn[NV], qm[2], qp[2];
+    // the lane before the chunk's last active lane takes V(f+2) from that
+    // lane's staged V(f+1)
+    const bool nextself = __shfl_down_sync(FULL, (int)selfp1, 1) != 0;
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      Vc[nv] = (R)stg[buf][nv][tid];
+      const R sp1 = selfp1 ? (R)stg[buf][NV + nv][tid] : R(0);
+      const R sp2 = (act && selfp1) ? (R)stg2[buf][w][nv] : R(0);
+      const R up1 = __shfl_up_sync(FULL, Vc[nv], 1);
+      const R up2 = __shfl_up_sync(FULL, Vc[nv], 2);
+      const R dn1 = __shfl_down_sync(FULL, Vc[nv], 1);
+      const R dn2 = __shfl_down_sync(FULL, Vc[nv], 2);
+      const R sp1n = __shfl_down_sync(FULL, sp1, 1);
+      const R vm1 = (lane == 0) ? pV1[nv] : up1;
+      const R vm2 = (lane == 0) ? pV2[nv] : ((lane == 1) ? pV1[nv] : up2);
+      const R vp1 = selfp1 ? sp1 : dn1;
+      const R vp2 = selfp1 ? sp2 : (nextself ? sp1n : dn2);
+      vLn[nv] = mp5_edge(vm2, vm1, Vc[nv], vp1, vp2);   // right edge: face f+1
+      vR[nv] = mp5_edge(vp2, vp1, Vc[nv], vm1, vm2);    // left edge: face f
+      if (nv == RHO) { qm[0] = vm1; qp[0] = vp1; }
+      if (nv == NV - 1) { qm[1] = vm1; qp[1] = vp1; }
+    }
+    mp5_fallback<PHYS, NV>(Vc, qm, qp, vR, vLn);
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      R l = __shfl_up_sync(FULL, vLn[nv], 1);
+      vL[nv] = (lane == 0) ? pVLn[nv] : l;
+    }
+    R Bn = R(0);
+    if constexpr (PHYS != PHYS_HD) {
+      Bn = (R)stg[buf][2 * NV][tid];
+      vL[BX1] = Bn;
+      vR[BX1] = Bn;
+    }
+    CTFace<R> ct;
+    uint32_t fe = 0;
+    cm = riemann<PHYS, RS, CT, 0>(vL, vR, F, gamma, Bn, ct, fe);
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++)
+      if (act && rhs_var<PHYS, NDIM>(nv) && isnan(F[nv])) fe |= ERR_NAN | ERR_QUIT;
+    if (fe && face_counts(g, 0, f, 1, row % g.ny, 2, row / g.ny)) err |= fe;
+    if constexpr (PHYS != PHYS_HD) {
+      if (act) store_ct(a, 0, rb + f, ct);
+    }
+    R Fm1[NV];
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      R t = __shfl_up_sync(FULL, F[nv], 1);
+      Fm1[nv] = (lane == 0) ? pF[nv] : t;
+    }
+    R cmm1;
+    {
+      R t = __shfl_up_sync(FULL, cm, 1);
+      cmm1 = (lane == 0) ? pCm : t;
+    }
+    if (act && f >= 1)
+      cell_update<PHYS, NV, NDIM>(a, n, rb + (f - 1), Fm1, F, cmm1, cm, 0);
+    if (c0 == 0) {
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) fF[nv] = F[nv];
+      fCm = cm;
+    }
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) {
+      pV2[nv] = __shfl_sync(FULL, Vc[nv], 30);
+      pV1[nv] = __shfl_sync(FULL, Vc[nv], 31);
+      pVLn[nv] = __shfl_sync(FULL, vLn[nv], 31);
+      pF[nv] = __shfl_sync(FULL, F[nv], 31);
+    }
+    pCm = __shfl_sync(FULL, cm, 31);
+  }
+  cp_async_wait0();
+  if (nf == nx) {  // periodic: the last cell's right face is face 0
+    R F0[NV];
+#pragma unroll
+    for (int nv = 0; nv < NV; nv++) F0[nv] = __shfl_sync(FULL, fF[nv], 0);
+    R cm0 = __shfl_sync(FULL, fCm, 0);
+    if (lane == ((nx - 1) & 31))
+      cell_update<PHYS, NV, NDIM>(a, n, rb + (nx - 1), F, F0, cm, cm0, 0);
+  }
+  if (err) atomicOr(a.err, err);
+}
+
 // One x-row per warp.  `stg_` is the block's staging area
 // (sweep_x_stage_doubles<NV>() doubles of shared memory), `tid` the thread's
 // index in its 128-thread block.
@@ -394,6 +569,10 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
                                             double* stg_, int tid) {
   if constexpr (LIM == LIM_PPM) {
     sweep_x_row_ppm<PHYS, NV, NDIM, RS, CT, R, CTT>(a, g, row, stg_, tid);
+    return;
+  }
+  if constexpr (LIM == LIM_MP5) {
+    sweep_x_row_mp5<PHYS, NV, NDIM, RS, CT, R, CTT>(a, g, row, stg_, tid);
     return;
   }
   constexpr unsigned FULL = 0xffffffffu;
@@ -648,6 +827,98 @@ __device__ __forceinline__ void sweep_m_col_ppm(const StageArgs<CTT>& a, const G
   if (err) atomicOr(a.err, err);
 }
 
+template <int PHYS, int NV, int NDIM, int RS, int CT, int DIR, typename R, typename CTT>
+__device__ __forceinline__ void sweep_m_col_mp5(const StageArgs<CTT>& a, const Grid3& g, int i,
+                                                int t, int seg, int S, double* stg_, int tid) {
+  double(*stg)[NV + 1][SWEEP_THREADS] = reinterpret_cast<double(*)[NV + 1][SWEEP_THREADS]>(stg_);
+  const int nd = (DIR == 1) ? g.ny : g.nz;
+  const long long n = g.n;
+  const R gamma = (R)a.gamma;
+  uint32_t err = 0;
+  if (i < g.nx) {
+    const long long stride = (DIR == 1) ? (long long)g.nx : (long long)g.nx * g.ny;
+    const long long base = (DIR == 1) ? i + (long long)g.nx * g.ny * t
+                                      : i + (long long)g.nx * t;
+    const int m0 = seg * S;
+    const int m1 = min(m0 + S, nd);
+    auto stage = [&](int mcell, int mface, int b) {
+      const long long cc = base + (long long)gidx(mcell, nd, g.outflow, DIR) * stride;
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) cp_async8(&stg[b][nv][tid], a.V + nv * n + cc);
+      if constexpr (PHYS != PHYS_HD)
+        cp_async8(&stg[b][NV][tid], a.Bs[DIR] + base + (long long)gidx(mface, nd, g.outflow, DIR) * stride);
+      cp_async_commit();
+    };
+    stage(m0 + 2, m0, 0);
+    // window: Wm = cell m-2, W0 = m-1, W1 = m, W2 = m+1, W3 = m+2
+    R Wm[NV], W0[NV], W1[NV], W2[NV], vLn[NV], Fp[NV], cmp = R(0);
+    {
+      R q3[NV];
+      load_cell<NV>(a.V, n, base + gidx(m0 - 3, nd, g.outflow, DIR) * stride, q3);
+      load_cell<NV>(a.V, n, base + gidx(m0 - 2, nd, g.outflow, DIR) * stride, Wm);
+      load_cell<NV>(a.V, n, base + gidx(m0 - 1, nd, g.outflow, DIR) * stride, W0);
+      load_cell<NV>(a.V, n, base + (long long)m0 * stride, W1);
+      load_cell<NV>(a.V, n, base + gidx(m0 + 1, nd, g.outflow, DIR) * stride, W2);
+      R vrp[NV];
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) {   // cell m0-1 (stencil m0-3 .. m0+1)
+        vLn[nv] = mp5_edge(q3[nv], Wm[nv], W0[nv], W1[nv], W2[nv]);
+        vrp[nv] = mp5_edge(W2[nv], W1[nv], W0[nv], Wm[nv], q3[nv]);
+        Fp[nv] = R(0);
+      }
+      const R qm[2] = {Wm[RHO], Wm[NV - 1]}, qp[2] = {W1[RHO], W1[NV - 1]};
+      mp5_fallback<PHYS, NV>(W0, qm, qp, vrp, vLn);
+    }
+    int buf = 0;
+    for (int m = m0; m <= m1; m++, buf ^= 1) {
+      stage(m + 3, m + 1, buf ^ 1);   // prefetch for the next iteration
+      cp_async_wait1();
+      R vL[NV], vR[NV], F[NV], W3[NV];
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) {
+        W3[nv] = (R)stg[buf][nv][tid];                             // cell m+2
+        vL[nv] = vLn[nv];
+        vLn[nv] = mp5_edge(Wm[nv], W0[nv], W1[nv], W2[nv], W3[nv]);  // cell m, right
+        vR[nv] = mp5_edge(W3[nv], W2[nv], W1[nv], W0[nv], Wm[nv]);   // cell m, left
+      }
+      {
+        const R qm[2] = {W0[RHO], W0[NV - 1]}, qp[2] = {W2[RHO], W2[NV - 1]};
+        mp5_fallback<PHYS, NV>(W1, qm, qp, vR, vLn);
+      }
+      R Bn = R(0);
+      if constexpr (PHYS != PHYS_HD) {
+        Bn = (R)stg[buf][NV][tid];
+        vL[BX1 + DIR] = Bn;
+        vR[BX1 + DIR] = Bn;
+      }
+      CTFace<R> ct;
+      uint32_t fe = 0;
+      R cm = riemann<PHYS, RS, CT, DIR>(vL, vR, F, gamma, Bn, ct, fe);
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++)
+        if (rhs_var<PHYS, NDIM>(nv) && isnan(F[nv])) fe |= ERR_NAN | ERR_QUIT;
+      if (fe && face_counts(g, DIR, m, 0, i, DIR == 1 ? 2 : 1, t)) err |= fe;
+      if constexpr (PHYS != PHYS_HD) {
+        if (m < m1) store_ct(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
+      }
+      if (m > m0)
+        cell_update<PHYS, NV, NDIM>(a, n, base + (long long)(m - 1) * stride, Fp, F, cmp, cm,
+                                    DIR);
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) {
+        Wm[nv] = W0[nv];
+        W0[nv] = W1[nv];
+        W1[nv] = W2[nv];
+        W2[nv] = W3[nv];
+        Fp[nv] = F[nv];
+      }
+      cmp = cm;
+    }
+    cp_async_wait0();
+  }
+  if (err) atomicOr(a.err, err);
+}
+
 // One (x column i, transverse index t, pencil segment seg) per thread: t is
 // k for DIR=1 and j for DIR=2; the segment covers cells [seg*S, seg*S+S).
 // `stg_` is the block's staging area (sweep_m_stage_doubles<NV>() doubles).
@@ -657,6 +928,10 @@ __device__ __forceinline__ void sweep_m_col(const StageArgs<CTT>& a, const Grid3
                                             int seg, int S, double* stg_, int tid) {
   if constexpr (LIM == LIM_PPM) {
     sweep_m_col_ppm<PHYS, NV, NDIM, RS, CT, DIR, R, CTT>(a, g, i, t, seg, S, stg_, tid);
+    return;
+  }
+  if constexpr (LIM == LIM_MP5) {
+    sweep_m_col_mp5<PHYS, NV, NDIM, RS, CT, DIR, R, CTT>(a, g, i, t, seg, S, stg_, tid);
     return;
   }
   double(*stg)[NV + 1][SWEEP_THREADS] = reinterpret_cast<double(*)[NV + 1][SWEEP_THREADS]>(stg_);
@@ -758,14 +1033,26 @@ __global__ void __launch_bounds__(SWEEP_THREADS, (sweep_m_minb<PHYS, R>()))
 // UCT edge EMF (Src/MHD/CT/ct_emf_average.cpp:535-995, reconstruction of
 // Src/array_reconstruct.cpp:45-206: face field with MC, stored velocities
 // with the scheme limiter).
-// b[0..3], q[0..3]: values at the four cells straddling the edge along the
-// reconstruction direction (edge between b[1] and b[2]).
+// b[0..W-1], q[0..W-1]: values at the W cells straddling the edge along the
+// reconstruction direction, W = emf_width<LIM>() (edge between b[W/2-1] and
+// b[W/2]).
 // ---------------------------------------------------------------------
+template <int LIM>
+__device__ __forceinline__ constexpr int emf_width() { return LIM == LIM_MP5 ? 6 : 4; }
+
 template <int LIM, typename R>
 __device__ __forceinline__ void uct_terms(const R* b, const R* q, R aL, R aR, R dL, R dR,
                                           R& avg, R& phi) {
   R bL, bR, vL, vR;
-  if constexpr (LIM == LIM_PPM) {
+  if constexpr (LIM == LIM_MP5) {
+    // MP5 edge values of both the face field and the velocity
+    // (Src/array_reconstruct.cpp:327-384): the right edge of cell b[2] and
+    // the left edge of cell b[3]
+    bL = mp5_edge(b[0], b[1], b[2], b[3], b[4]);
+    bR = mp5_edge(b[5], b[4], b[3], b[2], b[1]);
+    vL = mp5_edge(q[0], q[1], q[2], q[3], q[4]);
+    vR = mp5_edge(q[5], q[4], q[3], q[2], q[1]);
+  } else if constexpr (LIM == LIM_PPM) {
     // parabolic reconstruction of both the face field and the velocity
     // (Src/MHD/CT/ct_emf_average.cpp:556-559 with RECONSTRUCTION PARABOLIC)
     R p1, m1, p2, m2;
@@ -802,7 +1089,8 @@ __device__ __forceinline__ void face_coef(const StageArgs<CTT>& a, int d, long l
 
 // The edge EMFs whose lower corner is cell c (all three in 3-D, Ez in 2-D).
 // The wrapped offsets of the stencil rows (index - 2 .. index + 1 along each
-// direction) are formed once; every operand address is then a sum of three.
+// direction; index - 3 .. index + 2 with MP5) are formed once; every operand
+// address is then a sum of three.
 // Offsets are 32-bit: grids are limited to fewer than 2^31 cells.
 template <int NDIM, int LIM, typename R, typename CTT>
 __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g, long long c) {
@@ -813,32 +1101,33 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
   const int i = ci % nx;
   const int j = (ci / nx) % ny;
   const int k = ci / nxy;
-  int X[4], Y[4], Z[4];
+  constexpr int W = emf_width<LIM>(), C = W / 2;  // stencil cells i-C .. i+C-1
+  int X[W], Y[W], Z[W];
 #pragma unroll
-  for (int m = 0; m < 4; m++) {
-    X[m] = wrapi(i - 2 + m, nx);
-    Y[m] = nx * wrapi(j - 2 + m, ny);
-    Z[m] = NDIM == 3 ? nxy * wrapi(k - 2 + m, nz) : 0;
+  for (int m = 0; m < W; m++) {
+    X[m] = wrapi(i - C + m, nx);
+    Y[m] = nx * wrapi(j - C + m, ny);
+    Z[m] = NDIM == 3 ? nxy * wrapi(k - C + m, nz) : 0;
   }
-  R b[4], q[4], aL, aR, dL, dR, avg, phi;
+  R b[W], q[W], aL, aR, dL, dR, avg, phi;
   // Ez at (i-1/2, j-1/2, k)
   {
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-      const int e = X[m] + Y[2] + Z[2];
+    for (int m = 0; m < W; m++) {
+      const int e = X[m] + Y[C] + Z[C];
       b[m] = (R)a.Bs[1][e];
       q[m] = (R)a.ct[1][1][e];
     }
-    face_coef<R>(a, 0, X[2] + Y[1] + Z[2], c, aL, aR, dL, dR);
+    face_coef<R>(a, 0, X[C] + Y[C - 1] + Z[C], c, aL, aR, dL, dR);
     uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
     R Ez = avg + phi;
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-      const int e = X[2] + Y[m] + Z[2];
+    for (int m = 0; m < W; m++) {
+      const int e = X[C] + Y[m] + Z[C];
       b[m] = (R)a.Bs[0][e];
       q[m] = (R)a.ct[0][0][e];
     }
-    face_coef<R>(a, 1, X[1] + Y[2] + Z[2], c, aL, aR, dL, dR);
+    face_coef<R>(a, 1, X[C - 1] + Y[C] + Z[C], c, aL, aR, dL, dR);
     uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
     Ez += avg - phi;
     a.Ee[2][c] = (CTT)Ez;
@@ -847,21 +1136,21 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
     // Ey at (i-1/2, j, k-1/2)
     {
 #pragma unroll
-      for (int m = 0; m < 4; m++) {
-        const int e = X[m] + Y[2] + Z[2];
+      for (int m = 0; m < W; m++) {
+        const int e = X[m] + Y[C] + Z[C];
         b[m] = (R)a.Bs[2][e];
         q[m] = (R)a.ct[2][0][e];
       }
-      face_coef<R>(a, 0, X[2] + Y[2] + Z[1], c, aL, aR, dL, dR);
+      face_coef<R>(a, 0, X[C] + Y[C] + Z[C - 1], c, aL, aR, dL, dR);
       uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
       R Ey = avg - phi;
 #pragma unroll
-      for (int m = 0; m < 4; m++) {
-        const int e = X[2] + Y[2] + Z[m];
+      for (int m = 0; m < W; m++) {
+        const int e = X[C] + Y[C] + Z[m];
         b[m] = (R)a.Bs[0][e];
         q[m] = (R)a.ct[0][1][e];
       }
-      face_coef<R>(a, 2, X[1] + Y[2] + Z[2], c, aL, aR, dL, dR);
+      face_coef<R>(a, 2, X[C - 1] + Y[C] + Z[C], c, aL, aR, dL, dR);
       uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
       Ey += avg + phi;
       a.Ee[1][c] = (CTT)Ey;
@@ -869,21 +1158,21 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
     // Ex at (i, j-1/2, k-1/2)
     {
 #pragma unroll
-      for (int m = 0; m < 4; m++) {
-        const int e = X[2] + Y[m] + Z[2];
+      for (int m = 0; m < W; m++) {
+        const int e = X[C] + Y[m] + Z[C];
         b[m] = (R)a.Bs[2][e];
         q[m] = (R)a.ct[2][1][e];
       }
-      face_coef<R>(a, 1, X[2] + Y[2] + Z[1], c, aL, aR, dL, dR);
+      face_coef<R>(a, 1, X[C] + Y[C] + Z[C - 1], c, aL, aR, dL, dR);
       uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
       R Ex = avg + phi;
 #pragma unroll
-      for (int m = 0; m < 4; m++) {
-        const int e = X[2] + Y[2] + Z[m];
+      for (int m = 0; m < W; m++) {
+        const int e = X[C] + Y[C] + Z[m];
         b[m] = (R)a.Bs[1][e];
         q[m] = (R)a.ct[1][0][e];
       }
-      face_coef<R>(a, 2, X[2] + Y[1] + Z[2], c, aL, aR, dL, dR);
+      face_coef<R>(a, 2, X[C] + Y[C - 1] + Z[C], c, aL, aR, dL, dR);
       uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
       Ex += avg - phi;
       a.Ee[0][c] = (CTT)Ex;

@@ -94,7 +94,7 @@ static void run_stage(const StageArgs<CTT>& a, const GridDims& gd, int seg, cuda
   const unsigned nb = (unsigned)((gd.n + 255) / 256);
   if constexpr (PHYS != PHYS_HD) {
     pre();
-    if constexpr (NDIM == 3 && sizeof(RT) == 4) {  // mixed form: z-marching EMF
+    if constexpr (NDIM == 3 && sizeof(RT) == 4 && LIM != LIM_MP5) {  // mixed: z-marching EMF
       // the longest segment (<= EMF_SEGMENT planes) that still gives about
       // four waves of blocks over 148 SMs (3 blocks per SM)
       const long long cols = (long long)((gd.nx + EMF_TX - 1) / EMF_TX) *
@@ -122,6 +122,7 @@ static int by_lim(const StageArgs<CTT>& a, const GridDims& g, int lim, int seg, 
     case LIM_VL: run_stage<PHYS, NV, NDIM, RS, CT, LIM_VL>(a, g, seg, s, ev); return 0;
     case LIM_MINMOD: run_stage<PHYS, NV, NDIM, RS, CT, LIM_MINMOD>(a, g, seg, s, ev); return 0;
     case LIM_PPM: run_stage<PHYS, NV, NDIM, RS, CT, LIM_PPM>(a, g, seg, s, ev); return 0;
+    case LIM_MP5: run_stage<PHYS, NV, NDIM, RS, CT, LIM_MP5>(a, g, seg, s, ev); return 0;
     default: return -1;
   }
 }

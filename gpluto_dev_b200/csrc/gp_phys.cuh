@@ -31,9 +31,10 @@ constexpr uint32_t ERR_NAN = 1u << 11;
 constexpr uint32_t ERR_QUIT = 1u << 15;
 
 enum : int { PHYS_HD = 0, PHYS_MHD = 1, PHYS_RMHD = 2 };
-// LIM_PPM selects piecewise parabolic reconstruction (RECONSTRUCTION
-// PARABOLIC); it is carried in the limiter slot of the scheme templates.
-enum : int { LIM_FLAT = 0, LIM_MINMOD = 1, LIM_VL = 2, LIM_MC = 3, LIM_PPM = 4 };
+// LIM_PPM and LIM_MP5 select piecewise parabolic and monotonicity-preserving
+// 5th-order reconstruction (RECONSTRUCTION PARABOLIC / MP5); they are
+// carried in the limiter slot of the scheme templates.
+enum : int { LIM_FLAT = 0, LIM_MINMOD = 1, LIM_VL = 2, LIM_MC = 3, LIM_PPM = 4, LIM_MP5 = 5 };
 enum : int { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2 };
 enum : int { CT_UCT_HLL = 0, CT_UCT_HLLD = 1 };
 
@@ -72,6 +73,44 @@ __device__ __forceinline__ R limit(R dvp, R dvm) {
 template <typename R>
 __device__ __forceinline__ R minmod(R a, R b) {
   return (a * b > R(0) ? (rabs(a) < rabs(b) ? a : b) : R(0));
+}
+
+// MP5 edge value of Suresh & Huynh (1997) (Src/States/states.hpp:32-98,
+// MP5_ALPHA 4, reconstruction from cell averages).  The stencil is ordered
+// towards the edge: F0 the cell, Fp and Fpp the next cells on the edge's
+// side, Fm and Fmm the cells on the other side.
+template <typename R>
+__device__ __forceinline__ R mp5_edge(R Fmm, R Fm, R F0, R Fp, R Fpp) {
+  const R alpha = R(4), epsm = R(1.e-12);
+  const R dFp = Fp - F0, dFm = F0 - Fm;
+  R f = R(2) * Fmm - R(13) * Fm + R(47) * F0 + R(27) * Fp - R(3) * Fpp;  // Eq. (2.1)
+  f /= R(60);
+  const R fMP = F0 + minmod(dFp, alpha * dFm);                          // Eq. (2.12)
+  if ((f - F0) * (f - fMP) <= epsm) return f;
+  const R d2m = Fmm + F0 - R(2) * Fm;
+  const R d2 = Fm + Fp - R(2) * F0;
+  const R d2p = F0 + Fpp - R(2) * Fp;
+  R s1 = minmod(R(4) * d2 - d2p, R(4) * d2p - d2);
+  R s2 = minmod(d2, d2p);
+  const R dMMp = minmod(s1, s2);                                       // Eq. (2.27)
+  s1 = minmod(R(4) * d2m - d2, R(4) * d2 - d2m);
+  s2 = minmod(d2, d2m);
+  const R dMMm = minmod(s1, s2);
+  const R fUL = F0 + alpha * dFm;                                      // Eq. (2.8)
+  const R fAV = R(0.5) * (F0 + Fp);                                    // Eq. (2.16)
+  const R fMD = fAV - R(0.5) * dMMp;                                   // Eq. (2.28)
+  const R fLC = R(0.5) * (R(3) * F0 - Fm) + R(4.0 / 3.0) * dMMm;       // Eq. (2.29)
+  s1 = GP_MIN(F0, Fp);
+  s1 = GP_MIN(s1, fMD);
+  s2 = GP_MIN(F0, fUL);
+  s2 = GP_MIN(s2, fLC);
+  const R fmin = GP_MAX(s1, s2);                                       // Eq. (2.24a)
+  s1 = GP_MAX(F0, Fp);
+  s1 = GP_MAX(s1, fMD);
+  s2 = GP_MAX(F0, fUL);
+  s2 = GP_MAX(s2, fLC);
+  const R fmax = GP_MIN(s1, s2);                                       // Eq. (2.24b)
+  return f + minmod(fmin - f, fmax - f);                               // Eq. (2.26)
 }
 
 // PPM constrained face value between cells q0 and qp (stencil qm, q0, qp,

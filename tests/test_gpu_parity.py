@@ -212,6 +212,55 @@ def test_gpu_rk3_matches_oracle_bitwise(case):
         np.testing.assert_array_equal(a, b)
 
 
+MP5_CASES = [
+    # (generator, kwargs, solver, ct, side masks, rk, nsteps): rows of 33 and 65
+    # cells (a last chunk of 1 and of 1 face), a row shorter than a warp, 3-D
+    # marches, mirrored and outflow sides
+    (ics.mhd2d_turbulence, dict(n=(33, 20), seed=111), "hlld", "uct_hlld", dict(), 2, 10),
+    (ics.mhd2d_turbulence, dict(n=(65, 7), seed=112), "hll", "uct_hll",
+     dict(reflect=0b0011, outflow=0b1100), 3, 8),
+    (ics.mhd3d_turbulence, dict(n=(7, 12, 10), seed=113), "hlld", "uct_hlld",
+     dict(eqtsym=0b110000), 2, 6),
+    (ics.hd_turbulence, dict(n=(30, 9, 11), seed=114), "hllc", "uct_hll",
+     dict(outflow=0b000011, reflect=0b001100), 3, 8),
+]
+
+
+@pytest.mark.parametrize("case", range(len(MP5_CASES)))
+def test_gpu_mp5_matches_oracle_bitwise(case):
+    gen, kw, rs, ct, bc, rk, nsteps = MP5_CASES[case]
+    st = gen(**kw)
+    kwo = dict(limiter="mp5", solver=rs, rk=rk, **bc)
+    if st.physics != ics.PHYS_HD:
+        kwo["ct"] = ct
+    o = orc.Oracle(st, **kwo)
+    ohist, oerr = o.run(nsteps, 1e-4)
+    Vo, Uo, Bo = o.state()
+    s = make_solver(st, "mp5", rs, ct, rk=rk, **bc)
+    dt_after, hist, out = s.run(nsteps, 1e-4)
+    V, U, Bs = s.download()
+    assert out.err_bits == oerr
+    np.testing.assert_array_equal(hist, ohist[:-1])
+    np.testing.assert_array_equal(V, Vo)
+    np.testing.assert_array_equal(U, Uo)
+    for a, b in zip(Bs, Bo):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_mp5_mixed_form_stays_close_to_fp64():
+    st = ics.mhd3d_blast(n=(32, 32, 32), seed=115, radius=0.2)
+    a = make_solver(st, "mp5", "hlld", "uct_hlld")
+    _, hist, _ = a.run(20, 1e-4)
+    b = make_solver(st, "mp5", "hlld", "uct_hlld", precision=api.MIXED)
+    for dt in hist:
+        b.AdvanceStep(float(dt))
+    Ua, Ub = a.download()[1], b.download()[1]
+    for nv in range(8):
+        den = np.abs(Ua[nv]).sum()
+        if den > 0:
+            assert np.abs(Ub[nv] - Ua[nv]).sum() / den <= 1e-5, nv
+
+
 def test_ct_outflow_reference_layout_needs_the_scheme_ghost_depth():
     st = ics.mhd2d_turbulence(n=(20, 16), seed=62)
     s = make_solver(st, "mc", "hlld", "uct_hlld", outflow=0b0011)
