@@ -268,7 +268,7 @@ def mixed_error(make_solver, nsteps, st):
             "divB_rel_max": float(np.abs(div).max()) / (bmax / min(dx))}
 
 
-def measure_e2e(make_solver, ncell, world, steps, barrier, dist):
+def measure_e2e(make_solver, ncell, steps, ranks):
     """End to end through the C ABI with host buffers.
 
     Per step: host (pinned) -> device upload of the full reference-layout
@@ -292,7 +292,7 @@ def measure_e2e(make_solver, ncell, world, steps, barrier, dist):
     k = max(1, min(steps, 10))
     de = FIRST_DT
     torch.cuda.synchronize()
-    barrier()
+    ranks.barrier()
     t0 = time.perf_counter()
     for _ in range(k):
         api._check(L.gp_upload_state(se._h, api.LAYOUT_REFERENCE, api._dp(hU), api._dp(hV),
@@ -302,13 +302,10 @@ def measure_e2e(make_solver, ncell, world, steps, barrier, dist):
         dl()
     torch.cuda.synchronize()
     te = time.perf_counter() - t0
-    if dist is not None:
-        tt = torch.tensor([te], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        te = float(tt.item())
+    te = ranks.max_over_ranks(te)
     nbytes = (hU.numel() + hV.numel() + sum(b.numel() for b in hB if b is not None)) * 8
     se.close()
-    return {"value": world * ncell * k / te / 1e6, "unit": METRIC,
+    return {"value": ranks.world * ncell * k / te / 1e6, "unit": METRIC,
             "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": k,
             "path": "gp_upload_state(reference layout, pinned host) + gp_advance_step + "
                     "gp_download_state(reference layout) per step"}
@@ -318,25 +315,15 @@ def measure_e2e(make_solver, ncell, world, steps, barrier, dist):
 # --------------------------------------------------------------------------
 def impl_ours(args):
     import torch
-    from gpluto_dev_b200 import api, ics
+    from gpluto_dev_b200 import api, ics, replicas
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    ranks = replicas.init("nccl")          # replicas: one grid (set) per GPU
+    world, rank, local = ranks.world, ranks.rank, ranks.local
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
+    barrier = ranks.barrier
 
     n = args.n
-    st = ics.mhd3d_blast(n=(n, n, n), seed=1 + rank)
+    st = ics.mhd3d_blast(n=(n, n, n), seed=replicas.replica_seed(1, rank))
     ncell = n ** 3
 
     def solver(precision):
@@ -361,12 +348,9 @@ def impl_ours(args):
     clocks = clock.stop()
     barrier()
     t_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+    t_ms = ranks.max_over_ranks(t_ms)
     ms_step = t_ms / args.steps
-    value = world * ncell * args.steps / (t_ms * 1e-3) / 1e6
+    value = replicas.whole_job_rate(world, ncell, args.steps, t_ms)
     launches = args.steps * s64.launches_per_step
 
     # ---- per-kernel timing (CUDA events around every launch) -----------
@@ -408,11 +392,8 @@ def impl_ours(args):
         torch.cuda.synchronize()
         barrier()
         tm = e0.elapsed_time(e1)
-        if dist is not None:
-            tt = torch.tensor([tm], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            tm = float(tt.item())
-        mixed = {"value": world * ncell * args.steps / (tm * 1e-3) / 1e6,
+        tm = ranks.max_over_ranks(tm)
+        mixed = {"value": replicas.whole_job_rate(world, ncell, args.steps, tm),
                  "ms_per_step": tm / args.steps}
         mixed["speedup_vs_fp64"] = mixed["value"] / value
         mprof, _ = smx.profile(3, d2)
@@ -428,7 +409,7 @@ def impl_ours(args):
     # Per step: host (pinned) -> device upload of the full reference-layout
     # state (Uc, Vc, Vs with ghost zones, as Data holds it), one AdvanceStep,
     # device -> host download of the same arrays.
-    e2e = None if args.no_e2e else measure_e2e(solver, ncell, world, args.steps, barrier, dist)
+    e2e = None if args.no_e2e else measure_e2e(solver, ncell, args.steps, ranks)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -436,9 +417,7 @@ def impl_ours(args):
         v, sps, cores, kind, sample = run_reference_sample(nproc, 2, 1)
         cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample}
 
-    if dist is not None:
-        barrier()
-        dist.destroy_process_group()
+    ranks.close()
     if rank != 0:
         return 0
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
@@ -554,25 +533,15 @@ def _oracle_grid_worker(a):
 
 def impl_ensemble(args):
     import torch
-    from gpluto_dev_b200 import autotune, workloads
+    from gpluto_dev_b200 import autotune, replicas, workloads
     from gpluto_dev_b200 import batch as gb
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    ranks = replicas.init("nccl")          # replicas: one grid (set) per GPU
+    world, rank, local = ranks.world, ranks.rank, ranks.local
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    barrier = ranks.barrier
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    members = workloads.ensemble(args.grids, seed0=rank * args.grids)
+    members = workloads.ensemble(args.grids, seed0=replicas.replica_seed(0, rank, args.grids))
     cells = sum(m.state.ncells for m in members)
     stream = torch.cuda.Stream()
     pool = sum(gb.slot_bytes(m.state, m.scheme) for m in members) + (64 << 20)
@@ -611,10 +580,7 @@ def impl_ensemble(args):
     clocks = clock.stop()
     barrier()
     t_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+    t_ms = ranks.max_over_ranks(t_ms)
     err = 0
     done = []
     for s in slots:
@@ -624,7 +590,7 @@ def impl_ensemble(args):
     ctas = b.info()["ctas"]
     b.close()
     del b
-    value = world * cells * args.steps / (t_ms * 1e-3) / 1e6
+    value = replicas.whole_job_rate(world, cells, args.steps, t_ms)
     peak, peak_kind = peaks()
     achieved = ENSEMBLE_ALG_BYTES_ZONE * cells * args.steps / (t_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": "batch_sweep_kernel + batch_cell_kernel (all grids)",
@@ -652,10 +618,7 @@ def impl_ensemble(args):
         te = time.perf_counter() - t0
         b.close()
         nin = sum((m.state.V.size + sum(x.size for x in m.state.Bs)) * 8 for m in members)
-        if dist is not None:
-            tt = torch.tensor([te], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
+        te = ranks.max_over_ranks(te)
         e2e = {"value": world * cells * args.steps / te / 1e6, "unit": METRIC,
                "h2d_bytes_per_step": nin / args.steps, "d2h_bytes_per_step": nout / args.steps,
                "steps": args.steps,
@@ -666,9 +629,7 @@ def impl_ensemble(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu, _ = ensemble_cpu_baseline(args, max(1, min(os.cpu_count() or 1, 16)))
 
-    if dist is not None:
-        barrier()
-        dist.destroy_process_group()
+    ranks.close()
     if rank != 0:
         return 0
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
