@@ -57,3 +57,40 @@ def test_mixed_l1_error_and_divb(case):
         assert l1 <= 1e-5, (case, nv, l1)
     assert divb_rel(Bb, st.shape, st.ndim) <= 1e-12
     assert divb_rel(Ba, st.shape, st.ndim) <= 1e-12
+
+
+MIXED_SCHEMES = [
+    # (generator, kwargs, limiter, solver, ct, Solver keyword arguments, rk, nsteps)
+    (ics.hd_turbulence, dict(n=(96, 80), seed=121), "mc", "hllc", "uct_hll", dict(), 2, 40),
+    (ics.mhd2d_turbulence, dict(n=(96, 96), seed=122), "ppm", "hlld", "uct_hlld", dict(), 2, 40),
+    (ics.mhd2d_turbulence, dict(n=(80, 64), seed=123), "mc", "hlld", "uct_hlld",
+     dict(outflow=0b0011, reflect=0b1100), 3, 30),
+    (ics.mhd3d_turbulence, dict(n=(40, 36, 32), seed=124), "vl", "hll", "uct_hll",
+     dict(eqtsym=0b110000), 3, 15),
+]
+
+
+@pytest.mark.parametrize("case", range(len(MIXED_SCHEMES)))
+def test_mixed_l1_error_other_schemes(case):
+    """The ≤ 1e-5 relative L1 bound of the mixed form for HD, PPM, RK3 and
+    non-periodic sides, on the FP64 run's dt sequence."""
+    gen, kw, lim, rs, ct, bc, rk, n = MIXED_SCHEMES[case]
+    st = gen(**kw)
+
+    def scheme(prec):
+        return api.Scheme(physics=st.physics, limiter=lim, riemann=rs, ct_emf=ct,
+                          gamma=st.gamma, precision=prec, rk=rk)
+    a = api.Solver.from_state(st, scheme(api.FP64), **bc)
+    _, hist, oa = a.run(n, 1e-4)
+    b = api.Solver.from_state(st, scheme(api.MIXED), **bc)
+    for dt in hist:
+        ob = b.AdvanceStep(float(dt))
+    Ua, Ub = a.download()[1], b.download()[1]
+    a.close()
+    b.close()
+    assert oa.err_bits & api.ERR_QUIT == 0 and ob.err_bits & api.ERR_QUIT == 0
+    for nv in range(Ua.shape[0]):
+        den = np.abs(Ua[nv]).sum()
+        if den == 0.0:
+            continue
+        assert np.abs(Ub[nv] - Ua[nv]).sum() / den <= 1e-5, (case, nv)
