@@ -382,3 +382,47 @@ def test_full_size_2d_100_steps_matches_oracle():
     for nv in range(8):
         assert rel_linf(U[nv], Uo[nv]) <= RTOL_FP64
     assert np.array_equal(U, Uo)
+
+
+TINY_CASES = [
+    # the smallest grids: 2-3 cells along a direction (stencils wrap more
+    # than once), PLM needs 2, PPM/MP5 4
+    (ics.mhd2d_turbulence, dict(n=(2, 3), seed=131), "mc", "hlld", "uct_hlld", dict(), 6),
+    (ics.mhd3d_turbulence, dict(n=(3, 2, 2), seed=132), "vl", "hll", "uct_hll", dict(), 4),
+    (ics.hd_turbulence, dict(n=(2, 2, 3), seed=133), "mc", "hllc", "uct_hll", dict(), 6),
+    (ics.mhd2d_turbulence, dict(n=(4, 5), seed=134), "ppm", "hlld", "uct_hlld", dict(), 5),
+    (ics.mhd2d_turbulence, dict(n=(5, 4), seed=135), "mp5", "hlld", "uct_hlld", dict(), 5),
+    (ics.mhd2d_turbulence, dict(n=(4, 4), seed=136), "mc", "hlld", "uct_hlld",
+     dict(outflow=0b0011, reflect=0b1100), 5),
+]
+
+
+@pytest.mark.parametrize("case", range(len(TINY_CASES)))
+def test_gpu_tiny_grids_match_oracle_bitwise(case):
+    gen, kw, lim, rs, ct, bc, nsteps = TINY_CASES[case]
+    st = gen(**kw)
+    kwo = dict(limiter=lim, solver=rs, **bc)
+    if st.physics != ics.PHYS_HD:
+        kwo["ct"] = ct
+    o = orc.Oracle(st, **kwo)
+    ohist, oerr = o.run(nsteps, 1e-4)
+    Vo, Uo, Bo = o.state()
+    s = make_solver(st, lim, rs, ct, **bc)
+    dt_after, hist, out = s.run(nsteps, 1e-4)
+    V, U, Bs = s.download()
+    assert out.err_bits == oerr
+    np.testing.assert_array_equal(hist, ohist[:-1])
+    np.testing.assert_array_equal(V, Vo)
+    np.testing.assert_array_equal(U, Uo)
+    for a, b in zip(Bs, Bo):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_grids_beyond_the_cell_limit_are_refused_before_allocating():
+    sch = api.Scheme(physics=api.MHD)
+    with pytest.raises(api.GPError) as ei:          # 2048^3 > 2^31 cells
+        api.Solver(3, (2048, 2048, 2048), sch)
+    assert ei.value.code == -2
+    with pytest.raises(api.GPError) as ei:          # PPM below 4 cells
+        api.Solver(2, (3, 8), api.Scheme(physics=api.MHD, limiter="ppm"))
+    assert ei.value.code == api.GP_ERR_INVALID
