@@ -168,7 +168,7 @@ SlotLayout slot_layout(const gp_grid_desc* g, const gp_scheme* sc) {
   L.ndim = g->ndim;
   const long long nz = g->ndim == 3 ? g->nint[2] : 1;
   L.n = (long long)g->nint[0] * g->nint[1] * nz;
-  L.mhd = sc->physics == GP_MHD;
+  L.mhd = sc->physics != GP_HD;  // MHD and RMHD: staggered fields, UCT data, EMFs
   L.mixed = sc->precision == GP_MIXED;
   L.nvar = L.mhd ? 8 : 5;
   const size_t cell = sizeof(double) * (size_t)L.n;
@@ -194,6 +194,7 @@ bool scheme_built(const gp_scheme* sc) {
   if (sc->limiter != GP_LIM_MC || sc->reconstruction != GP_REC_LINEAR) return false;
   if (sc->precision != GP_FP64 && sc->precision != GP_MIXED) return false;
   if (sc->physics == GP_MHD) return sc->riemann == GP_RS_HLLD && sc->ct_emf == GP_CT_UCT_HLLD;
+  if (sc->physics == GP_RMHD) return sc->riemann == GP_RS_HLLD && sc->ct_emf == GP_CT_UCT_HLL;
   if (sc->physics == GP_HD) return sc->riemann == GP_RS_HLLC;
   return false;
 }
@@ -302,7 +303,7 @@ void tile_counts(BatchSlot& s) {
   s.ntiles[gp::BP_SWEEP_Z] = s.ndim == 3 ? items(s.nz, s.ny) : 0;
   const long long per = (long long)gp::BATCH_THREADS * s.cpt;
   const int cells = (int)((s.n + per - 1) / per);
-  s.ntiles[gp::BP_EMF] = s.physics == gp::PHYS_MHD ? cells : 0;
+  s.ntiles[gp::BP_EMF] = s.physics != gp::PHYS_HD ? cells : 0;
   s.ntiles[gp::BP_FINISH] = cells;
   s.need[gp::BG_SWEEPS] = s.ntiles[0] + s.ntiles[1] + s.ntiles[2];
   s.need[gp::BG_EMF] = s.ntiles[gp::BP_EMF];
@@ -477,14 +478,15 @@ int gp_batch_add(gp_batch* b, const gp_grid_desc* grid, const gp_scheme* scheme,
   if (grid->ndim != 2 && grid->ndim != 3) return gp::fail(GP_ERR_UNSUPPORTED, "ndim must be 2 or 3");
   if (!gp::scheme_built(scheme))
     return gp::fail(GP_ERR_UNSUPPORTED,
-                    "batches are built for MHD PLM-MC/HLLD/UCT_HLLD and HD PLM-MC/HLLC, RK2");
+                    "batches are built for MHD PLM-MC/HLLD/UCT_HLLD, RMHD PLM-MC/HLLD/UCT_HLL "
+                    "and HD PLM-MC/HLLC, RK2");
   for (int d = 0; d < grid->ndim; d++) {
     if (grid->nint[d] < 2) return gp::fail(GP_ERR_INVALID, "nint[%d] < 2", d);
     if (grid->lbound[d] != GP_BC_PERIODIC || grid->rbound[d] != GP_BC_PERIODIC)
       return gp::fail(GP_ERR_UNSUPPORTED, "only periodic boundaries are built");
   }
   if (!(dt0 > 0.0) || nsteps < 0) return gp::fail(GP_ERR_INVALID, "bad dt0 or nsteps");
-  const bool mhd = scheme->physics == GP_MHD;
+  const bool mhd = scheme->physics != GP_HD;  // staggered fields (MHD, RMHD)
   if (mhd && (!Vs0 || !Vs1 || (grid->ndim == 3 && !Vs2)))
     return gp::fail(GP_ERR_INVALID, "face fields missing");
   int idx = -1;

@@ -5,9 +5,9 @@
 // GP_MIXED=0 (FP64, -fmad=false: bit-identical to the single-grid FP64 step)
 // and GP_MIXED=1 (FP32 reconstruction/Riemann/EMF, contraction allowed).
 //
-// Schemes built for batches: ideal MHD with PLM-MC + HLLD + UCT_HLLD and
-// hydrodynamics with PLM-MC + HLLC, in 2-D and 3-D (the ensemble and serving
-// workloads); the host refuses any other combination.
+// Schemes built for batches: ideal MHD with PLM-MC + HLLD + UCT_HLLD,
+// relativistic MHD with PLM-MC + HLLD + UCT_HLL, and hydrodynamics with
+// PLM-MC + HLLC, in 2-D and 3-D; the host refuses any other combination.
 #include "gp_batch.h"
 
 #ifndef GP_MIXED
@@ -152,6 +152,13 @@ __device__ void GP_BATCH_TILE(const BatchSlot& s, const BatchTile& t, int stage)
     else
       run_tile<PHYS_MHD, 8, 3, RS_HLLD, CT_UCT_HLLD, LIM_MC>(a, g, seg, cpt, t.phase, t.idx,
                                                              stage, smem);
+  } else if (s.physics == PHYS_RMHD) {
+    if (s.ndim == 2)
+      run_tile<PHYS_RMHD, 8, 2, RS_HLLD, CT_UCT_HLL, LIM_MC>(a, g, seg, cpt, t.phase, t.idx,
+                                                            stage, smem);
+    else
+      run_tile<PHYS_RMHD, 8, 3, RS_HLLD, CT_UCT_HLL, LIM_MC>(a, g, seg, cpt, t.phase, t.idx,
+                                                            stage, smem);
   } else {
     if (s.ndim == 2)
       run_tile<PHYS_HD, 5, 2, RS_HLLC, 0, LIM_MC>(a, g, seg, cpt, t.phase, t.idx, stage, smem);

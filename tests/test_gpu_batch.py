@@ -28,6 +28,11 @@ def hd(precision=api.FP64):
     return api.Scheme(physics=api.HD, riemann="hllc", precision=precision)
 
 
+def rmhd(precision=api.FP64):
+    return api.Scheme(physics=api.RMHD, riemann="hlld", ct_emf="uct_hll", cfl=0.3,
+                      precision=precision)
+
+
 def cases():
     # uneven sizes: rows not a multiple of 32, odd pencils, 2-D and 3-D
     return [
@@ -40,6 +45,10 @@ def cases():
         ("mhd2d_mixed_96x64", ics.mhd2d_turbulence(n=(96, 64), seed=77), mhd(api.MIXED)),
         ("mhd3d_mixed_16x16x24", ics.mhd3d_turbulence(n=(16, 16, 24), seed=78), mhd(api.MIXED)),
         ("hd2d_mixed_48x48", ics.hd_turbulence(n=(48, 48), seed=79), hd(api.MIXED)),
+        ("rmhd3d_20x12x10", ics.rmhd3d_turbulence(n=(20, 12, 10), seed=80, lorentz_max=5.0),
+         rmhd()),
+        ("rmhd3d_mixed_16x18x8", ics.rmhd3d_turbulence(n=(16, 18, 8), seed=81, lorentz_max=5.0),
+         rmhd(api.MIXED)),
     ]
 
 
