@@ -1334,6 +1334,258 @@ __global__ void __launch_bounds__(EMF_TX * EMF_TY, 3)
   }
 }
 
+// 3-D edge EMFs with the in-plane stencils staged in shared memory.  Blocks
+// of ETX x ETY (i, j) columns march k over a segment of planes.  While plane
+// k is computed, the block's cp.async copies of plane k+1 fill the other half
+// of a double buffer: the face fields and velocities along x and along y with
+// their stencil halos, and the three directions' face coefficients with their
+// i-1 / j-1 neighbours, each tile row a contiguous run of one array.  The
+// z-stencils (Bs_x, Bs_y and their velocities along z) roll through a W-plane
+// register window and the cell's own face coefficients are kept for the next
+// plane's k-1 neighbour.  Operands and operation order are emf_cell's, so the
+// FP64 form is bit-identical to it.
+constexpr int ETX = 32, ETY = 8, ET_THREADS = ETX * ETY, ET_SEGMENT = 32;
+
+template <int LIM, typename CTT>
+struct EmfTile {
+  static constexpr int W = emf_width<LIM>(), HL = W / 2;  // stencil i-HL .. i+HL-1
+  static constexpr int XW = ETX + W - 1, YH = ETY + W - 1;
+  static constexpr int NXG = XW * ETY;              // tiles of the x stencils
+  static constexpr int NYG = ETX * YH;              // tiles of the y stencils
+  static constexpr int NB2 = XW * YH;               // Bs_z: both stencils
+  static constexpr int N0 = ETX * (ETY + 1);        // direction-0 coefficients, j-1 row
+  static constexpr int N1 = (ETX + 1) * ETY;        // direction-1 coefficients, i-1 column
+  static constexpr int N2 = (ETX + 1) * (ETY + 1);  // direction-2 coefficients, both
+  // One plane: Bs_y (x tile), Bs_x (y tile), Bs_z as double; then ct[1][1],
+  // ct[2][0] (x tiles), ct[0][0], ct[2][1] (y tiles) and the 4 coefficient
+  // arrays of each direction as CTT.
+  static constexpr int ND = NXG + NYG + NB2;
+  static constexpr int NC = 2 * NXG + 2 * NYG + 4 * (N0 + N1 + N2);
+  static constexpr int PLANE = (ND * 8 + NC * (int)sizeof(CTT) + 15) / 16 * 16;
+  static constexpr int SMEM = 2 * PLANE + (XW + YH) * 4;  // + wrapped column/row offsets
+};
+
+// Resident blocks per SM the tile kernel is compiled for: two FP64 blocks
+// (91 KB of shared memory each), three mixed ones (54 KB).
+template <typename R>
+__host__ __device__ constexpr int emf_tile_minb() { return sizeof(R) == 8 ? 2 : 3; }
+
+__device__ __forceinline__ int wrap_any(int i, int n) {
+  const int r = i % n;
+  return r < 0 ? r + n : r;
+}
+
+__device__ __forceinline__ void cp_async_el(double* s, const double* g) { cp_async8(s, g); }
+__device__ __forceinline__ void cp_async_el(float* s, const float* g) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(g) : "memory");
+}
+
+// Copies a TW x TH tile of NA arrays (array q to s + q * TW * TH, row-major)
+// whose element (lx, ly) is the cell at wrapped column offset xo[lx + OX] and
+// row offset yo[ly + OY] of plane offset zk.
+template <int TW, int TH, int OX, int OY, int NA, typename T>
+__device__ __forceinline__ void stage_tile(T* s, const T* const (&src)[NA], const int* xo,
+                                           const int* yo, int zk, int tid) {
+  for (int e = tid; e < TW * TH; e += ET_THREADS) {
+    const int ly = e / TW, lx = e - ly * TW;
+    const int off = xo[lx + OX] + yo[ly + OY] + zk;
+#pragma unroll
+    for (int q = 0; q < NA; q++) cp_async_el(s + q * (TW * TH) + e, src[q] + off);
+  }
+}
+
+template <int LIM, typename R, typename CTT>
+__device__ __forceinline__ void emf_stage_plane(const StageArgs<CTT>& a, unsigned char* p,
+                                                const int* xo, const int* yo, int zk,
+                                                int tid) {
+  using T = EmfTile<LIM, CTT>;
+  constexpr int HL = T::HL, XW = T::XW, YH = T::YH;
+  double* bsy = reinterpret_cast<double*>(p);
+  double* bsx = bsy + T::NXG;
+  double* bsz = bsx + T::NYG;
+  CTT* qx = reinterpret_cast<CTT*>(bsz + T::NB2);  // ct[1][1], ct[2][0]
+  CTT* qy = qx + 2 * T::NXG;                       // ct[0][0], ct[2][1]
+  CTT* k0 = qy + 2 * T::NYG;
+  CTT* k1 = k0 + 4 * T::N0;
+  CTT* k2 = k1 + 4 * T::N1;
+  {
+    const double* s1[1] = {a.Bs[1]};
+    stage_tile<XW, ETY, 0, HL, 1>(bsy, s1, xo, yo, zk, tid);
+    const double* s0[1] = {a.Bs[0]};
+    stage_tile<ETX, YH, HL, 0, 1>(bsx, s0, xo, yo, zk, tid);
+    const double* s2[1] = {a.Bs[2]};
+    stage_tile<XW, YH, 0, 0, 1>(bsz, s2, xo, yo, zk, tid);
+  }
+  {
+    const CTT* sx[2] = {a.ct[1][1], a.ct[2][0]};
+    stage_tile<XW, ETY, 0, HL, 2>(qx, sx, xo, yo, zk, tid);
+    const CTT* sy[2] = {a.ct[0][0], a.ct[2][1]};
+    stage_tile<ETX, YH, HL, 0, 2>(qy, sy, xo, yo, zk, tid);
+  }
+  {
+    const CTT* c0[4] = {a.ct[0][2], a.ct[0][3], a.ct[0][4], a.ct[0][5]};
+    stage_tile<ETX, ETY + 1, HL, HL - 1, 4>(k0, c0, xo, yo, zk, tid);
+    const CTT* c1[4] = {a.ct[1][2], a.ct[1][3], a.ct[1][4], a.ct[1][5]};
+    stage_tile<ETX + 1, ETY, HL - 1, HL, 4>(k1, c1, xo, yo, zk, tid);
+    const CTT* c2[4] = {a.ct[2][2], a.ct[2][3], a.ct[2][4], a.ct[2][5]};
+    stage_tile<ETX + 1, ETY + 1, HL - 1, HL - 1, 4>(k2, c2, xo, yo, zk, tid);
+  }
+}
+
+template <typename R, typename CTT>
+__device__ __forceinline__ void coef_tile(const CTT* k, int n, int e, R* c) {
+#pragma unroll
+  for (int q = 0; q < 4; q++) c[q] = (R)k[q * n + e];
+}
+
+template <int LIM, typename R, typename CTT>
+__global__ void __launch_bounds__(ET_THREADS, (emf_tile_minb<R>()))
+    emf_tile_kernel(StageArgs<CTT> a, Grid3 g, int sz) {
+  using T = EmfTile<LIM, CTT>;
+  constexpr int W = T::W, HL = T::HL, HR = W - 1 - HL, XW = T::XW, YH = T::YH;
+  extern __shared__ __align__(16) unsigned char emf_smem[];
+  int* xo = reinterpret_cast<int*>(emf_smem + 2 * T::PLANE);
+  int* yo = xo + XW;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int nxy = nx * ny;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * ETX + tx;
+  const int i = blockIdx.x * ETX + tx, j = blockIdx.y * ETY + ty;
+  const bool valid = i < nx && j < ny;
+  const int k0 = blockIdx.z * sz, k1 = min(k0 + sz, nz);
+  for (int l = tid; l < XW; l += ET_THREADS) xo[l] = wrap_any(blockIdx.x * ETX - HL + l, nx);
+  for (int l = tid; l < YH; l += ET_THREADS) yo[l] = nx * wrap_any(blockIdx.y * ETY - HL + l, ny);
+  __syncthreads();
+  emf_stage_plane<LIM, R, CTT>(a, emf_smem, xo, yo, nxy * k0, tid);
+  cp_async_commit();
+
+  const int cxy = i + nx * j;
+  // z window: plane k-HL+m in slot m
+  R zb0[W], zq0[W], zb1[W], zq1[W];
+  R c0m[4], c1m[4];  // face coefficients of directions 0 and 1 at (i, j, k-1)
+  if (valid) {
+#pragma unroll
+    for (int m = 0; m < W - 1; m++) {
+      const int e = cxy + nxy * wrapi(k0 - HL + m, nz);
+      zb0[m] = (R)a.Bs[0][e];
+      zq0[m] = (R)a.ct[0][1][e];
+      zb1[m] = (R)a.Bs[1][e];
+      zq1[m] = (R)a.ct[1][0][e];
+    }
+    const int e = cxy + nxy * wrapi(k0 - 1, nz);
+    coef_load<R>(a, 0, e, c0m);
+    coef_load<R>(a, 1, e, c1m);
+  }
+  // this thread's elements of each tile
+  const int ex = ty * XW + tx;          // x tiles, stencil start (i-HL, j)
+  const int ey = ty * ETX + tx;         // y tiles, stencil start (i, j-HL)
+  const int e0 = ty * ETX + tx;         // direction-0 coefficients at (i, j-1); +ETX: (i, j)
+  const int e1 = ty * (ETX + 1) + tx;   // direction-1 coefficients at (i-1, j); +1: (i, j)
+  const int e2 = ty * (ETX + 1) + tx;   // direction-2: (i, j-1) at e2+1, (i-1, j) at
+                                        // e2+ETX+1, (i, j) at e2+ETX+2
+  for (int k = k0; k < k1; k++) {
+    const int buf = (k - k0) & 1;
+    if (valid) {
+      const int e = cxy + nxy * wrapi(k + HR, nz);
+      zb0[W - 1] = (R)a.Bs[0][e];
+      zq0[W - 1] = (R)a.ct[0][1][e];
+      zb1[W - 1] = (R)a.Bs[1][e];
+      zq1[W - 1] = (R)a.ct[1][0][e];
+    }
+    cp_async_wait0();
+    __syncthreads();  // plane k staged by every thread; plane k-1 read by every thread
+    if (k + 1 < k1)
+      emf_stage_plane<LIM, R, CTT>(a, emf_smem + (buf ^ 1) * T::PLANE, xo, yo, nxy * (k + 1),
+                                   tid);
+    cp_async_commit();
+    if (valid) {
+      unsigned char* p = emf_smem + buf * T::PLANE;
+      const double* bsy = reinterpret_cast<const double*>(p);
+      const double* bsx = bsy + T::NXG;
+      const double* bsz = bsx + T::NYG;
+      const CTT* qx = reinterpret_cast<const CTT*>(bsz + T::NB2);
+      const CTT* qy = qx + 2 * T::NXG;
+      const CTT* kk0 = qy + 2 * T::NYG;
+      const CTT* kk1 = kk0 + 4 * T::N0;
+      const CTT* kk2 = kk1 + 4 * T::N1;
+      R b[W], q[W], f1[4], cc[4], aL, aR, dL, dR, avg, phi, Ez, Ey, Ex;
+      coef_tile(kk0, T::N0, e0 + ETX, cc);
+      {  // Ez, first term: Bs_y along x
+#pragma unroll
+        for (int m = 0; m < W; m++) {
+          b[m] = (R)bsy[ex + m];
+          q[m] = (R)qx[ex + m];
+        }
+        coef_tile(kk0, T::N0, e0, f1);
+        coef_pair(f1, cc, aL, aR, dL, dR);
+        uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+        Ez = avg + phi;
+      }
+      {  // Ey, first term: Bs_z along x
+#pragma unroll
+        for (int m = 0; m < W; m++) {
+          b[m] = (R)bsz[(ty + HL) * XW + tx + m];
+          q[m] = (R)qx[T::NXG + ex + m];
+        }
+        coef_pair(c0m, cc, aL, aR, dL, dR);
+        uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+        Ey = avg - phi;
+      }
+#pragma unroll
+      for (int m = 0; m < 4; m++) c0m[m] = cc[m];
+      coef_tile(kk1, T::N1, e1 + 1, cc);
+      {  // Ez, second term: Bs_x along y
+#pragma unroll
+        for (int m = 0; m < W; m++) {
+          b[m] = (R)bsx[ey + m * ETX];
+          q[m] = (R)qy[ey + m * ETX];
+        }
+        coef_tile(kk1, T::N1, e1, f1);
+        coef_pair(f1, cc, aL, aR, dL, dR);
+        uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+        Ez += avg - phi;
+      }
+      {  // Ex, first term: Bs_z along y
+#pragma unroll
+        for (int m = 0; m < W; m++) {
+          b[m] = (R)bsz[(ty + m) * XW + tx + HL];
+          q[m] = (R)qy[T::NYG + ey + m * ETX];
+        }
+        coef_pair(c1m, cc, aL, aR, dL, dR);
+        uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+        Ex = avg + phi;
+      }
+#pragma unroll
+      for (int m = 0; m < 4; m++) c1m[m] = cc[m];
+      coef_tile(kk2, T::N2, e2 + ETX + 2, cc);
+      {  // Ey, second term: Bs_x along z (window)
+        coef_tile(kk2, T::N2, e2 + ETX + 1, f1);
+        coef_pair(f1, cc, aL, aR, dL, dR);
+        uct_terms<LIM>(zb0, zq0, aL, aR, dL, dR, avg, phi);
+        Ey += avg + phi;
+      }
+      {  // Ex, second term: Bs_y along z (window)
+        coef_tile(kk2, T::N2, e2 + 1, f1);
+        coef_pair(f1, cc, aL, aR, dL, dR);
+        uct_terms<LIM>(zb1, zq1, aL, aR, dL, dR, avg, phi);
+        Ex += avg - phi;
+      }
+      const int c = cxy + nxy * k;
+      a.Ee[2][c] = (CTT)Ez;
+      a.Ee[1][c] = (CTT)Ey;
+      a.Ee[0][c] = (CTT)Ex;
+#pragma unroll
+      for (int m = 0; m < W - 1; m++) {
+        zb0[m] = zb0[m + 1];
+        zq0[m] = zq0[m + 1];
+        zb1[m] = zb1[m + 1];
+        zq1[m] = zq1[m + 1];
+      }
+    }
+  }
+  cp_async_wait0();
+}
+
 // ---------------------------------------------------------------------
 // Stage finish: CT update (Src/MHD/CT/ct_update.cpp:181-423), face RK
 // combine (Src/rk_step.cpp:378-385, 536-552), cell-centred average

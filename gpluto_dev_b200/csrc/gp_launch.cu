@@ -94,7 +94,18 @@ static void run_stage(const StageArgs<CTT>& a, const GridDims& gd, int seg, cuda
   const unsigned nb = (unsigned)((gd.n + 255) / 256);
   if constexpr (PHYS != PHYS_HD) {
     pre();
-    if constexpr (NDIM == 3 && sizeof(RT) == 4 && LIM != LIM_MP5) {  // mixed: z-marching EMF
+    if constexpr (NDIM == 3 && (sizeof(RT) == 8 || LIM == LIM_MP5)) {  // plane-staged EMF
+      using T = EmfTile<LIM, CTT>;
+      cudaFuncSetAttribute(emf_tile_kernel<LIM, RT, CTT>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, T::SMEM);
+      // the longest segment (<= ET_SEGMENT planes) that still gives about
+      // four waves of resident blocks over 148 SMs
+      const long long cols = (long long)((gd.nx + ETX - 1) / ETX) * ((gd.ny + ETY - 1) / ETY);
+      int sz = ET_SEGMENT;
+      while (sz > 4 && cols * ((gd.nz + sz - 1) / sz) < 148LL * emf_tile_minb<RT>() * 4) sz /= 2;
+      dim3 grid((gd.nx + ETX - 1) / ETX, (gd.ny + ETY - 1) / ETY, (gd.nz + sz - 1) / sz);
+      emf_tile_kernel<LIM, RT, CTT><<<grid, dim3(ETX, ETY), T::SMEM, s>>>(a, g, sz);
+    } else if constexpr (NDIM == 3) {  // mixed PLM/PPM: z-marching EMF, loads through L1
       // the longest segment (<= EMF_SEGMENT planes) that still gives about
       // four waves of blocks over 148 SMs (3 blocks per SM)
       const long long cols = (long long)((gd.nx + EMF_TX - 1) / EMF_TX) *
