@@ -14,6 +14,7 @@ from __future__ import annotations
 import ctypes
 import dataclasses
 import os
+import traceback
 
 import numpy as np
 
@@ -25,6 +26,7 @@ LIB_PATH = os.environ.get("GPLUTO_B200_LIB") or os.path.join(_HERE, "_build",
 
 GP_OK, GP_ERR_INVALID, GP_ERR_QUIT, GP_ERR_NO_DEVICE, GP_ERR_IO = 0, -1, -5, -6, -7
 BC_PERIODIC, BC_OUTFLOW, BC_REFLECTIVE, BC_AXISYMMETRIC, BC_EQTSYMMETRIC = 0, 1, 2, 3, 4
+BC_USERDEF = 8
 HD, MHD, RMHD = 0, 1, 2
 # "ppm" and "mp5" select RECONSTRUCTION PARABOLIC and MP5 (the limiter then
 # plays no part)
@@ -95,6 +97,7 @@ def lib():
         L.gp_read_dbl.argtypes = [P, ctypes.c_char_p, ctypes.c_int, D, D,
                                   ctypes.POINTER(ctypes.c_int)]
         L.gp_data_minmax.argtypes = [P, D, D, D]
+        L.gp_set_userdef_boundary.argtypes = [P, UserdefFn, P]
         _lib = L
     return _lib
 
@@ -154,15 +157,70 @@ class StepOut:
     dt_next: float
 
 
+class GpUserdefSide(ctypes.Structure):
+    _fields_ = [("side", ctypes.c_int), ("stage", ctypes.c_int),
+                ("beg", ctypes.c_int * 3), ("end", ctypes.c_int * 3),
+                ("dom_beg", ctypes.c_int * 3), ("nint", ctypes.c_int * 3),
+                ("dims", ctypes.c_int * 3), ("nvar", ctypes.c_int),
+                ("V", ctypes.c_void_p), ("Vs", ctypes.c_void_p * 3)]
+
+
+UserdefFn = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(GpUserdefSide),
+                             ctypes.c_void_p)
+
+
+class _DeviceArray:
+    """A float64 device array described by __cuda_array_interface__."""
+
+    def __init__(self, ptr: int, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8",
+                                         "data": (ptr, False), "version": 3,
+                                         "strides": None, "stream": None}
+
+
+class UserdefSide:
+    """One USERDEF side as the library hands it to the fill: ``side`` (0..5:
+    X1_BEG, X1_END, ... X3_END), ``stage``, the inclusive ghost box
+    ``beg``/``end`` (i, j, k array indices), ``dom_beg`` (first domain cell),
+    ``nint``, the array extents ``dims``, ``nvar``, the device pointers ``V``
+    and ``Vs`` and the ``stream`` the fill's work must go on."""
+
+    def __init__(self, c: GpUserdefSide, stream):
+        self.side, self.stage, self.nvar = c.side, c.stage, c.nvar
+        self.beg, self.end = tuple(c.beg), tuple(c.end)
+        self.dom_beg, self.nint, self.dims = tuple(c.dom_beg), tuple(c.nint), tuple(c.dims)
+        self.V, self.Vs = c.V, [c.Vs[e] for e in range(3)]
+        self.stream = stream or 0
+
+    def tensors(self):
+        """torch views (no copy) of V as [nvar, nz, ny, nx] and of each face
+        field as [nz, ny, nx] (None where absent)."""
+        import torch
+        nx, ny, nz = self.dims
+        V = torch.as_tensor(_DeviceArray(self.V, (self.nvar, nz, ny, nx)), device="cuda")
+        Vs = [torch.as_tensor(_DeviceArray(p, (nz, ny, nx)), device="cuda") if p else None
+              for p in self.Vs]
+        return V, Vs
+
+    def torch_stream(self):
+        """A torch stream context for ``self.stream``."""
+        import torch
+        st = (torch.cuda.ExternalStream(self.stream) if self.stream
+              else torch.cuda.default_stream())
+        return torch.cuda.stream(st)
+
+
 class Solver:
     """Device-resident state of one grid and its Godunov step."""
 
     def __init__(self, ndim: int, shape, scheme: Scheme, xbeg=(0.0, 0.0, 0.0),
                  xend=(1.0, 1.0, 1.0), nghost: int = 2, stream=None, outflow: int = 0,
-                 reflect: int = 0, eqtsym: int = 0):
+                 reflect: int = 0, eqtsym: int = 0, userdef: int = 0, userdef_fill=None):
         """Side masks: bit 2d (2d+1) of ``outflow`` / ``reflect`` / ``eqtsym``
-        makes the low (high) side of direction d an OUTFLOW / REFLECTIVE /
-        EQTSYMMETRIC boundary; other sides are periodic."""
+        / ``userdef`` makes the low (high) side of direction d an OUTFLOW /
+        REFLECTIVE / EQTSYMMETRIC / USERDEF boundary; other sides are
+        periodic.  USERDEF sides are filled by ``userdef_fill`` (see
+        set_userdef_boundary)."""
         g = GpGridDesc()
         g.ndim = ndim
         nx, ny, nz = (tuple(shape) + (1, 1, 1))[:3]
@@ -179,8 +237,12 @@ class Solver:
                     t = BC_REFLECTIVE
                 elif (eqtsym >> bit) & 1:
                     t = BC_EQTSYMMETRIC
+                elif (userdef >> bit) & 1:
+                    t = BC_USERDEF
                 getattr(g, attr)[d] = t
         self.outflow, self.reflect, self.eqtsym = outflow, reflect, eqtsym
+        self.userdef = userdef
+        self._ud_cb = None
         self.ndim, self.shape = ndim, (nx, ny, nz if ndim == 3 else 1)
         self.scheme = scheme
         self.nvar = 5 if scheme.physics == HD else 8
@@ -190,6 +252,24 @@ class Solver:
         sp = ctypes.c_void_p(stream) if stream is not None else None
         _check(lib().gp_create(ctypes.byref(g), ctypes.byref(self._sdesc), sp, ctypes.byref(h)))
         self._h = h
+        if userdef_fill is not None:
+            self.set_userdef_boundary(userdef_fill)
+
+    def set_userdef_boundary(self, fill):
+        """Register the fill of the USERDEF sides: ``fill(side)`` is called
+        before every RK stage with a :class:`UserdefSide` and enqueues its
+        device work on ``side.stream`` (e.g. torch operations on
+        ``side.tensors()`` inside ``with side.torch_stream():``).  It returns
+        nothing; an exception aborts the step (GPError GP_ERR_INVALID)."""
+        def cb(user, sp, stream):
+            try:
+                fill(UserdefSide(sp.contents, stream))
+                return 0
+            except Exception:
+                traceback.print_exc()
+                return 1
+        self._ud_cb = UserdefFn(cb) if fill is not None else None
+        _check(lib().gp_set_userdef_boundary(self._h, self._ud_cb or UserdefFn(), None))
 
     # -- construction helpers -------------------------------------------
     @classmethod

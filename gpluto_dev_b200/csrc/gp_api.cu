@@ -296,6 +296,21 @@ __global__ void ghost_average_kernel(double* __restrict__ V, double* B0, double*
   ghost_average(s, V, B, ndim, (int)(t % s.P[s.a]), (int)(t / s.P[s.a]), beg);
 }
 
+// The extra high-side padding cell of a user-filled side (not a reference
+// ghost): finite copies of the last ghost, as for a mirrored side.
+__global__ void extra_cell_kernel(double* __restrict__ V, int nvar, double* B0, double* B1,
+                                  double* B2, int nb, Pad p, int d) {
+  const SideGeom s = side_geom(p, d);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)s.P[s.a] * s.P[s.b]) return;
+  const int ta = (int)(t % s.P[s.a]), tb = (int)(t / s.P[s.a]);
+  double* B[3] = {B0, B1, B2};
+  const long long c = s.idx(s.P[d] - 1, ta, tb), cl = s.idx(s.P[d] - 2, ta, tb);
+  for (int nv = 0; nv < nvar; nv++) V[nv * s.pn + c] = V[nv * s.pn + cl];
+  for (int e = 0; e < nb; e++)
+    if (e != d) B[e][c] = B[e][cl];
+}
+
 bool uniform(const double* dx, int n) {
   if (!dx) return true;
   for (int i = 1; i < n; i++)
@@ -334,6 +349,9 @@ struct gp_handle {
   unsigned outflow;      // outflow sides (bit 2d low, 2d+1 high)
   unsigned reflect;      // reflective (or axisymmetric) sides, same bits
   unsigned eqtsym;       // equatorially symmetric sides, same bits
+  unsigned userdef;      // user-filled sides, same bits
+  gp_userdef_fn ud_fn;   // the user's fill and its argument
+  void* ud_user;
   // Outflow with constrained transport pads the outflow directions with
   // ghost cells filled before every stage (S = ghost cells of the scheme,
   // plus one on the high side so that the outermost ghost's faces exist).
@@ -385,17 +403,50 @@ gp::GridDims grid_dims(const gp_handle* h) {
 
 // ghost zones of the non-periodic sides of a padded grid, sides in the
 // reference's order (Src/boundary.cpp:144-310)
-void fill_boundaries(gp_handle* h, double* const* Bs) {
+int fill_boundaries(gp_handle* h, double* const* Bs, int stage) {
   const Pad p = pad_of(h);
   const int P[3] = {h->px, h->py, h->pz};
   const int nb = h->scheme.physics == GP_HD ? 0 : h->ndim;  // staggered components
   for (int side = 0; side < 2 * h->ndim; side++) {
     const unsigned bit = 1u << side;
-    if (!((h->outflow | h->reflect | h->eqtsym) & bit)) continue;
+    if (!((h->outflow | h->reflect | h->eqtsym | h->userdef) & bit)) continue;
     const int d = side / 2, beg = side % 2 == 0;
     const int a = (d == 0) ? 1 : 0, b = (d == 2) ? 1 : 2;
     const long long nt = (long long)P[a] * P[b];
     const unsigned nblk = (unsigned)((nt + 127) / 128);
+    if (h->userdef & bit) {
+      // UserDefBoundary, then CT_FillStaggeredFields and the ghost averages
+      // (Src/boundary.cpp:238-307)
+      if (!h->ud_fn)
+        return fail(GP_ERR_INVALID, "USERDEF side %d without a fill (gp_set_userdef_boundary)",
+                    side);
+      gp_userdef_side u;
+      std::memset(&u, 0, sizeof(u));
+      const int n[3] = {h->nx, h->ny, h->nz};
+      u.side = side;
+      u.stage = stage;
+      for (int e = 0; e < 3; e++) {
+        u.beg[e] = 0;
+        u.end[e] = P[e] - 1;
+        u.dom_beg[e] = h->lo[e];
+        u.nint[e] = n[e];
+        u.dims[e] = P[e];
+      }
+      u.beg[d] = beg ? 0 : h->lo[d] + n[d];
+      u.end[d] = beg ? h->lo[d] - 1 : h->lo[d] + n[d] + h->lo[d] - 1;
+      u.nvar = h->nvar;
+      u.V = h->V;
+      for (int e = 0; e < nb; e++) u.Vs[e] = Bs[e];
+      const int rc = h->ud_fn(h->ud_user, &u, (void*)h->stream);
+      if (rc != 0) return fail(GP_ERR_INVALID, "USERDEF fill of side %d returned %d", side, rc);
+      if (!beg)
+        extra_cell_kernel<<<nblk, 128, 0, h->stream>>>(h->V, h->nvar, Bs[0], Bs[1], Bs[2], nb, p,
+                                                       d);
+      if (nb)
+        outflow_march_kernel<<<nblk, 128, 0, h->stream>>>(h->V, Bs[0], Bs[1], Bs[2], h->ndim, p,
+                                                          d, beg, h->A[0], h->A[1], h->A[2]);
+      continue;
+    }
     if (h->outflow & bit) {
       outflow_copy_kernel<<<nblk, 128, 0, h->stream>>>(h->V, h->nvar, Bs[0], Bs[1], Bs[2], nb,
                                                        p, d, beg);
@@ -417,6 +468,7 @@ void fill_boundaries(gp_handle* h, double* const* Bs) {
       ghost_average_kernel<<<nblk, 128, 0, h->stream>>>(h->V, Bs[0], Bs[1], Bs[2], h->ndim, p, d,
                                                         beg);
   }
+  return GP_OK;
 }
 
 int enqueue_step(gp_handle* h, double* hist, int slot, cudaEvent_t* ev = nullptr) {
@@ -445,7 +497,10 @@ int enqueue_step(gp_handle* h, double* hist, int slot, cudaEvent_t* ev = nullptr
                     : gp::launch_stage_fp64(sd, g, h->key, h->seg, h->stream, e);
   };
   // stage 1: (U^n, B^n) -> (U1, B1)
-  if (h->padded) fill_boundaries(h, h->Bs[b0]);
+  if (h->padded) {
+    const int r = fill_boundaries(h, h->Bs[b0], 1);
+    if (r) return r;
+  }
   d.stage = 1;
   d.V = h->V;
   d.Vout = h->V;
@@ -463,7 +518,10 @@ int enqueue_step(gp_handle* h, double* hist, int slot, cudaEvent_t* ev = nullptr
     // (U^n, U2, B^n, B2) -> (U^{n+1} in place of U^n, B^{n+1} in B1's buffer).
     // The finish reads only its own cell's U and its neighbours' input faces,
     // so cells update in place and faces rotate (Src/rk_step.cpp:30-61)
-    if (h->padded) fill_boundaries(h, h->Bs[b1]);
+    if (h->padded) {
+      const int r = fill_boundaries(h, h->Bs[b1], 2);
+      if (r) return r;
+    }
     d.stage = 2;
     d.w0 = 0.75;
     d.w1 = 0.25;
@@ -476,7 +534,10 @@ int enqueue_step(gp_handle* h, double* hist, int slot, cudaEvent_t* ev = nullptr
       d.Bsout[q] = mhd ? h->Bs[b2][q] : nullptr;
     }
     if (launch(d) != 0) return fail(GP_ERR_UNSUPPORTED, "scheme not compiled");
-    if (h->padded) fill_boundaries(h, h->Bs[b2]);
+    if (h->padded) {
+      const int r = fill_boundaries(h, h->Bs[b2], 3);
+      if (r) return r;
+    }
     d.stage = 3;
     d.w0 = 1.0 / 3.0;
     d.w1 = 2.0 / 3.0;
@@ -491,7 +552,10 @@ int enqueue_step(gp_handle* h, double* hist, int slot, cudaEvent_t* ev = nullptr
     if (launch(d) != 0) return fail(GP_ERR_UNSUPPORTED, "scheme not compiled");
   } else {
     // stage 2: (U^n, U1, B^n, B1) -> (U^{n+1} in place of U^n, B^{n+1})
-    if (h->padded) fill_boundaries(h, h->Bs[b1]);
+    if (h->padded) {
+      const int r = fill_boundaries(h, h->Bs[b1], 2);
+      if (r) return r;
+    }
     d.stage = 2;
     d.w0 = d.w1 = d.wr = 0.5;
     d.Uc = h->U[1];
@@ -563,11 +627,13 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
     if (d < grid->ndim) {
       if (grid->nint[d] < 2) return fail(GP_ERR_INVALID, "nint[%d] < 2", d);
       const int lb = grid->lbound[d], rb = grid->rbound[d];
-      if (lb < GP_BC_PERIODIC || lb > GP_BC_EQTSYMMETRIC || rb < GP_BC_PERIODIC ||
-          rb > GP_BC_EQTSYMMETRIC)
+      auto known = [](int t) {
+        return (t >= GP_BC_PERIODIC && t <= GP_BC_EQTSYMMETRIC) || t == GP_BC_USERDEF;
+      };
+      if (!known(lb) || !known(rb))
         return fail(GP_ERR_UNSUPPORTED,
-                    "boundary types are periodic, outflow, reflective, axisymmetric or "
-                    "eqtsymmetric");
+                    "boundary types are periodic, outflow, reflective, axisymmetric, "
+                    "eqtsymmetric or userdef");
       if ((lb == GP_BC_PERIODIC) != (rb == GP_BC_PERIODIC))
         return fail(GP_ERR_INVALID, "a periodic direction needs both sides periodic");
 
@@ -610,14 +676,16 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
       // geometry (FlipSign, Src/boundary.cpp:838-920)
       if (t[e] == GP_BC_REFLECTIVE || t[e] == GP_BC_AXISYMMETRIC) h->reflect |= bit;
       if (t[e] == GP_BC_EQTSYMMETRIC) h->eqtsym |= bit;
+      if (t[e] == GP_BC_USERDEF) h->userdef |= bit;
     }
   }
   // Non-periodic directions are padded with stored ghost cells filled before
   // every stage: with constrained transport (the staggered field's ghost
   // faces), and for mirrored sides of every physics.  HD outflow alone keeps
   // the clamped ghost index of the sweeps.
-  const unsigned nonper = h->outflow | h->reflect | h->eqtsym;
-  h->padded = (h->reflect | h->eqtsym) != 0 || (h->outflow != 0 && scheme->physics != GP_HD);
+  const unsigned nonper = h->outflow | h->reflect | h->eqtsym | h->userdef;
+  h->padded = (h->reflect | h->eqtsym | h->userdef) != 0 ||
+              (h->outflow != 0 && scheme->physics != GP_HD);
   {
     // ghost depth of the scheme (Src/get_nghost.cpp:33-44)
     const int S = scheme->reconstruction == GP_REC_LINEAR ? 2 : 3;
@@ -707,7 +775,11 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   {
     int fills = 0;
     for (int side = 0; side < 2 * h->ndim; side++)
-      if (h->padded && ((nonper >> side) & 1u)) fills += scheme->physics == GP_HD ? 1 : 2;
+      if (!h->padded || !((nonper >> side) & 1u)) continue;
+      else if ((h->userdef >> side) & 1u)  // the extra-cell copy (high side), the march
+        fills += (side & 1) + (scheme->physics == GP_HD ? 0 : 1);
+      else
+        fills += scheme->physics == GP_HD ? 1 : 2;
     h->launches_per_step = scheme->rk_stages * (gp::stage_launch_count(h->key) + fills) + 1;
   }
   if (h->padded) {  // padding cells start finite
@@ -863,7 +935,8 @@ int gp_download_state(gp_handle* h, int layout, double* Uc, double* Vc, double* 
   if (!h) return fail(GP_ERR_INVALID, "null handle");
   int rc;
   // ghost zones of the current state, as Boundary() would fill them
-  if (h->padded && layout == GP_LAYOUT_REFERENCE) fill_boundaries(h, h->Bs[h->bcur]);
+  if (h->padded && layout == GP_LAYOUT_REFERENCE && (rc = fill_boundaries(h, h->Bs[h->bcur], 0)))
+    return rc;
   if (Uc && (rc = download_one(h, layout, h->U[0], Uc, h->nvar, -1, true))) return rc;
   if (Vc && (rc = download_one(h, layout, h->V, Vc, h->nvar, -1))) return rc;
   if (h->scheme.physics != GP_HD) {
@@ -939,6 +1012,13 @@ int gp_device_state(gp_handle* h, double** Uc, double** Vc, double** Vs) {
 }
 
 int gp_launches_per_step(const gp_handle* h) { return h ? h->launches_per_step : 0; }
+
+int gp_set_userdef_boundary(gp_handle* h, gp_userdef_fn fn, void* user) {
+  if (!h) return fail(GP_ERR_INVALID, "null handle");
+  h->ud_fn = fn;
+  h->ud_user = user;
+  return GP_OK;
+}
 
 int gp_profile_steps(gp_handle* h, int nsteps, double* dt, float* kernel_ms, int cap,
                      int* nkernels) {

@@ -56,10 +56,14 @@ enum { GP_LIM_FLAT = 0, GP_LIM_MINMOD = 1, GP_LIM_VANLEER = 2, GP_LIM_MC = 3 };
 enum { GP_RS_HLL = 0, GP_RS_HLLC = 1, GP_RS_HLLD = 2 };
 /* CT_EMF_AVERAGE (Src/MHD/CT/ct.hpp:19-27) */
 enum { GP_CT_UCT_HLL = 0, GP_CT_UCT_HLLD = 1 };
-/* [Boundary] types (Src/boundary.cpp): periodic, or outflow (zero-gradient
-   ghost copy, OutflowBoundary Src/boundary.cpp:677-780; built for HD) */
+/* [Boundary] types (Src/boundary.cpp:144-310; the reference's values,
+   Src/gpluto.hpp:205-212, except periodic): outflow (zero-gradient ghost
+   copy, OutflowBoundary Src/boundary.cpp:677-780), reflective,
+   axisymmetric and eqtsymmetric (ReflectiveBoundary with the signs of
+   FlipSign, 838-1060), userdef (the caller's fill, see
+   gp_set_userdef_boundary) */
 enum { GP_BC_PERIODIC = 0, GP_BC_OUTFLOW = 1, GP_BC_REFLECTIVE = 2, GP_BC_AXISYMMETRIC = 3,
-       GP_BC_EQTSYMMETRIC = 4 };
+       GP_BC_EQTSYMMETRIC = 4, GP_BC_USERDEF = 8 };
 /* RECONSTRUCTION (definitions.hpp): LINEAR (PLM with LIMITER) or PARABOLIC
    (PPM, Src/States/ppm_states.cpp) */
 enum { GP_REC_LINEAR = 0, GP_REC_PARABOLIC = 1, GP_REC_MP5 = 2 };
@@ -136,6 +140,42 @@ double gp_next_time_step(double invDt_hyp, double cfl, double cfl_max_var, doubl
 /* Device pointers of the current state (interior layout), for callers that
    keep data on the GPU.  Valid until the next step. */
 int gp_device_state(gp_handle *h, double **Uc, double **Vc, double **Vs);
+
+/* ---- user-defined boundaries -------------------------------------------
+   A USERDEF side is filled by the caller, as UserDefBoundary(data, box, side,
+   grid) fills it in the reference (Src/boundary.cpp:238-256): before every
+   RK stage, in the reference's side order among the other sides, the
+   library calls `fn` on the host with the side's ghost box; `fn` enqueues on
+   `stream` (a cudaStream_t) the device work that sets, in that box, every
+   primitive variable of V and, with a staggered field, the tangential face
+   fields Vs[e] (e != the side's direction; their box is one face wider
+   along e, which here means the whole array extent).  The library then
+   sets the normal face field of the ghost zone from div B = 0
+   (CT_FillStaggeredFields, Src/MHD/CT/ct_fill_mag_field.cpp:39) and the
+   ghost cells' B from their faces (Src/boundary.cpp:285-307), as for an
+   outflow side.  Arrays are the library's padded layout: a direction with
+   a non-periodic side stores dom_beg[d] ghost cells below the domain and
+   dom_beg[d] + 1 above it (the last one has no counterpart in the
+   reference: the library fills it); periodic directions store no ghosts.
+   `fn` returns 0, or a nonzero value that makes the step return
+   GP_ERR_INVALID.  It is called while the step is being enqueued: work it
+   enqueues on `stream` runs in order with the step's kernels. */
+typedef struct gp_userdef_side {
+  int side;            /* 0..5: X1_BEG, X1_END, X2_BEG, X2_END, X3_BEG, X3_END */
+  int stage;           /* the RK stage the boundary is set for: 1, 2 (3 with RK3); 0
+                          when gp_download_state fills the reference layout's ghosts */
+  int beg[3], end[3];  /* the ghost box (inclusive array indices, i j k) */
+  int dom_beg[3];      /* array index of the first domain cell per direction */
+  int nint[3];         /* domain cells per direction */
+  int dims[3];         /* array extents: cell (i,j,k) is i + dims[0]*(j + dims[1]*k) */
+  int nvar;            /* variables of V */
+  double *V;           /* device: primitives, [nvar][dims[0]*dims[1]*dims[2]] */
+  double *Vs[3];       /* device: left-face fields (NULL for HD and inactive directions) */
+} gp_userdef_side;
+typedef int (*gp_userdef_fn)(void *user, const gp_userdef_side *side, void *stream);
+/* Registers the fill of the handle's USERDEF sides (fn NULL: none; a step
+   with USERDEF sides and no fill returns GP_ERR_INVALID). */
+int gp_set_userdef_boundary(gp_handle *h, gp_userdef_fn fn, void *user);
 
 /* Kernel launches issued per RK step (for launch accounting). */
 int gp_launches_per_step(const gp_handle *h);

@@ -771,6 +771,41 @@ static void Boundary(orc_t *o) {
       }
       continue;
     }
+    if ((o->c.userdef >> side) & 1) {
+      /* USERDEF (Src/boundary.cpp:238-256): UserDefBoundary fills the ghost
+         cells and the tangential staggered fields -- here the inflow rule of
+         the parity cases: the domain cell next to the side, then density
+         ud_rho and normal velocity ud_vn into the domain; tangential faces
+         copied one face wider -- then CT_FillStaggeredFields and the ghost
+         cell-centred B, as for an outflow side. */
+      int i0 = beg ? o->beg[d] : o->end[d];
+      for (k = lo[2]; k <= hi[2]; k++)
+      for (j = lo[1]; j <= hi[1]; j++)
+      for (i = lo[0]; i <= hi[0]; i++) {
+        int s[3] = {i, j, k}; s[d] = i0;
+        for (nv = 0; nv < o->nvar; nv++)
+          *VC(o, o->Vc, nv, i, j, k) = *VC(o, o->Vc, nv, s[0], s[1], s[2]);
+        *VC(o, o->Vc, RHO, i, j, k) = o->c.ud_rho;
+        *VC(o, o->Vc, VX1 + d, i, j, k) = beg ? o->c.ud_vn : -o->c.ud_vn;
+      }
+      if (isMHD) {
+        int c;
+        for (c = 0; c < o->c.ndim; c++) {
+          if (c == d) continue;
+          int h[3] = {hi[0], hi[1], hi[2]};
+          h[c] += 1;
+          for (k = lo[2]; k <= h[2]; k++)
+          for (j = lo[1]; j <= h[1]; j++)
+          for (i = lo[0]; i <= h[0]; i++) {
+            int s[3] = {i, j, k}; s[d] = i0;
+            o->Vs[c][SI(o,c,i,j,k)] = o->Vs[c][SI(o,c,s[0],s[1],s[2])];
+          }
+        }
+        CT_FillNormal(o, d, beg);
+        AverageStaggered(o, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], 1);
+      }
+      continue;
+    }
     if (((o->c.reflect | o->c.eqtsym) >> side) & 1) {
       /* ReflectiveBoundary with the signs of FlipSign
          (Src/boundary.cpp:203-216, 838-900, 931-1060): ghost cell m copies

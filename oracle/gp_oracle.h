@@ -24,6 +24,8 @@ typedef struct {
   int reflect;   /* same bits: REFLECTIVE (or AXISYMMETRIC, identical in Cartesian) */
   int eqtsym;    /* same bits: EQTSYMMETRIC */
   int rk;        /* TIME_STEPPING: 2 (RK2, also for 0) or 3 (RK3) */
+  int userdef;   /* same bits: USERDEF, filled by the inflow rule of the parity cases */
+  double ud_rho, ud_vn;  /* the inflow's density and normal speed into the domain */
 } orc_cfg;
 
 void    *orc_create(const orc_cfg *cfg);

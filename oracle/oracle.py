@@ -27,7 +27,12 @@ class OrcCfg(ctypes.Structure):
                 ("gamma", ctypes.c_double), ("dx", ctypes.c_double * 3),
                 ("cfl", ctypes.c_double), ("cfl_max_var", ctypes.c_double),
                 ("outflow", ctypes.c_int), ("reflect", ctypes.c_int),
-                ("eqtsym", ctypes.c_int), ("rk", ctypes.c_int)]
+                ("eqtsym", ctypes.c_int), ("rk", ctypes.c_int),
+                ("userdef", ctypes.c_int), ("ud_rho", ctypes.c_double),
+                ("ud_vn", ctypes.c_double)]
+
+# The inflow of the USERDEF parity cases (oracle/ref/init.cpp UserDefBoundary)
+UD_RHO, UD_VN = 1.25, 0.25
 
 
 def build() -> str:
@@ -91,7 +96,8 @@ class Oracle:
     """One grid advanced by the CPU restatement."""
 
     def __init__(self, state, limiter="mc", solver="hlld", ct="uct_hlld",
-                 cfl=0.4, cfl_max_var=1.1, outflow=0, reflect=0, eqtsym=0, rk=2):
+                 cfl=0.4, cfl_max_var=1.1, outflow=0, reflect=0, eqtsym=0, rk=2,
+                 userdef=0):
         nx, ny, nz = state.shape
         c = OrcCfg()
         c.physics, c.ndim = state.physics, state.ndim
@@ -103,6 +109,7 @@ class Oracle:
         c.cfl, c.cfl_max_var = cfl, cfl_max_var
         c.outflow, c.reflect, c.eqtsym = outflow, reflect, eqtsym
         c.rk = rk
+        c.userdef, c.ud_rho, c.ud_vn = userdef, UD_RHO, UD_VN
         self.cfg = c
         self.shape = (nx, ny, nz)
         self.physics, self.ndim, self.nvar = state.physics, state.ndim, state.nvar

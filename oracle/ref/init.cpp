@@ -176,6 +176,43 @@ void Analysis (Data *data, Grid *grid)
 }
 
 ////////////////////////////////////////////////////////////////////////
+// USERDEF sides of the parity cases: an inflow.  Every ghost cell of the
+// side takes the primitive state of the domain cell next to the side, then
+// the fixed density kUdRho and the normal velocity kUdVn pointing into the
+// domain; the tangential staggered fields copy the domain face next to the
+// side (one face wider along their own direction).  The normal staggered
+// field and the ghost cell-centred B are left to the framework
+// (CT_FillStaggeredFields and the averages, Src/boundary.cpp:238-307).
+static const double kUdRho = 1.25, kUdVn = 0.25;
+
 void UserDefBoundary (const Data *data, RBox *box, int side, Grid *grid)
 {
+  if (side < X1_BEG || side > X3_END) return;
+  const int d = (side - X1_BEG)/2, beg = ((side - X1_BEG)%2 == 0);
+  const int m0 = beg ? grid->lbeg[d] : grid->lend[d];
+  const int lo[3] = {box->ibeg, box->jbeg, box->kbeg};
+  const int hi[3] = {box->iend, box->jend, box->kend};
+  for (int k = lo[2]; k <= hi[2]; k++){
+  for (int j = lo[1]; j <= hi[1]; j++){
+  for (int i = lo[0]; i <= hi[0]; i++){
+    int s[3] = {i, j, k};
+    s[d] = m0;
+    for (int nv = 0; nv < NVAR; nv++) data->Vc(i,j,k,nv) = data->Vc(s[0],s[1],s[2],nv);
+    data->Vc(i,j,k,RHO) = kUdRho;
+    data->Vc(i,j,k,VX1+d) = beg ? kUdVn : -kUdVn;
+  }}}
+  #ifdef STAGGERED_MHD
+  for (int c = 0; c < DIMENSIONS; c++){
+    if (c == d) continue;
+    int h[3] = {hi[0], hi[1], hi[2]};
+    h[c] += 1;
+    for (int k = lo[2]; k <= h[2]; k++){
+    for (int j = lo[1]; j <= h[1]; j++){
+    for (int i = lo[0]; i <= h[0]; i++){
+      int s[3] = {i, j, k};
+      s[d] = m0;
+      data->Vs[c](i,j,k) = data->Vs[c](s[0],s[1],s[2]);
+    }}}
+  }
+  #endif
 }

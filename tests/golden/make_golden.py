@@ -189,6 +189,31 @@ CASES = {
                                dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
                                     ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
                                     reconstruction="MP5"), 6),
+    # USERDEF sides: the inflow rule of oracle/ref/init.cpp UserDefBoundary,
+    # then the framework's div B = 0 normal faces and ghost averages
+    "mhd2d_mc_hlld_ucthlld_userdefx": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=111),
+                                       dict(physics="MHD", ndim=2, limiter="MC_LIM",
+                                            solver="hlld", ct_emf="UCT_HLLD", cfl=0.4,
+                                            first_dt=1e-4,
+                                            bc=("userdef", "periodic", "periodic")), 12),
+    "mhd2d_ppm_hlld_ucthlld_userdefx_outflowy": (
+        ics.mhd2d_turbulence, dict(n=(22, 18), seed=112),
+        dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld", ct_emf="UCT_HLLD", cfl=0.4,
+             first_dt=1e-4, reconstruction="PARABOLIC", bc=("userdef", "outflow", "periodic")), 10),
+    "mhd2d_mp5_hll_ucthll_userdefy_rk3": (
+        ics.mhd2d_turbulence, dict(n=(20, 24), seed=113),
+        dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hll", ct_emf="UCT_HLL", cfl=0.4,
+             first_dt=1e-4, reconstruction="MP5", rk="RK3",
+             bc=("periodic", "userdef", "periodic")), 10),
+    "hd2d_mc_hllc_userdefy": (ics.hd_turbulence, dict(n=(20, 22), seed=114),
+                              dict(physics="HD", ndim=2, limiter="MC_LIM", solver="hllc",
+                                   cfl=0.4, first_dt=1e-4,
+                                   bc=("reflective", "userdef", "periodic")), 12),
+    "mhd3d_mc_hlld_ucthlld_userdefz": (ics.mhd3d_turbulence, dict(n=(12, 10, 14), seed=115),
+                                       dict(physics="MHD", ndim=3, limiter="MC_LIM",
+                                            solver="hlld", ct_emf="UCT_HLLD", cfl=0.4,
+                                            first_dt=1e-4,
+                                            bc=("outflow", "periodic", "userdef")), 8),
 }
 
 
@@ -293,7 +318,8 @@ def make(name: str) -> str:
         cfl=rc["cfl"], cfl_max_var=1.1, first_dt=rc["first_dt"],
         reconstruction=rc.get("reconstruction", "LINEAR"), outflow=outflow_mask(rc),
         reflect=side_mask(rc, ("reflective", "axisymmetric")),
-        eqtsym=side_mask(rc, ("eqtsymmetric",)), rk=3 if rc.get("rk") == "RK3" else 2)
+        eqtsym=side_mask(rc, ("eqtsymmetric",)), userdef=side_mask(rc, ("userdef",)),
+        rk=3 if rc.get("rk") == "RK3" else 2)
     return out
 
 

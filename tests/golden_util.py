@@ -43,8 +43,11 @@ class Golden:
         self.outflow = int(z["outflow"]) if "outflow" in z else 0
         self.reflect = int(z["reflect"]) if "reflect" in z else 0
         self.eqtsym = int(z["eqtsym"]) if "eqtsym" in z else 0
+        self.userdef = int(z["userdef"]) if "userdef" in z else 0
         # side types as keyword arguments of the oracle and of api.Solver
         self.bc = dict(outflow=self.outflow, reflect=self.reflect, eqtsym=self.eqtsym)
+        if self.userdef:
+            self.bc["userdef"] = self.userdef
         self.rk = int(z["rk"]) if "rk" in z else 2
         if self.reconstruction == "PARABOLIC":
             self.limiter = "ppm"

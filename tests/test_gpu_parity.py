@@ -10,6 +10,7 @@ import pytest
 
 import golden_util as gu
 import oracle as orc
+import userdef_util as ud
 from gpluto_dev_b200 import api, ics
 
 pytestmark = pytest.mark.gpu
@@ -22,11 +23,14 @@ def rel_linf(a, b):
 
 
 def make_solver(st, limiter, solver, ct, cfl=0.4, cfl_max_var=1.1, precision=api.FP64,
-                outflow=0, reflect=0, eqtsym=0, rk=2):
+                outflow=0, reflect=0, eqtsym=0, rk=2, userdef=0):
+    """USERDEF sides get the inflow fill of the parity cases."""
     sch = api.Scheme(physics=st.physics, limiter=limiter, riemann=solver, ct_emf=ct,
                      precision=precision, gamma=st.gamma, cfl=cfl, cfl_max_var=cfl_max_var,
                      rk=rk)
-    return api.Solver.from_state(st, sch, outflow=outflow, reflect=reflect, eqtsym=eqtsym)
+    return api.Solver.from_state(st, sch, outflow=outflow, reflect=reflect, eqtsym=eqtsym,
+                                 userdef=userdef,
+                                 userdef_fill=ud.inflow_fill if userdef else None)
 
 
 @pytest.mark.parametrize("name", [n for n in gu.names() if not n.startswith("rmhd")])
@@ -154,6 +158,16 @@ MIRROR_CASES = [
      dict(reflect=0b110000, outflow=0b000011), 8),
     (ics.hd_turbulence, dict(n=(31, 17), seed=86), "mc", "hll", "uct_hll",
      dict(reflect=0b1111), 12),
+    # USERDEF sides (the inflow fill): alone, with mirrored and outflow sides,
+    # every side of a grid, MP5 and PPM widths
+    (ics.mhd3d_turbulence, dict(n=(11, 10, 9), seed=87), "mc", "hlld", "uct_hlld",
+     dict(userdef=0b110011), 6),
+    (ics.mhd3d_blast, dict(n=(12, 10, 9), seed=88, radius=0.25), "mp5", "hll", "uct_hll",
+     dict(userdef=0b001100, reflect=0b000011), 5),
+    (ics.hd_turbulence, dict(n=(21, 17), seed=89), "ppm", "hllc", "uct_hll",
+     dict(outflow=0b0001, userdef=0b0010, reflect=0b1100), 10),
+    (ics.mhd2d_turbulence, dict(n=(25, 19), seed=90), "vl", "hlld", "uct_hlld",
+     dict(userdef=0b1111), 10),
 ]
 
 
@@ -161,7 +175,9 @@ MIRROR_CASES = [
 def test_gpu_mirrored_sides_match_oracle_bitwise(case):
     """Reflective / eqtsymmetric sides (mixed with outflow and periodic ones):
     padded ghost zones filled before every stage by mirror copies with the
-    reference's signs, then the ghost cells' B averaged from their faces."""
+    reference's signs, then the ghost cells' B averaged from their faces.
+    USERDEF sides: the caller's fill, then the div B = 0 normal faces and the
+    ghost averages."""
     gen, kw, lim, rs, ct, bc, nsteps = MIRROR_CASES[case]
     st = gen(**kw)
     kwo = dict(limiter=lim, solver=rs, **bc)
@@ -426,3 +442,38 @@ def test_grids_beyond_the_cell_limit_are_refused_before_allocating():
     with pytest.raises(api.GPError) as ei:          # PPM below 4 cells
         api.Solver(2, (3, 8), api.Scheme(physics=api.MHD, limiter="ppm"))
     assert ei.value.code == api.GP_ERR_INVALID
+
+
+def test_gpu_userdef_side_needs_a_fill():
+    st = ics.mhd2d_turbulence(n=(16, 12), seed=91)
+    sch = api.Scheme(physics=api.MHD, gamma=st.gamma)
+    s = api.Solver.from_state(st, sch, userdef=0b0011)
+    with pytest.raises(api.GPError) as ei:
+        s.run(1, 1e-4)
+    assert ei.value.code == api.GP_ERR_INVALID
+
+    def bad_fill(side):
+        raise RuntimeError("fill failed")
+
+    s = api.Solver.from_state(st, sch, userdef=0b0011, userdef_fill=bad_fill)
+    with pytest.raises(api.GPError) as ei:
+        s.run(1, 1e-4)
+    assert ei.value.code == api.GP_ERR_INVALID
+
+
+def test_gpu_userdef_fill_sees_the_reference_ghost_box():
+    """The box handed to the fill: the reference's ghost zone along the
+    side's direction, the whole array across it; stages 1 and 2 per step."""
+    st = ics.mhd3d_turbulence(n=(10, 9, 8), seed=92)
+    seen = []
+
+    def fill(side):
+        seen.append((side.side, side.stage, side.beg, side.end, side.dom_beg, side.dims))
+        ud.inflow_fill(side)
+
+    sch = api.Scheme(physics=api.MHD, gamma=st.gamma)
+    s = api.Solver.from_state(st, sch, userdef=0b000010, outflow=0b000001, userdef_fill=fill)
+    s.run(1, 1e-4)
+    dims = (10 + 5, 9, 8)
+    assert seen == [(1, 1, (12, 0, 0), (13, 8, 7), (2, 0, 0), dims),
+                    (1, 2, (12, 0, 0), (13, 8, 7), (2, 0, 0), dims)]
