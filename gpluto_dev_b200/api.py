@@ -30,7 +30,8 @@ BC_USERDEF = 8
 HD, MHD, RMHD = 0, 1, 2
 # "ppm" and "mp5" select RECONSTRUCTION PARABOLIC and MP5 (the limiter then
 # plays no part)
-LIMITERS = {"flat": 0, "minmod": 1, "vl": 2, "vanleer": 2, "mc": 3, "ppm": 3, "mp5": 3}
+LIMITERS = {"flat": 0, "minmod": 1, "vl": 2, "vanleer": 2, "mc": 3, "ppm": 3, "mp5": 3,
+            "vanalbada": 6, "ospre": 7, "umist": 8}
 RECONSTRUCTION = {"ppm": 1, "mp5": 2}
 SOLVERS = {"hll": 0, "hllc": 1, "hlld": 2}
 CT_AVG = {"uct_hll": 0, "uct_hlld": 1}

@@ -649,7 +649,8 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
       scheme->reconstruction != GP_REC_MP5)
     return fail(GP_ERR_UNSUPPORTED, "reconstruction %d not built", scheme->reconstruction);
   if (scheme->reconstruction == GP_REC_LINEAR &&
-      (scheme->limiter < GP_LIM_MINMOD || scheme->limiter > GP_LIM_MC))
+      !((scheme->limiter >= GP_LIM_FLAT && scheme->limiter <= GP_LIM_MC) ||
+        (scheme->limiter >= GP_LIM_VANALBADA && scheme->limiter <= GP_LIM_UMIST)))
     return fail(GP_ERR_UNSUPPORTED, "limiter %d not built", scheme->limiter);
   if (scheme->reconstruction != GP_REC_LINEAR)
     for (int d = 0; d < grid->ndim; d++)

@@ -134,6 +134,12 @@ static int by_lim(const StageArgs<CTT>& a, const GridDims& g, int lim, int seg, 
     case LIM_MINMOD: run_stage<PHYS, NV, NDIM, RS, CT, LIM_MINMOD>(a, g, seg, s, ev); return 0;
     case LIM_PPM: run_stage<PHYS, NV, NDIM, RS, CT, LIM_PPM>(a, g, seg, s, ev); return 0;
     case LIM_MP5: run_stage<PHYS, NV, NDIM, RS, CT, LIM_MP5>(a, g, seg, s, ev); return 0;
+    case LIM_FLAT: run_stage<PHYS, NV, NDIM, RS, CT, LIM_FLAT>(a, g, seg, s, ev); return 0;
+    case LIM_VANALBADA:
+      run_stage<PHYS, NV, NDIM, RS, CT, LIM_VANALBADA>(a, g, seg, s, ev);
+      return 0;
+    case LIM_OSPRE: run_stage<PHYS, NV, NDIM, RS, CT, LIM_OSPRE>(a, g, seg, s, ev); return 0;
+    case LIM_UMIST: run_stage<PHYS, NV, NDIM, RS, CT, LIM_UMIST>(a, g, seg, s, ev); return 0;
     default: return -1;
   }
 }

@@ -76,6 +76,10 @@ extern "C" int gp_advance_step_noalloc(const gp_grid_desc* grid, const gp_scheme
   if (grid->ndim != 2 && grid->ndim != 3) return GP_ERR_UNSUPPORTED;
   if (scheme->rk_stages != 2) return GP_ERR_UNSUPPORTED;
   if (scheme->reconstruction == GP_REC_MP5) return GP_ERR_UNSUPPORTED;
+  if (scheme->reconstruction == GP_REC_LINEAR &&
+      !((scheme->limiter >= GP_LIM_FLAT && scheme->limiter <= GP_LIM_MC) ||
+        (scheme->limiter >= GP_LIM_VANALBADA && scheme->limiter <= GP_LIM_UMIST)))
+    return GP_ERR_UNSUPPORTED;
   if (scheme->physics != GP_HD && scheme->physics != GP_MHD && scheme->physics != GP_RMHD)
     return GP_ERR_UNSUPPORTED;
   if (scheme->precision != GP_FP64 && scheme->precision != GP_MIXED) return GP_ERR_INVALID;

@@ -34,7 +34,8 @@ enum : int { PHYS_HD = 0, PHYS_MHD = 1, PHYS_RMHD = 2 };
 // LIM_PPM and LIM_MP5 select piecewise parabolic and monotonicity-preserving
 // 5th-order reconstruction (RECONSTRUCTION PARABOLIC / MP5); they are
 // carried in the limiter slot of the scheme templates.
-enum : int { LIM_FLAT = 0, LIM_MINMOD = 1, LIM_VL = 2, LIM_MC = 3, LIM_PPM = 4, LIM_MP5 = 5 };
+enum : int { LIM_FLAT = 0, LIM_MINMOD = 1, LIM_VL = 2, LIM_MC = 3, LIM_PPM = 4, LIM_MP5 = 5,
+             LIM_VANALBADA = 6, LIM_OSPRE = 7, LIM_UMIST = 8 };
 enum : int { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2 };
 enum : int { CT_UCT_HLL = 0, CT_UCT_HLLD = 1 };
 
@@ -48,8 +49,9 @@ template <> __device__ __forceinline__ float rabs(float x) { return fabsf(x); }
 #define GP_MIN(a, b) ((a) <= (b) ? (a) : (b))      // Src/macros.hpp:194
 
 // ---------------------------------------------------------------------
-// PLM slope limiters on a uniform Cartesian grid,
-// Src/States/plm_coeffs.hpp:88-100 and Src/macros.hpp:200.
+// PLM slope limiters on a uniform Cartesian grid (SET_*_LIMITER of
+// Src/plm_coeffs.hpp:55-110, ABS_MIN of Src/macros.hpp:14) and
+// Src/macros.hpp:200; FLAT gives a zero slope.
 // ---------------------------------------------------------------------
 template <int LIM, typename R>
 __device__ __forceinline__ R limit(R dvp, R dvm) {
@@ -64,6 +66,24 @@ __device__ __forceinline__ R limit(R dvp, R dvm) {
     return (dvp * dvm > R(0) ? R(2) * dvp * dvm / (dvp + dvm) : R(0));
   } else if constexpr (LIM == LIM_MINMOD) {
     return (dvp * dvm > R(0) ? (rabs(dvp) < rabs(dvm) ? dvp : dvm) : R(0));
+  } else if constexpr (LIM == LIM_VANALBADA) {
+    if (dvp * dvm > R(0)) {
+      R dpp = dvp * dvp, dmm = dvm * dvm;
+      return (dvp * (dmm + R(1.e-18)) + dvm * (dpp + R(1.e-18))) / (dpp + dmm + R(1.e-18));
+    }
+    return R(0);
+  } else if constexpr (LIM == LIM_OSPRE) {
+    return (dvp * dvm > R(0)
+                ? R(1.5) * dvp * dvm * (dvm + dvp) / (dvp * dvp + dvm * dvm + dvp * dvm)
+                : R(0));
+  } else if constexpr (LIM == LIM_UMIST) {
+    if (dvp * dvm > R(0)) {
+      R ddp = R(0.25) * (dvp + R(3) * dvm), ddm = R(0.25) * (dvm + R(3) * dvp);
+      R d2 = R(2) * (rabs(dvp) < rabs(dvm) ? dvp : dvm);
+      d2 = rabs(d2) < rabs(ddp) ? d2 : ddp;
+      return rabs(d2) < rabs(ddm) ? d2 : ddm;
+    }
+    return R(0);
   } else {
     return R(0);
   }

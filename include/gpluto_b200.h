@@ -50,8 +50,10 @@ enum gp_status {
 
 /* PHYSICS (definitions.hpp) */
 enum { GP_HD = 0, GP_MHD = 1, GP_RMHD = 2 };
-/* LIMITER (Src/States/plm_coeffs.hpp) */
-enum { GP_LIM_FLAT = 0, GP_LIM_MINMOD = 1, GP_LIM_VANLEER = 2, GP_LIM_MC = 3 };
+/* LIMITER (Src/gpluto.hpp:329-335, Src/plm_coeffs.hpp:55-110); 4 and 5 are
+   not limiters (they stand for PPM and MP5 inside the library) */
+enum { GP_LIM_FLAT = 0, GP_LIM_MINMOD = 1, GP_LIM_VANLEER = 2, GP_LIM_MC = 3,
+       GP_LIM_VANALBADA = 6, GP_LIM_OSPRE = 7, GP_LIM_UMIST = 8 };
 /* [Solver] in pluto.ini (Src/MHD/set_solver.cpp:35-47) */
 enum { GP_RS_HLL = 0, GP_RS_HLLC = 1, GP_RS_HLLD = 2 };
 /* CT_EMF_AVERAGE (Src/MHD/CT/ct.hpp:19-27) */

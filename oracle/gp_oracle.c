@@ -578,8 +578,8 @@ static double HD_HLL(orc_t *o, int dir, double *vl, double *vr, double *flux) {
 /* reconstruction                                                      */
 /* ------------------------------------------------------------------ */
 
-/* Src/States/plm_coeffs.hpp:88-100 (uniform Cartesian grid) and
-   Src/macros.hpp:200 (minmod) */
+/* SET_*_LIMITER of Src/plm_coeffs.hpp:55-110 (uniform Cartesian grid) and
+   Src/macros.hpp:200 (minmod); FLAT (and any other label) gives 0 */
 static double Limit(int lim, double dvp, double dvm) {
   double dv;
   if (lim == ORC_LIM_MC) {
@@ -591,6 +591,20 @@ static double Limit(int lim, double dvp, double dvm) {
     dv = (dvp*dvm > 0.0 ? 2.0*dvp*dvm/(dvp + dvm) : 0.0);
   } else if (lim == ORC_LIM_MINMOD) {
     dv = (dvp*dvm > 0.0 ? ABS_MIN(dvp, dvm) : 0.0);
+  } else if (lim == ORC_LIM_VANALBADA) {
+    if (dvp*dvm > 0.0) {
+      double dpp = dvp*dvp, dmm = dvm*dvm;
+      dv = (dvp*(dmm + 1.e-18) + dvm*(dpp + 1.e-18))/(dpp + dmm + 1.e-18);
+    } else dv = 0.0;
+  } else if (lim == ORC_LIM_OSPRE) {
+    dv = (dvp*dvm > 0.0 ? 1.5*dvp*dvm*(dvm + dvp)/(dvp*dvp + dvm*dvm + dvp*dvm) : 0.0);
+  } else if (lim == ORC_LIM_UMIST) {
+    if (dvp*dvm > 0.0) {
+      double ddp = 0.25*(dvp + 3.0*dvm), ddm = 0.25*(dvm + 3.0*dvp);
+      double d2 = 2.0*ABS_MIN(dvp, dvm);
+      d2 = ABS_MIN(d2, ddp);
+      dv = ABS_MIN(d2, ddm);
+    } else dv = 0.0;
   } else {
     dv = 0.0;
   }

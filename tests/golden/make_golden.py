@@ -189,6 +189,27 @@ CASES = {
                                dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
                                     ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
                                     reconstruction="MP5"), 6),
+    # the other PLM limiters of Src/plm_coeffs.hpp (uniform-grid forms)
+    "mhd2d_flat_hlld_ucthlld": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=121),
+                                dict(physics="MHD", ndim=2, limiter="FLAT_LIM", solver="hlld",
+                                     ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4), 10),
+    "mhd2d_vanalbada_hlld_ucthlld": (ics.mhd2d_turbulence, dict(n=(22, 26), seed=122),
+                                     dict(physics="MHD", ndim=2, limiter="VANALBADA_LIM",
+                                          solver="hlld", ct_emf="UCT_HLLD", cfl=0.4,
+                                          first_dt=1e-4), 12),
+    "mhd3d_ospre_hlld_ucthll": (ics.mhd3d_turbulence, dict(n=(12, 10, 14), seed=123),
+                                dict(physics="MHD", ndim=3, limiter="OSPRE_LIM", solver="hlld",
+                                     ct_emf="UCT_HLL", cfl=0.4, first_dt=1e-4), 8),
+    "mhd2d_umist_hll_ucthll_outflow": (
+        ics.mhd2d_turbulence, dict(n=(20, 18), seed=124),
+        dict(physics="MHD", ndim=2, limiter="UMIST_LIM", solver="hll", ct_emf="UCT_HLL", cfl=0.4,
+             first_dt=1e-4, bc=("outflow", "periodic", "periodic")), 12),
+    "hd3d_umist_hllc": (ics.hd_turbulence, dict(n=(12, 14, 10), seed=125),
+                        dict(physics="HD", ndim=3, limiter="UMIST_LIM", solver="hllc", cfl=0.4,
+                             first_dt=1e-4), 8),
+    "hd2d_ospre_hll": (ics.hd_turbulence, dict(n=(26, 20), seed=126),
+                       dict(physics="HD", ndim=2, limiter="OSPRE_LIM", solver="hll", cfl=0.4,
+                            first_dt=1e-4), 12),
     # USERDEF sides: the inflow rule of oracle/ref/init.cpp UserDefBoundary,
     # then the framework's div B = 0 normal faces and ghost averages
     "mhd2d_mc_hlld_ucthlld_userdefx": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=111),

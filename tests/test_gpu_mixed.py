@@ -67,13 +67,18 @@ MIXED_SCHEMES = [
      dict(outflow=0b0011, reflect=0b1100), 3, 30),
     (ics.mhd3d_turbulence, dict(n=(40, 36, 32), seed=124), "vl", "hll", "uct_hll",
      dict(eqtsym=0b110000), 3, 15),
+    (ics.mhd2d_turbulence, dict(n=(80, 72), seed=125), "vanalbada", "hlld", "uct_hlld",
+     dict(), 2, 30),
+    (ics.mhd3d_turbulence, dict(n=(36, 32, 28), seed=126), "ospre", "hlld", "uct_hlld",
+     dict(), 2, 12),
 ]
 
 
 @pytest.mark.parametrize("case", range(len(MIXED_SCHEMES)))
 def test_mixed_l1_error_other_schemes(case):
-    """The ≤ 1e-5 relative L1 bound of the mixed form for HD, PPM, RK3 and
-    non-periodic sides, on the FP64 run's dt sequence."""
+    """The ≤ 1e-5 relative L1 bound of the mixed form for HD, PPM, RK3,
+    non-periodic sides and the van Albada and OSPRE limiters, on the FP64
+    run's dt sequence."""
     gen, kw, lim, rs, ct, bc, rk, n = MIXED_SCHEMES[case]
     st = gen(**kw)
 

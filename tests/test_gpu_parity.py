@@ -63,6 +63,11 @@ CASES = [
     (ics.mhd3d_turbulence, dict(n=(20, 18, 16), seed=29), "ppm", "hlld", "uct_hlld", 8),
     (ics.hd_turbulence, dict(n=(65, 5), seed=30), "ppm", "hllc", "uct_hll", 12),
     (ics.mhd2d_turbulence, dict(n=(6, 40), seed=31), "ppm", "hll", "uct_hll", 10),
+    # the other PLM limiters (flat, van Albada, OSPRE, UMIST) on odd sizes
+    (ics.mhd3d_turbulence, dict(n=(13, 11, 9), seed=131), "vanalbada", "hlld", "uct_hlld", 6),
+    (ics.mhd2d_turbulence, dict(n=(35, 19), seed=132), "ospre", "hlld", "uct_hll", 10),
+    (ics.hd_turbulence, dict(n=(33, 7), seed=133), "umist", "hllc", "uct_hll", 12),
+    (ics.mhd2d_turbulence, dict(n=(17, 23), seed=134), "flat", "hll", "uct_hll", 10),
 ]
 
 
