@@ -646,7 +646,7 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   if (scheme->physics == GP_HD && scheme->riemann == GP_RS_HLLD)
     return fail(GP_ERR_UNSUPPORTED, "HD has no HLLD solver");
   if (scheme->reconstruction != GP_REC_LINEAR && scheme->reconstruction != GP_REC_PARABOLIC &&
-      scheme->reconstruction != GP_REC_MP5)
+      scheme->reconstruction != GP_REC_MP5 && scheme->reconstruction != GP_REC_WENOZ)
     return fail(GP_ERR_UNSUPPORTED, "reconstruction %d not built", scheme->reconstruction);
   if (scheme->reconstruction == GP_REC_LINEAR &&
       !((scheme->limiter >= GP_LIM_FLAT && scheme->limiter <= GP_LIM_MC) ||
@@ -730,6 +730,7 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   h->key = gp::SchemeKey{scheme->physics, grid->ndim, scheme->riemann, scheme->ct_emf,
                          scheme->reconstruction == GP_REC_PARABOLIC ? 4   /* LIM_PPM */
                          : scheme->reconstruction == GP_REC_MP5     ? 5   /* LIM_MP5 */
+                         : scheme->reconstruction == GP_REC_WENOZ   ? 9   /* LIM_WENOZ */
                                                                     : scheme->limiter};
   // pencil segment for the marching sweeps: enough threads to fill 148 SMs
   {

@@ -220,7 +220,7 @@ __device__ __forceinline__ void store_ct(const StageArgs<CTT>& a, int dir, long 
 template <int NV, int LIM = LIM_MC>
 constexpr int sweep_x_stage_doubles() {
   return 2 * (2 * NV + 1) * SWEEP_THREADS +
-         ((LIM == LIM_PPM || LIM == LIM_MP5) ? 2 * (SWEEP_THREADS / 32) * NV : 0);
+         ((LIM == LIM_PPM || five_point<LIM>()) ? 2 * (SWEEP_THREADS / 32) * NV : 0);
 }
 template <int NV>
 constexpr int sweep_m_stage_doubles() { return 2 * (NV + 1) * SWEEP_THREADS; }
@@ -406,7 +406,7 @@ __device__ __forceinline__ void mp5_fallback(const R* w0, const R* qm, const R* 
   if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(w0, vR, vLn);
 }
 
-template <int PHYS, int NV, int NDIM, int RS, int CT, typename R, typename CTT>
+template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, typename R, typename CTT>
 __device__ __forceinline__ void sweep_x_row_mp5(const StageArgs<CTT>& a, const Grid3& g, int row,
                                                 double* stg_, int tid) {
   constexpr unsigned FULL = 0xffffffffu;
@@ -434,8 +434,8 @@ __device__ __forceinline__ void sweep_x_row_mp5(const StageArgs<CTT>& a, const G
     R vrp[NV];
 #pragma unroll
     for (int nv = 0; nv < NV; nv++) {   // cell nx-1 (stencil nx-3 .. nx+1)
-      pVLn[nv] = mp5_edge(q[0][nv], q[1][nv], q[2][nv], q[3][nv], q[4][nv]);
-      vrp[nv] = mp5_edge(q[4][nv], q[3][nv], q[2][nv], q[1][nv], q[0][nv]);
+      pVLn[nv] = edge5<LIM>(q[0][nv], q[1][nv], q[2][nv], q[3][nv], q[4][nv]);
+      vrp[nv] = edge5<LIM>(q[4][nv], q[3][nv], q[2][nv], q[1][nv], q[0][nv]);
       pV1[nv] = q[2][nv];
       pV2[nv] = q[1][nv];
       pF[nv] = R(0);
@@ -495,8 +495,8 @@ __device__ __forceinline__ void sweep_x_row_mp5(const StageArgs<CTT>& a, const G
       const R vm2 = (lane == 0) ? pV2[nv] : ((lane == 1) ? pV1[nv] : up2);
       const R vp1 = selfp1 ? sp1 : dn1;
       const R vp2 = selfp1 ? sp2 : (nextself ? sp1n : dn2);
-      vLn[nv] = mp5_edge(vm2, vm1, Vc[nv], vp1, vp2);   // right edge: face f+1
-      vR[nv] = mp5_edge(vp2, vp1, Vc[nv], vm1, vm2);    // left edge: face f
+      vLn[nv] = edge5<LIM>(vm2, vm1, Vc[nv], vp1, vp2);   // right edge: face f+1
+      vR[nv] = edge5<LIM>(vp2, vp1, Vc[nv], vm1, vm2);    // left edge: face f
       if (nv == RHO) { qm[0] = vm1; qp[0] = vp1; }
       if (nv == NV - 1) { qm[1] = vm1; qp[1] = vp1; }
     }
@@ -571,8 +571,8 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
     sweep_x_row_ppm<PHYS, NV, NDIM, RS, CT, R, CTT>(a, g, row, stg_, tid);
     return;
   }
-  if constexpr (LIM == LIM_MP5) {
-    sweep_x_row_mp5<PHYS, NV, NDIM, RS, CT, R, CTT>(a, g, row, stg_, tid);
+  if constexpr (five_point<LIM>()) {
+    sweep_x_row_mp5<PHYS, NV, NDIM, RS, CT, LIM, R, CTT>(a, g, row, stg_, tid);
     return;
   }
   constexpr unsigned FULL = 0xffffffffu;
@@ -827,7 +827,8 @@ __device__ __forceinline__ void sweep_m_col_ppm(const StageArgs<CTT>& a, const G
   if (err) atomicOr(a.err, err);
 }
 
-template <int PHYS, int NV, int NDIM, int RS, int CT, int DIR, typename R, typename CTT>
+template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, int DIR, typename R,
+          typename CTT>
 __device__ __forceinline__ void sweep_m_col_mp5(const StageArgs<CTT>& a, const Grid3& g, int i,
                                                 int t, int seg, int S, double* stg_, int tid) {
   double(*stg)[NV + 1][SWEEP_THREADS] = reinterpret_cast<double(*)[NV + 1][SWEEP_THREADS]>(stg_);
@@ -862,8 +863,8 @@ __device__ __forceinline__ void sweep_m_col_mp5(const StageArgs<CTT>& a, const G
       R vrp[NV];
 #pragma unroll
       for (int nv = 0; nv < NV; nv++) {   // cell m0-1 (stencil m0-3 .. m0+1)
-        vLn[nv] = mp5_edge(q3[nv], Wm[nv], W0[nv], W1[nv], W2[nv]);
-        vrp[nv] = mp5_edge(W2[nv], W1[nv], W0[nv], Wm[nv], q3[nv]);
+        vLn[nv] = edge5<LIM>(q3[nv], Wm[nv], W0[nv], W1[nv], W2[nv]);
+        vrp[nv] = edge5<LIM>(W2[nv], W1[nv], W0[nv], Wm[nv], q3[nv]);
         Fp[nv] = R(0);
       }
       const R qm[2] = {Wm[RHO], Wm[NV - 1]}, qp[2] = {W1[RHO], W1[NV - 1]};
@@ -878,8 +879,8 @@ __device__ __forceinline__ void sweep_m_col_mp5(const StageArgs<CTT>& a, const G
       for (int nv = 0; nv < NV; nv++) {
         W3[nv] = (R)stg[buf][nv][tid];                             // cell m+2
         vL[nv] = vLn[nv];
-        vLn[nv] = mp5_edge(Wm[nv], W0[nv], W1[nv], W2[nv], W3[nv]);  // cell m, right
-        vR[nv] = mp5_edge(W3[nv], W2[nv], W1[nv], W0[nv], Wm[nv]);   // cell m, left
+        vLn[nv] = edge5<LIM>(Wm[nv], W0[nv], W1[nv], W2[nv], W3[nv]);  // cell m, right
+        vR[nv] = edge5<LIM>(W3[nv], W2[nv], W1[nv], W0[nv], Wm[nv]);   // cell m, left
       }
       {
         const R qm[2] = {W0[RHO], W0[NV - 1]}, qp[2] = {W2[RHO], W2[NV - 1]};
@@ -930,8 +931,8 @@ __device__ __forceinline__ void sweep_m_col(const StageArgs<CTT>& a, const Grid3
     sweep_m_col_ppm<PHYS, NV, NDIM, RS, CT, DIR, R, CTT>(a, g, i, t, seg, S, stg_, tid);
     return;
   }
-  if constexpr (LIM == LIM_MP5) {
-    sweep_m_col_mp5<PHYS, NV, NDIM, RS, CT, DIR, R, CTT>(a, g, i, t, seg, S, stg_, tid);
+  if constexpr (five_point<LIM>()) {
+    sweep_m_col_mp5<PHYS, NV, NDIM, RS, CT, LIM, DIR, R, CTT>(a, g, i, t, seg, S, stg_, tid);
     return;
   }
   double(*stg)[NV + 1][SWEEP_THREADS] = reinterpret_cast<double(*)[NV + 1][SWEEP_THREADS]>(stg_);
@@ -1038,20 +1039,20 @@ __global__ void __launch_bounds__(SWEEP_THREADS, (sweep_m_minb<PHYS, R>()))
 // b[W/2]).
 // ---------------------------------------------------------------------
 template <int LIM>
-__device__ __forceinline__ constexpr int emf_width() { return LIM == LIM_MP5 ? 6 : 4; }
+__device__ __forceinline__ constexpr int emf_width() { return five_point<LIM>() ? 6 : 4; }
 
 template <int LIM, typename R>
 __device__ __forceinline__ void uct_terms(const R* b, const R* q, R aL, R aR, R dL, R dR,
                                           R& avg, R& phi) {
   R bL, bR, vL, vR;
-  if constexpr (LIM == LIM_MP5) {
-    // MP5 edge values of both the face field and the velocity
+  if constexpr (five_point<LIM>()) {
+    // MP5 (WENO-Z) edge values of both the face field and the velocity
     // (Src/array_reconstruct.cpp:327-384): the right edge of cell b[2] and
     // the left edge of cell b[3]
-    bL = mp5_edge(b[0], b[1], b[2], b[3], b[4]);
-    bR = mp5_edge(b[5], b[4], b[3], b[2], b[1]);
-    vL = mp5_edge(q[0], q[1], q[2], q[3], q[4]);
-    vR = mp5_edge(q[5], q[4], q[3], q[2], q[1]);
+    bL = edge5<LIM>(b[0], b[1], b[2], b[3], b[4]);
+    bR = edge5<LIM>(b[5], b[4], b[3], b[2], b[1]);
+    vL = edge5<LIM>(q[0], q[1], q[2], q[3], q[4]);
+    vR = edge5<LIM>(q[5], q[4], q[3], q[2], q[1]);
   } else if constexpr (LIM == LIM_PPM) {
     // parabolic reconstruction of both the face field and the velocity
     // (Src/MHD/CT/ct_emf_average.cpp:556-559 with RECONSTRUCTION PARABOLIC)

@@ -94,7 +94,7 @@ static void run_stage(const StageArgs<CTT>& a, const GridDims& gd, int seg, cuda
   const unsigned nb = (unsigned)((gd.n + 255) / 256);
   if constexpr (PHYS != PHYS_HD) {
     pre();
-    if constexpr (NDIM == 3 && (sizeof(RT) == 8 || LIM == LIM_MP5)) {  // plane-staged EMF
+    if constexpr (NDIM == 3 && (sizeof(RT) == 8 || five_point<LIM>())) {  // plane-staged EMF
       using T = EmfTile<LIM, CTT>;
       cudaFuncSetAttribute(emf_tile_kernel<LIM, RT, CTT>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, T::SMEM);
@@ -134,6 +134,7 @@ static int by_lim(const StageArgs<CTT>& a, const GridDims& g, int lim, int seg, 
     case LIM_MINMOD: run_stage<PHYS, NV, NDIM, RS, CT, LIM_MINMOD>(a, g, seg, s, ev); return 0;
     case LIM_PPM: run_stage<PHYS, NV, NDIM, RS, CT, LIM_PPM>(a, g, seg, s, ev); return 0;
     case LIM_MP5: run_stage<PHYS, NV, NDIM, RS, CT, LIM_MP5>(a, g, seg, s, ev); return 0;
+    case LIM_WENOZ: run_stage<PHYS, NV, NDIM, RS, CT, LIM_WENOZ>(a, g, seg, s, ev); return 0;
     case LIM_FLAT: run_stage<PHYS, NV, NDIM, RS, CT, LIM_FLAT>(a, g, seg, s, ev); return 0;
     case LIM_VANALBADA:
       run_stage<PHYS, NV, NDIM, RS, CT, LIM_VANALBADA>(a, g, seg, s, ev);

@@ -35,7 +35,12 @@ enum : int { PHYS_HD = 0, PHYS_MHD = 1, PHYS_RMHD = 2 };
 // 5th-order reconstruction (RECONSTRUCTION PARABOLIC / MP5); they are
 // carried in the limiter slot of the scheme templates.
 enum : int { LIM_FLAT = 0, LIM_MINMOD = 1, LIM_VL = 2, LIM_MC = 3, LIM_PPM = 4, LIM_MP5 = 5,
-             LIM_VANALBADA = 6, LIM_OSPRE = 7, LIM_UMIST = 8 };
+             LIM_VANALBADA = 6, LIM_OSPRE = 7, LIM_UMIST = 8, LIM_WENOZ = 9 };
+
+// MP5 and WENO-Z share the 5-point driver (Src/States/mp5_states.cpp) and
+// differ only in the edge value.
+template <int LIM>
+__host__ __device__ constexpr bool five_point() { return LIM == LIM_MP5 || LIM == LIM_WENOZ; }
 enum : int { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2 };
 enum : int { CT_UCT_HLL = 0, CT_UCT_HLLD = 1 };
 
@@ -131,6 +136,42 @@ __device__ __forceinline__ R mp5_edge(R Fmm, R Fm, R F0, R Fp, R Fpp) {
   s2 = GP_MAX(s2, fLC);
   const R fmax = GP_MIN(s1, s2);                                       // Eq. (2.24b)
   return f + minmod(fmin - f, fmax - f);                               // Eq. (2.26)
+}
+
+// WENO-Z edge value of Borges et al. (2008), the 3rd-order-weights form of
+// Src/States/states.hpp:108-166 (no HIGH_ORDER), stencil ordered towards
+// the edge as for mp5_edge.  The smoothness floor is 1e-40 in FP64; in the
+// mixed form's flushed FP32 it would vanish, so FP32 uses 1e-30.
+template <typename R>
+__device__ __forceinline__ R wenoz_edge(R Fmm, R Fm, R F0, R Fp, R Fpp) {
+  const R c13_12 = R(13.0 / 12.0);
+  const R eps = sizeof(R) == 8 ? R(1.e-40) : R(1.e-30);
+  R a0 = Fmm - R(2) * Fm + F0;
+  R a1 = Fmm - R(4) * Fm + R(3) * F0;
+  const R b0 = c13_12 * a0 * a0 + R(0.25) * a1 * a1;
+  a0 = Fm - R(2) * F0 + Fp;
+  a1 = Fm - Fp;
+  const R b1 = c13_12 * a0 * a0 + R(0.25) * a1 * a1;
+  a0 = F0 - R(2) * Fp + Fpp;
+  a1 = R(3) * F0 - R(4) * Fp + Fpp;
+  const R b2 = c13_12 * a0 * a0 + R(0.25) * a1 * a1;
+  const R t5 = rabs(b0 - b2);
+  a0 = R(1) * (R(1) + t5 / (b0 + eps));
+  a1 = R(6) * (R(1) + t5 / (b1 + eps));
+  const R a2 = R(3) * (R(1) + t5 / (b2 + eps));
+  const R sum_a = R(1) / (a0 + a1 + a2);
+  const R w0 = a0 * sum_a, w1 = a1 * sum_a, w2 = a2 * sum_a;
+  const R f0 = R(2) * Fmm - R(7) * Fm + R(11) * F0;
+  const R f1 = -Fm + R(5) * F0 + R(2) * Fp;
+  const R f2 = R(2) * F0 + R(5) * Fp - Fpp;
+  return (w0 * f0 + w1 * f1 + w2 * f2) / R(6);
+}
+
+// The 5-point edge value of the scheme (MP5 or WENO-Z).
+template <int LIM, typename R>
+__device__ __forceinline__ R edge5(R Fmm, R Fm, R F0, R Fp, R Fpp) {
+  if constexpr (LIM == LIM_WENOZ) return wenoz_edge(Fmm, Fm, F0, Fp, Fpp);
+  else return mp5_edge(Fmm, Fm, F0, Fp, Fpp);
 }
 
 // PPM constrained face value between cells q0 and qp (stencil qm, q0, qp,

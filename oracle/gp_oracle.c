@@ -679,6 +679,41 @@ static double MP5_Edge(const double *F, long st, int sign) {
   return f;
 }
 
+/* WENO-Z edge value of Borges et al. (2008) with the 3rd-order weights
+   (1, 6, 3), Src/States/states.hpp:108-166 without HIGH_ORDER; F points at
+   the cell, `st` is the stride, sign +1 the right edge, -1 the left. */
+static double WENOZ_Edge(const double *F, long st, int sign) {
+  const double Fmm = F[-2*sign*st], Fm = F[-sign*st], F0 = F[0], Fp = F[sign*st],
+               Fpp = F[2*sign*st];
+  const double c13_12 = 13.0/12.0;
+  double a0, a1, a2, b0, b1, b2, t5, sum_a, w0, w1, w2, f0, f1, f2;
+  a0 = Fmm - 2.0*Fm + F0;
+  a1 = Fmm - 4.0*Fm + 3.0*F0;
+  b0 = c13_12*a0*a0 + 0.25*a1*a1;
+  a0 = Fm - 2.0*F0 + Fp;
+  a1 = Fm - Fp;
+  b1 = c13_12*a0*a0 + 0.25*a1*a1;
+  a0 = F0 - 2.0*Fp + Fpp;
+  a1 = 3.0*F0 - 4.0*Fp + Fpp;
+  b2 = c13_12*a0*a0 + 0.25*a1*a1;
+  t5 = fabs(b0 - b2);
+  a0 = 1.0*(1.0 + t5/(b0 + 1.e-40));
+  a1 = 6.0*(1.0 + t5/(b1 + 1.e-40));
+  a2 = 3.0*(1.0 + t5/(b2 + 1.e-40));
+  sum_a = 1.0/(a0 + a1 + a2);
+  w0 = a0*sum_a; w1 = a1*sum_a; w2 = a2*sum_a;
+  f0 = 2.0*Fmm - 7.0*Fm + 11.0*F0;
+  f1 = -Fm + 5.0*F0 + 2.0*Fp;
+  f2 = 2.0*F0 + 5.0*Fp - Fpp;
+  return (w0*f0 + w1*f1 + w2*f2)/6.0;
+}
+
+/* the 5-point schemes sharing Src/States/mp5_states.cpp */
+static int FivePoint(int lim) { return lim == ORC_LIM_MP5 || lim == ORC_LIM_WENOZ; }
+static double Edge5(int lim, const double *F, long st, int sign) {
+  return lim == ORC_LIM_WENOZ ? WENOZ_Edge(F, st, sign) : MP5_Edge(F, st, sign);
+}
+
 /* ------------------------------------------------------------------ */
 /* boundary: Src/boundary.cpp:67-322 + PeriodicBoundary 502-675         */
 /* ------------------------------------------------------------------ */
@@ -922,9 +957,9 @@ static void Sweep(orc_t *o, int dir, double dt) {
        Src/States/ppm_states.cpp:110-164 */
     for (nv = 0; nv < nvar; nv++)
       for (i = ib-1; i <= ie+1; i++) {
-        if (o->c.limiter == ORC_LIM_MP5) {   /* Src/States/mp5_states.cpp:125-172 */
-          vL[(i+1)*nvar + nv] = MP5_Edge(v + i*nvar + nv, nvar, +1);
-          vR[i*nvar + nv]     = MP5_Edge(v + i*nvar + nv, nvar, -1);
+        if (FivePoint(o->c.limiter)) {   /* Src/States/mp5_states.cpp:125-182 */
+          vL[(i+1)*nvar + nv] = Edge5(o->c.limiter, v + i*nvar + nv, nvar, +1);
+          vR[i*nvar + nv]     = Edge5(o->c.limiter, v + i*nvar + nv, nvar, -1);
           continue;
         }
         if (o->c.limiter == ORC_LIM_PPM) {
@@ -942,7 +977,7 @@ static void Sweep(orc_t *o, int dir, double dt) {
       }
     /* MP5: density and pressure edges that came out negative fall back to
        minmod PLM (Src/States/mp5_states.cpp:184-213, uniform grid) */
-    if (o->c.limiter == ORC_LIM_MP5) {
+    if (FivePoint(o->c.limiter)) {
       const int qv[2] = {RHO, nvar - 1};
       int q;
       for (i = ib-1; i <= ie+1; i++)
@@ -1021,11 +1056,11 @@ static void ArrayRec(orc_t *o, int dir, int t1, int t2, int stag, const double *
     TrueIdx(dir, i, t1, t2, &ti, &tj, &tk);
     q[i] = (stag >= 0) ? o->Vs[stag][SI(o, stag, ti, tj, tk)] : Qe[EI(o, ti, tj, tk)];
   }
-  if (lim == ORC_LIM_MP5) {
-    /* MP5 branch, Src/array_reconstruct.cpp:327-384 */
+  if (FivePoint(lim)) {
+    /* WENOZ / MP5 branch, Src/array_reconstruct.cpp:327-384 */
     for (i = 2; i < nd-2; i++) {
-      qL[i+1] = MP5_Edge(q + i, 1, +1);
-      qR[i]   = MP5_Edge(q + i, 1, -1);
+      qL[i+1] = Edge5(lim, q + i, 1, +1);
+      qR[i]   = Edge5(lim, q + i, 1, -1);
     }
     return;
   }
@@ -1066,7 +1101,7 @@ static void ComputeEMF(orc_t *o) {
   /* Src/MHD/CT/ct_emf_average.cpp:553-559: MC for B and the scheme limiter
      for velocities with linear reconstruction; parabolic for both with PPM */
   int recV = o->c.limiter,
-      recB = (o->c.limiter == ORC_LIM_PPM || o->c.limiter == ORC_LIM_MP5) ? o->c.limiter
+      recB = (o->c.limiter == ORC_LIM_PPM || FivePoint(o->c.limiter)) ? o->c.limiter
                                                                          : ORC_LIM_MC;
   int ib = o->beg[0], ie = o->end[0] + 1;
   int jb = o->beg[1], je = o->end[1] + 1;
@@ -1407,7 +1442,7 @@ void *orc_create(const orc_cfg *cfg) {
   int d, e;
   o->c = *cfg;
   o->nvar = (cfg->physics == ORC_HD) ? 5 : 8;
-  o->ng = (cfg->limiter == ORC_LIM_PPM || cfg->limiter == ORC_LIM_MP5) ? 3 : 2;
+  o->ng = (cfg->limiter == ORC_LIM_PPM || FivePoint(cfg->limiter)) ? 3 : 2;
   /* Src/get_nghost.cpp:33-44 */
   o->ncell = 1;
   for (d = 0; d < 3; d++) {

@@ -189,6 +189,25 @@ CASES = {
                                dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
                                     ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
                                     reconstruction="MP5"), 6),
+    # WENO-Z reconstruction (the 5-point driver of MP5, 3 ghost cells)
+    "mhd2d_wenoz_hlld_ucthlld": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=141),
+                                 dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",
+                                      ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4,
+                                      reconstruction="WENOZ"), 10),
+    "mhd3d_wenoz_hll_ucthll_outflow_rk3": (
+        ics.mhd3d_turbulence, dict(n=(12, 10, 9), seed=142),
+        dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="hll", ct_emf="UCT_HLL", cfl=0.4,
+             first_dt=1e-4, reconstruction="WENOZ", rk="RK3",
+             bc=("outflow", "periodic", "periodic")), 6),
+    "hd2d_wenoz_hllc_reflect": (ics.hd_turbulence, dict(n=(22, 18), seed=143),
+                                dict(physics="HD", ndim=2, limiter="MC_LIM", solver="hllc",
+                                     cfl=0.4, first_dt=1e-4, reconstruction="WENOZ",
+                                     bc=("periodic", "reflective", "periodic")), 12),
+    "rmhd3d_wenoz_hlld_ucthll": (ics.rmhd3d_turbulence, dict(n=(10, 8, 8), seed=144,
+                                                             lorentz_max=5.0),
+                                 dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                      ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
+                                      reconstruction="WENOZ"), 6),
     # the other PLM limiters of Src/plm_coeffs.hpp (uniform-grid forms)
     "mhd2d_flat_hlld_ucthlld": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=121),
                                 dict(physics="MHD", ndim=2, limiter="FLAT_LIM", solver="hlld",
@@ -288,7 +307,8 @@ def make_io(name: str) -> str:
 
 
 def ref_cfg_name(rc: dict) -> str:
-    lim = {"PARABOLIC": "ppm", "MP5": "mp5"}.get(rc.get("reconstruction"), rc["limiter"])
+    lim = {"PARABOLIC": "ppm", "MP5": "mp5", "WENOZ": "wenoz"}.get(rc.get("reconstruction"),
+                                                                 rc["limiter"])
     rk = "_rk3" if rc.get("rk") == "RK3" else ""
     return "{physics}{ndim}d_{lim}_{solver}_{ct}".format(
         ct=rc.get("ct_emf", "none"), lim=lim, **rc).lower() + rk

@@ -54,3 +54,5 @@ class Golden:
             self.limiter = "ppm"
         elif self.reconstruction == "MP5":
             self.limiter = "mp5"
+        elif self.reconstruction == "WENOZ":
+            self.limiter = "wenoz"

@@ -247,17 +247,19 @@ MP5_CASES = [
 ]
 
 
+@pytest.mark.parametrize("rec", ["mp5", "wenoz"])
 @pytest.mark.parametrize("case", range(len(MP5_CASES)))
-def test_gpu_mp5_matches_oracle_bitwise(case):
+def test_gpu_mp5_matches_oracle_bitwise(case, rec):
+    """MP5 and WENO-Z (the same 5-point driver, different edge values)."""
     gen, kw, rs, ct, bc, rk, nsteps = MP5_CASES[case]
     st = gen(**kw)
-    kwo = dict(limiter="mp5", solver=rs, rk=rk, **bc)
+    kwo = dict(limiter=rec, solver=rs, rk=rk, **bc)
     if st.physics != ics.PHYS_HD:
         kwo["ct"] = ct
     o = orc.Oracle(st, **kwo)
     ohist, oerr = o.run(nsteps, 1e-4)
     Vo, Uo, Bo = o.state()
-    s = make_solver(st, "mp5", rs, ct, rk=rk, **bc)
+    s = make_solver(st, rec, rs, ct, rk=rk, **bc)
     dt_after, hist, out = s.run(nsteps, 1e-4)
     V, U, Bs = s.download()
     assert out.err_bits == oerr
@@ -268,11 +270,12 @@ def test_gpu_mp5_matches_oracle_bitwise(case):
         np.testing.assert_array_equal(a, b)
 
 
-def test_mp5_mixed_form_stays_close_to_fp64():
+@pytest.mark.parametrize("rec", ["mp5", "wenoz"])
+def test_mp5_mixed_form_stays_close_to_fp64(rec):
     st = ics.mhd3d_blast(n=(32, 32, 32), seed=115, radius=0.2)
-    a = make_solver(st, "mp5", "hlld", "uct_hlld")
+    a = make_solver(st, rec, "hlld", "uct_hlld")
     _, hist, _ = a.run(20, 1e-4)
-    b = make_solver(st, "mp5", "hlld", "uct_hlld", precision=api.MIXED)
+    b = make_solver(st, rec, "hlld", "uct_hlld", precision=api.MIXED)
     for dt in hist:
         b.AdvanceStep(float(dt))
     Ua, Ub = a.download()[1], b.download()[1]
