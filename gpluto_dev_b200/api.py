@@ -28,11 +28,11 @@ GP_OK, GP_ERR_INVALID, GP_ERR_QUIT, GP_ERR_NO_DEVICE, GP_ERR_IO = 0, -1, -5, -6,
 BC_PERIODIC, BC_OUTFLOW, BC_REFLECTIVE, BC_AXISYMMETRIC, BC_EQTSYMMETRIC = 0, 1, 2, 3, 4
 BC_USERDEF = 8
 HD, MHD, RMHD = 0, 1, 2
-# "ppm", "mp5" and "wenoz" select RECONSTRUCTION PARABOLIC, MP5 and WENOZ (the limiter then
+# "ppm", "mp5", "wenoz", "limo3" and "weno3" select those RECONSTRUCTIONs (the limiter then
 # plays no part)
 LIMITERS = {"flat": 0, "minmod": 1, "vl": 2, "vanleer": 2, "mc": 3, "ppm": 3, "mp5": 3,
-            "wenoz": 3, "vanalbada": 6, "ospre": 7, "umist": 8}
-RECONSTRUCTION = {"ppm": 1, "mp5": 2, "wenoz": 3}
+            "wenoz": 3, "limo3": 3, "weno3": 3, "vanalbada": 6, "ospre": 7, "umist": 8}
+RECONSTRUCTION = {"ppm": 1, "mp5": 2, "wenoz": 3, "limo3": 4, "weno3": 5}
 SOLVERS = {"hll": 0, "hllc": 1, "hlld": 2}
 CT_AVG = {"uct_hll": 0, "uct_hlld": 1}
 FP64, MIXED = 0, 1

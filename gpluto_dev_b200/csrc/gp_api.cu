@@ -646,16 +646,23 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   if (scheme->physics == GP_HD && scheme->riemann == GP_RS_HLLD)
     return fail(GP_ERR_UNSUPPORTED, "HD has no HLLD solver");
   if (scheme->reconstruction != GP_REC_LINEAR && scheme->reconstruction != GP_REC_PARABOLIC &&
-      scheme->reconstruction != GP_REC_MP5 && scheme->reconstruction != GP_REC_WENOZ)
+      scheme->reconstruction != GP_REC_MP5 && scheme->reconstruction != GP_REC_WENOZ &&
+      scheme->reconstruction != GP_REC_LIMO3 && scheme->reconstruction != GP_REC_WENO3)
     return fail(GP_ERR_UNSUPPORTED, "reconstruction %d not built", scheme->reconstruction);
   if (scheme->reconstruction == GP_REC_LINEAR &&
       !((scheme->limiter >= GP_LIM_FLAT && scheme->limiter <= GP_LIM_MC) ||
         (scheme->limiter >= GP_LIM_VANALBADA && scheme->limiter <= GP_LIM_UMIST)))
     return fail(GP_ERR_UNSUPPORTED, "limiter %d not built", scheme->limiter);
-  if (scheme->reconstruction != GP_REC_LINEAR)
+  // ghost depth of the scheme (Src/get_nghost.cpp:33-44): 3 for the
+  // PARABOLIC, MP5 and WENOZ stencils, 2 for LINEAR, LimO3 and WENO3
+  const bool wide = scheme->reconstruction == GP_REC_PARABOLIC ||
+                    scheme->reconstruction == GP_REC_MP5 ||
+                    scheme->reconstruction == GP_REC_WENOZ;
+  if (wide)
     for (int d = 0; d < grid->ndim; d++)
       if (grid->nint[d] < 4)
-        return fail(GP_ERR_INVALID, "PPM and MP5 need at least 4 cells along each direction");
+        return fail(GP_ERR_INVALID,
+                    "PPM, MP5 and WENO-Z need at least 4 cells along each direction");
   int rc = check_device();
   if (rc) return rc;
   gp_handle* h = new (std::nothrow) gp_handle;
@@ -688,8 +695,7 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   h->padded = (h->reflect | h->eqtsym | h->userdef) != 0 ||
               (h->outflow != 0 && scheme->physics != GP_HD);
   {
-    // ghost depth of the scheme (Src/get_nghost.cpp:33-44)
-    const int S = scheme->reconstruction == GP_REC_LINEAR ? 2 : 3;
+    const int S = wide ? 3 : 2;
     const int nn[3] = {h->nx, h->ny, h->nz};
     int pp[3];
     for (int d = 0; d < 3; d++) {
@@ -731,6 +737,8 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
                          scheme->reconstruction == GP_REC_PARABOLIC ? 4   /* LIM_PPM */
                          : scheme->reconstruction == GP_REC_MP5     ? 5   /* LIM_MP5 */
                          : scheme->reconstruction == GP_REC_WENOZ   ? 9   /* LIM_WENOZ */
+                         : scheme->reconstruction == GP_REC_LIMO3   ? 10  /* LIM_LIMO3 */
+                         : scheme->reconstruction == GP_REC_WENO3   ? 11  /* LIM_WENO3 */
                                                                     : scheme->limiter};
   // pencil segment for the marching sweeps: enough threads to fill 148 SMs
   {

@@ -596,15 +596,28 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
     load_cell<NV>(a.V, n, rb + gidx(-1, nx, ob, 0), v0);
     load_cell<NV>(a.V, n, rb + 0, vp);
     R pVR[NV];
+    if constexpr (three_point<LIM>()) {
+      const R dx = (R)a.dx[0];
 #pragma unroll
-    for (int nv = 0; nv < NV; nv++) {
-      R dv = limit<LIM>(vp[nv] - v0[nv], v0[nv] - vm[nv]);
-      pV[nv] = v0[nv];
-      pVLn[nv] = v0[nv] + R(0.5) * dv;
-      pVR[nv] = v0[nv] - R(0.5) * dv;
-      pF[nv] = R(0);
+      for (int nv = 0; nv < NV; nv++) {
+        pV[nv] = v0[nv];
+        pVLn[nv] = edge3<LIM>(vm[nv], v0[nv], vp[nv], dx);
+        pVR[nv] = edge3<LIM>(vp[nv], v0[nv], vm[nv], dx);
+        pF[nv] = R(0);
+      }
+      const R qm[2] = {vm[RHO], vm[NV - 1]}, qp[2] = {vp[RHO], vp[NV - 1]};
+      mp5_fallback<PHYS, NV>(v0, qm, qp, pVR, pVLn);
+    } else {
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) {
+        R dv = limit<LIM>(vp[nv] - v0[nv], v0[nv] - vm[nv]);
+        pV[nv] = v0[nv];
+        pVLn[nv] = v0[nv] + R(0.5) * dv;
+        pVR[nv] = v0[nv] - R(0.5) * dv;
+        pF[nv] = R(0);
+      }
+      if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(v0, pVR, pVLn);
     }
-    if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(v0, pVR, pVLn);
   }
   R fF[NV], fCm = R(0);  // flux of face 0 (lane 0 of the first chunk)
   R F[NV], cm = R(0);
@@ -641,17 +654,32 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
       Vc[nv] = (R)stg[buf][nv][tid];
       if (selfp1) Vp1[nv] = (R)stg[buf][NV + nv][tid];
     }
+    if constexpr (three_point<LIM>()) {
+      const R dx = (R)a.dx[0];
 #pragma unroll
-    for (int nv = 0; nv < NV; nv++) {
-      R up = __shfl_up_sync(FULL, Vc[nv], 1);
-      R dn = __shfl_down_sync(FULL, Vc[nv], 1);
-      Vm1[nv] = (lane == 0) ? pV[nv] : up;
-      if (!selfp1) Vp1[nv] = dn;
-      R dv = limit<LIM>(Vp1[nv] - Vc[nv], Vc[nv] - Vm1[nv]);
-      vR[nv] = Vc[nv] - R(0.5) * dv;
-      vLn[nv] = Vc[nv] + R(0.5) * dv;
+      for (int nv = 0; nv < NV; nv++) {
+        R up = __shfl_up_sync(FULL, Vc[nv], 1);
+        R dn = __shfl_down_sync(FULL, Vc[nv], 1);
+        Vm1[nv] = (lane == 0) ? pV[nv] : up;
+        if (!selfp1) Vp1[nv] = dn;
+        vR[nv] = edge3<LIM>(Vp1[nv], Vc[nv], Vm1[nv], dx);
+        vLn[nv] = edge3<LIM>(Vm1[nv], Vc[nv], Vp1[nv], dx);
+      }
+      const R qm[2] = {Vm1[RHO], Vm1[NV - 1]}, qp[2] = {Vp1[RHO], Vp1[NV - 1]};
+      mp5_fallback<PHYS, NV>(Vc, qm, qp, vR, vLn);
+    } else {
+#pragma unroll
+      for (int nv = 0; nv < NV; nv++) {
+        R up = __shfl_up_sync(FULL, Vc[nv], 1);
+        R dn = __shfl_down_sync(FULL, Vc[nv], 1);
+        Vm1[nv] = (lane == 0) ? pV[nv] : up;
+        if (!selfp1) Vp1[nv] = dn;
+        R dv = limit<LIM>(Vp1[nv] - Vc[nv], Vc[nv] - Vm1[nv]);
+        vR[nv] = Vc[nv] - R(0.5) * dv;
+        vLn[nv] = Vc[nv] + R(0.5) * dv;
+      }
+      if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(Vc, vR, vLn);
     }
-    if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(Vc, vR, vLn);
 #pragma unroll
     for (int nv = 0; nv < NV; nv++) {
       R l = __shfl_up_sync(FULL, vLn[nv], 1);
@@ -962,29 +990,54 @@ __device__ __forceinline__ void sweep_m_col(const StageArgs<CTT>& a, const Grid3
       load_cell<NV>(a.V, n, base + gidx(m0 - 1, nd, g.outflow, DIR) * stride, Vp);
       load_cell<NV>(a.V, n, base + (long long)m0 * stride, Vc);
       R vrp[NV];
+      if constexpr (three_point<LIM>()) {
+        const R dx = (R)a.dx[DIR];
 #pragma unroll
-      for (int nv = 0; nv < NV; nv++) {
-        R dv = limit<LIM>(Vc[nv] - Vp[nv], Vp[nv] - vmm[nv]);
-        vLn[nv] = Vp[nv] + R(0.5) * dv;
-        vrp[nv] = Vp[nv] - R(0.5) * dv;
-        Fp[nv] = R(0);
+        for (int nv = 0; nv < NV; nv++) {
+          vLn[nv] = edge3<LIM>(vmm[nv], Vp[nv], Vc[nv], dx);
+          vrp[nv] = edge3<LIM>(Vc[nv], Vp[nv], vmm[nv], dx);
+          Fp[nv] = R(0);
+        }
+        const R qm[2] = {vmm[RHO], vmm[NV - 1]}, qp[2] = {Vc[RHO], Vc[NV - 1]};
+        mp5_fallback<PHYS, NV>(Vp, qm, qp, vrp, vLn);
+      } else {
+#pragma unroll
+        for (int nv = 0; nv < NV; nv++) {
+          R dv = limit<LIM>(Vc[nv] - Vp[nv], Vp[nv] - vmm[nv]);
+          vLn[nv] = Vp[nv] + R(0.5) * dv;
+          vrp[nv] = Vp[nv] - R(0.5) * dv;
+          Fp[nv] = R(0);
+        }
+        if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(Vp, vrp, vLn);
       }
-      if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(Vp, vrp, vLn);
     }
     int buf = 0;
     for (int m = m0; m <= m1; m++, buf ^= 1) {
       stage(m + 2, m + 1, buf ^ 1);   // prefetch for the next iteration
       cp_async_wait1();
       R Vn[NV], vL[NV], vR[NV], F[NV];
+      if constexpr (three_point<LIM>()) {
+        const R dx = (R)a.dx[DIR];
 #pragma unroll
-      for (int nv = 0; nv < NV; nv++) {
-        Vn[nv] = (R)stg[buf][nv][tid];
-        R dv = limit<LIM>(Vn[nv] - Vc[nv], Vc[nv] - Vp[nv]);
-        vL[nv] = vLn[nv];
-        vR[nv] = Vc[nv] - R(0.5) * dv;
-        vLn[nv] = Vc[nv] + R(0.5) * dv;
+        for (int nv = 0; nv < NV; nv++) {
+          Vn[nv] = (R)stg[buf][nv][tid];
+          vL[nv] = vLn[nv];
+          vR[nv] = edge3<LIM>(Vn[nv], Vc[nv], Vp[nv], dx);
+          vLn[nv] = edge3<LIM>(Vp[nv], Vc[nv], Vn[nv], dx);
+        }
+        const R qm[2] = {Vp[RHO], Vp[NV - 1]}, qp[2] = {Vn[RHO], Vn[NV - 1]};
+        mp5_fallback<PHYS, NV>(Vc, qm, qp, vR, vLn);
+      } else {
+#pragma unroll
+        for (int nv = 0; nv < NV; nv++) {
+          Vn[nv] = (R)stg[buf][nv][tid];
+          R dv = limit<LIM>(Vn[nv] - Vc[nv], Vc[nv] - Vp[nv]);
+          vL[nv] = vLn[nv];
+          vR[nv] = Vc[nv] - R(0.5) * dv;
+          vLn[nv] = Vc[nv] + R(0.5) * dv;
+        }
+        if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(Vc, vR, vLn);
       }
-      if constexpr (PHYS == PHYS_RMHD) rmhd_vel_limit<NV>(Vc, vR, vLn);
       R Bn = R(0);
       if constexpr (PHYS != PHYS_HD) {
         Bn = (R)stg[buf][NV][tid];
@@ -1043,9 +1096,16 @@ __device__ __forceinline__ constexpr int emf_width() { return five_point<LIM>() 
 
 template <int LIM, typename R>
 __device__ __forceinline__ void uct_terms(const R* b, const R* q, R aL, R aR, R dL, R dR,
-                                          R& avg, R& phi) {
+                                          R& avg, R& phi, R dx) {
   R bL, bR, vL, vR;
-  if constexpr (five_point<LIM>()) {
+  if constexpr (three_point<LIM>()) {
+    // LimO3 / WENO3 edge values of both the face field and the velocity
+    // (Src/array_reconstruct.cpp:272-325), dx the cell width along b
+    bL = edge3<LIM>(b[0], b[1], b[2], dx);
+    bR = edge3<LIM>(b[3], b[2], b[1], dx);
+    vL = edge3<LIM>(q[0], q[1], q[2], dx);
+    vR = edge3<LIM>(q[3], q[2], q[1], dx);
+  } else if constexpr (five_point<LIM>()) {
     // MP5 (WENO-Z) edge values of both the face field and the velocity
     // (Src/array_reconstruct.cpp:327-384): the right edge of cell b[2] and
     // the left edge of cell b[3]
@@ -1120,7 +1180,7 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
       q[m] = (R)a.ct[1][1][e];
     }
     face_coef<R>(a, 0, X[C] + Y[C - 1] + Z[C], c, aL, aR, dL, dR);
-    uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+    uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[0]);
     R Ez = avg + phi;
 #pragma unroll
     for (int m = 0; m < W; m++) {
@@ -1129,7 +1189,7 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
       q[m] = (R)a.ct[0][0][e];
     }
     face_coef<R>(a, 1, X[C - 1] + Y[C] + Z[C], c, aL, aR, dL, dR);
-    uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+    uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[1]);
     Ez += avg - phi;
     a.Ee[2][c] = (CTT)Ez;
   }
@@ -1143,7 +1203,7 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
         q[m] = (R)a.ct[2][0][e];
       }
       face_coef<R>(a, 0, X[C] + Y[C] + Z[C - 1], c, aL, aR, dL, dR);
-      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[0]);
       R Ey = avg - phi;
 #pragma unroll
       for (int m = 0; m < W; m++) {
@@ -1152,7 +1212,7 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
         q[m] = (R)a.ct[0][1][e];
       }
       face_coef<R>(a, 2, X[C - 1] + Y[C] + Z[C], c, aL, aR, dL, dR);
-      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[2]);
       Ey += avg + phi;
       a.Ee[1][c] = (CTT)Ey;
     }
@@ -1165,7 +1225,7 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
         q[m] = (R)a.ct[2][1][e];
       }
       face_coef<R>(a, 1, X[C] + Y[C] + Z[C - 1], c, aL, aR, dL, dR);
-      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[1]);
       R Ex = avg + phi;
 #pragma unroll
       for (int m = 0; m < W; m++) {
@@ -1174,7 +1234,7 @@ __device__ __forceinline__ void emf_cell(const StageArgs<CTT>& a, const Grid3& g
         q[m] = (R)a.ct[1][0][e];
       }
       face_coef<R>(a, 2, X[C] + Y[C - 1] + Z[C], c, aL, aR, dL, dR);
-      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[2]);
       Ex += avg - phi;
       a.Ee[0][c] = (CTT)Ex;
     }
@@ -1267,7 +1327,7 @@ __global__ void __launch_bounds__(EMF_TX * EMF_TY, 3)
       }
       coef_load<R>(a, 0, X[2] + Y[1] + Zk, f1);
       coef_pair(f1, cc, aL, aR, dL, dR);
-      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[0]);
       Ez = avg + phi;
     }
     {  // Ey, first term: Bs_z along x
@@ -1278,7 +1338,7 @@ __global__ void __launch_bounds__(EMF_TX * EMF_TY, 3)
         q[m] = (R)a.ct[2][0][e];
       }
       coef_pair(c0m, cc, aL, aR, dL, dR);
-      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[0]);
       Ey = avg - phi;
     }
 #pragma unroll
@@ -1293,7 +1353,7 @@ __global__ void __launch_bounds__(EMF_TX * EMF_TY, 3)
       }
       coef_load<R>(a, 1, X[1] + Y[2] + Zk, f1);
       coef_pair(f1, cc, aL, aR, dL, dR);
-      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[1]);
       Ez += avg - phi;
     }
     {  // Ex, first term: Bs_z along y
@@ -1304,7 +1364,7 @@ __global__ void __launch_bounds__(EMF_TX * EMF_TY, 3)
         q[m] = (R)a.ct[2][1][e];
       }
       coef_pair(c1m, cc, aL, aR, dL, dR);
-      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+      uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[1]);
       Ex = avg + phi;
     }
 #pragma unroll
@@ -1313,13 +1373,13 @@ __global__ void __launch_bounds__(EMF_TX * EMF_TY, 3)
     {  // Ey, second term: Bs_x along z (window)
       coef_load<R>(a, 2, X[1] + Y[2] + Zk, f1);
       coef_pair(f1, cc, aL, aR, dL, dR);
-      uct_terms<LIM>(zb0, zq0, aL, aR, dL, dR, avg, phi);
+      uct_terms<LIM>(zb0, zq0, aL, aR, dL, dR, avg, phi, (R)a.dx[2]);
       Ey += avg + phi;
     }
     {  // Ex, second term: Bs_y along z (window)
       coef_load<R>(a, 2, X[2] + Y[1] + Zk, f1);
       coef_pair(f1, cc, aL, aR, dL, dR);
-      uct_terms<LIM>(zb1, zq1, aL, aR, dL, dR, avg, phi);
+      uct_terms<LIM>(zb1, zq1, aL, aR, dL, dR, avg, phi, (R)a.dx[2]);
       Ex += avg - phi;
     }
     a.Ee[2][c] = (CTT)Ez;
@@ -1519,7 +1579,7 @@ __global__ void __launch_bounds__(ET_THREADS, (emf_tile_minb<R>()))
         }
         coef_tile(kk0, T::N0, e0, f1);
         coef_pair(f1, cc, aL, aR, dL, dR);
-        uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+        uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[0]);
         Ez = avg + phi;
       }
       {  // Ey, first term: Bs_z along x
@@ -1529,7 +1589,7 @@ __global__ void __launch_bounds__(ET_THREADS, (emf_tile_minb<R>()))
           q[m] = (R)qx[T::NXG + ex + m];
         }
         coef_pair(c0m, cc, aL, aR, dL, dR);
-        uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+        uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[0]);
         Ey = avg - phi;
       }
 #pragma unroll
@@ -1543,7 +1603,7 @@ __global__ void __launch_bounds__(ET_THREADS, (emf_tile_minb<R>()))
         }
         coef_tile(kk1, T::N1, e1, f1);
         coef_pair(f1, cc, aL, aR, dL, dR);
-        uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+        uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[1]);
         Ez += avg - phi;
       }
       {  // Ex, first term: Bs_z along y
@@ -1553,7 +1613,7 @@ __global__ void __launch_bounds__(ET_THREADS, (emf_tile_minb<R>()))
           q[m] = (R)qy[T::NYG + ey + m * ETX];
         }
         coef_pair(c1m, cc, aL, aR, dL, dR);
-        uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi);
+        uct_terms<LIM>(b, q, aL, aR, dL, dR, avg, phi, (R)a.dx[1]);
         Ex = avg + phi;
       }
 #pragma unroll
@@ -1562,13 +1622,13 @@ __global__ void __launch_bounds__(ET_THREADS, (emf_tile_minb<R>()))
       {  // Ey, second term: Bs_x along z (window)
         coef_tile(kk2, T::N2, e2 + ETX + 1, f1);
         coef_pair(f1, cc, aL, aR, dL, dR);
-        uct_terms<LIM>(zb0, zq0, aL, aR, dL, dR, avg, phi);
+        uct_terms<LIM>(zb0, zq0, aL, aR, dL, dR, avg, phi, (R)a.dx[2]);
         Ey += avg + phi;
       }
       {  // Ex, second term: Bs_y along z (window)
         coef_tile(kk2, T::N2, e2 + 1, f1);
         coef_pair(f1, cc, aL, aR, dL, dR);
-        uct_terms<LIM>(zb1, zq1, aL, aR, dL, dR, avg, phi);
+        uct_terms<LIM>(zb1, zq1, aL, aR, dL, dR, avg, phi, (R)a.dx[2]);
         Ex += avg - phi;
       }
       const int c = cxy + nxy * k;

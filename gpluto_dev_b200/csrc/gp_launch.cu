@@ -135,6 +135,8 @@ static int by_lim(const StageArgs<CTT>& a, const GridDims& g, int lim, int seg, 
     case LIM_PPM: run_stage<PHYS, NV, NDIM, RS, CT, LIM_PPM>(a, g, seg, s, ev); return 0;
     case LIM_MP5: run_stage<PHYS, NV, NDIM, RS, CT, LIM_MP5>(a, g, seg, s, ev); return 0;
     case LIM_WENOZ: run_stage<PHYS, NV, NDIM, RS, CT, LIM_WENOZ>(a, g, seg, s, ev); return 0;
+    case LIM_LIMO3: run_stage<PHYS, NV, NDIM, RS, CT, LIM_LIMO3>(a, g, seg, s, ev); return 0;
+    case LIM_WENO3: run_stage<PHYS, NV, NDIM, RS, CT, LIM_WENO3>(a, g, seg, s, ev); return 0;
     case LIM_FLAT: run_stage<PHYS, NV, NDIM, RS, CT, LIM_FLAT>(a, g, seg, s, ev); return 0;
     case LIM_VANALBADA:
       run_stage<PHYS, NV, NDIM, RS, CT, LIM_VANALBADA>(a, g, seg, s, ev);

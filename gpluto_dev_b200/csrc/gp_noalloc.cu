@@ -75,7 +75,7 @@ extern "C" int gp_advance_step_noalloc(const gp_grid_desc* grid, const gp_scheme
   if (!grid || !scheme || !Uc || !Vc) return GP_ERR_INVALID;
   if (grid->ndim != 2 && grid->ndim != 3) return GP_ERR_UNSUPPORTED;
   if (scheme->rk_stages != 2) return GP_ERR_UNSUPPORTED;
-  if (scheme->reconstruction == GP_REC_MP5 || scheme->reconstruction == GP_REC_WENOZ)
+  if (scheme->reconstruction != GP_REC_LINEAR && scheme->reconstruction != GP_REC_PARABOLIC)
     return GP_ERR_UNSUPPORTED;
   if (scheme->reconstruction == GP_REC_LINEAR &&
       !((scheme->limiter >= GP_LIM_FLAT && scheme->limiter <= GP_LIM_MC) ||

@@ -35,12 +35,16 @@ enum : int { PHYS_HD = 0, PHYS_MHD = 1, PHYS_RMHD = 2 };
 // 5th-order reconstruction (RECONSTRUCTION PARABOLIC / MP5); they are
 // carried in the limiter slot of the scheme templates.
 enum : int { LIM_FLAT = 0, LIM_MINMOD = 1, LIM_VL = 2, LIM_MC = 3, LIM_PPM = 4, LIM_MP5 = 5,
-             LIM_VANALBADA = 6, LIM_OSPRE = 7, LIM_UMIST = 8, LIM_WENOZ = 9 };
+             LIM_VANALBADA = 6, LIM_OSPRE = 7, LIM_UMIST = 8, LIM_WENOZ = 9, LIM_LIMO3 = 10,
+             LIM_WENO3 = 11 };
 
 // MP5 and WENO-Z share the 5-point driver (Src/States/mp5_states.cpp) and
-// differ only in the edge value.
+// differ only in the edge value; LimO3 and WENO3 use the same driver with a
+// 3-point stencil (the PLM stencil and ghost depth).
 template <int LIM>
 __host__ __device__ constexpr bool five_point() { return LIM == LIM_MP5 || LIM == LIM_WENOZ; }
+template <int LIM>
+__host__ __device__ constexpr bool three_point() { return LIM == LIM_LIMO3 || LIM == LIM_WENO3; }
 enum : int { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2 };
 enum : int { CT_UCT_HLL = 0, CT_UCT_HLLD = 1 };
 
@@ -165,6 +169,60 @@ __device__ __forceinline__ R wenoz_edge(R Fmm, R Fm, R F0, R Fp, R Fpp) {
   const R f1 = -Fm + R(5) * F0 + R(2) * Fp;
   const R f2 = R(2) * F0 + R(5) * Fp - Fpp;
   return (w0 * f0 + w1 * f1 + w2 * f2) / R(6);
+}
+
+// 3-point edge values on a uniform grid of cell width dx, stencil ordered
+// towards the edge (Fm the cell away from it, F0 the cell, Fp the cell
+// across it).  WENO3: the "improved" weights of Yamaleev & Carpenter (2009),
+// Src/States/states.hpp:178-226 without HIGH_ORDER.
+template <typename R>
+__device__ __forceinline__ R weno3_edge(R Fm, R F0, R Fp, R dx) {
+  const R dx2 = dx * dx;
+  R b0 = Fp - F0, b1 = Fm - F0;
+  b0 = b0 * b0;
+  b1 = b1 * b1;
+  R tau = Fp - R(2) * F0 + Fm;
+  tau = tau * tau;
+  const R a0 = R(2) * (R(1) + tau / (dx2 + b0));
+  const R a1 = R(1) * (R(1) + tau / (dx2 + b1));
+  const R w0 = a0 / (a0 + a1), w1 = a1 / (a0 + a1);
+  const R f0 = R(0.5) * (Fp + F0), f1 = R(0.5) * (-Fm + R(3) * F0);
+  return w0 * f0 + w1 * f1;
+}
+
+// LimO3: the third-order limiter of Cada & Torrilhon (2009), Eq. 3.22, as
+// Src/States/states.hpp:239-281 (r = 0.1, blending width 1e-12).
+template <typename R>
+__device__ __forceinline__ R limo3_edge(R Fm, R F0, R Fp, R dx) {
+  const R r = R(0.1), eps = R(1.e-12);
+  const R dvp = Fp - F0, dvm = F0 - Fm;
+  const R sp = dvp >= R(0) ? R(1) : R(-1);
+  const R advp = rabs(dvp), dvm1 = sp * dvm;
+  const R q = (R(2) * dvp + dvm) / R(3);
+  const R q1 = (R(2) * rabs(dvp) + sp * dvm) / R(3);
+  R a = GP_MIN(R(1.5) * advp, R(2) * dvm1);
+  a = GP_MIN(q1, a);
+  const R b = GP_MAX(R(-0.5) * dvm1, a);
+  const R c = GP_MIN(q1, b);
+  R psi = sp * GP_MAX(R(0), c);
+  R eta = r * dx;
+  eta = (dvm * dvm + dvp * dvp) / (eta * eta);
+  R lim;
+  if (eta <= R(1) - eps) {
+    lim = q;
+  } else if (eta >= R(1) + eps) {
+    lim = psi;
+  } else {
+    psi = (R(1) - (eta - R(1)) / eps) * q + (R(1) + (eta - R(1)) / eps) * psi;
+    lim = R(0.5) * psi;
+  }
+  return F0 + R(0.5) * lim;
+}
+
+template <int LIM, typename R>
+__device__ __forceinline__ R edge3(R Fm, R F0, R Fp, R dx) {
+  if constexpr (LIM == LIM_LIMO3) return limo3_edge(Fm, F0, Fp, dx);
+  else return weno3_edge(Fm, F0, Fp, dx);
 }
 
 // The 5-point edge value of the scheme (MP5 or WENO-Z).

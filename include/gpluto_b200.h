@@ -67,8 +67,10 @@ enum { GP_CT_UCT_HLL = 0, GP_CT_UCT_HLLD = 1 };
 enum { GP_BC_PERIODIC = 0, GP_BC_OUTFLOW = 1, GP_BC_REFLECTIVE = 2, GP_BC_AXISYMMETRIC = 3,
        GP_BC_EQTSYMMETRIC = 4, GP_BC_USERDEF = 8 };
 /* RECONSTRUCTION (definitions.hpp): LINEAR (PLM with LIMITER), PARABOLIC
-   (PPM, Src/States/ppm_states.cpp), MP5 or WENOZ (Src/States/mp5_states.cpp) */
-enum { GP_REC_LINEAR = 0, GP_REC_PARABOLIC = 1, GP_REC_MP5 = 2, GP_REC_WENOZ = 3 };
+   (PPM, Src/States/ppm_states.cpp), MP5, WENOZ, LimO3 or WENO3
+   (Src/States/mp5_states.cpp) */
+enum { GP_REC_LINEAR = 0, GP_REC_PARABOLIC = 1, GP_REC_MP5 = 2, GP_REC_WENOZ = 3,
+       GP_REC_LIMO3 = 4, GP_REC_WENO3 = 5 };
 /* arithmetic form */
 enum { GP_FP64 = 0, GP_MIXED = 1 };
 /* host array layouts */
@@ -98,7 +100,7 @@ typedef struct gp_scheme {
   double cfl_max_var;     /* Runtime::cfl_max_var */
   double small_rho;       /* RunConfig::small_rho (1e-12 default) */
   double small_prs;       /* RunConfig::small_prs (1e-12 default) */
-  int reconstruction;     /* GP_REC_LINEAR (limiter applies), _PARABOLIC, _MP5 or _WENOZ */
+  int reconstruction;     /* GP_REC_LINEAR (limiter applies) or another GP_REC_* */
 } gp_scheme;
 
 /* Per-step result: what the host needs for NextTimeStep and error handling. */

@@ -714,6 +714,63 @@ static double Edge5(int lim, const double *F, long st, int sign) {
   return lim == ORC_LIM_WENOZ ? WENOZ_Edge(F, st, sign) : MP5_Edge(F, st, sign);
 }
 
+/* WENO3 edge value, the "improved" weights of Yamaleev & Carpenter (2009),
+   Src/States/states.hpp:178-226 without HIGH_ORDER; dx the cell width. */
+static double WENO3_Edge(const double *F, long st, int sign, double dx) {
+  const double Fp = F[sign*st], Fm = F[-sign*st], F0 = F[0];
+  double a0, a1, b0, b1, w0, w1, f0, f1, tau, dx2;
+  dx2 = dx*dx;
+  b0 = Fp - F0;
+  b1 = Fm - F0;
+  b0 = b0*b0;
+  b1 = b1*b1;
+  tau = (Fp - 2.0*F0 + Fm);
+  tau = tau*tau;
+  a0 = 2.0*(1.0 + tau/(dx2 + b0));
+  a1 = 1.0*(1.0 + tau/(dx2 + b1));
+  w0 = a0/(a0 + a1);
+  w1 = a1/(a0 + a1);
+  f0 = 0.5*(Fp + F0);
+  f1 = 0.5*(-Fm + 3.0*F0);
+  return (w0*f0 + w1*f1);
+}
+
+/* LimO3 edge value (the third-order limiter of Cada & Torrilhon 2009,
+   Eq. 3.22), Src/States/states.hpp:239-281. */
+static double LimO3_Edge(const double *v, long st, int sign, double dx) {
+  const double r = 0.1, eps = 1.e-12;
+  double a, b, c, q, q1, lim, eta, psi;
+  double dvp = v[sign*st] - v[0];
+  double dvm = v[0] - v[-sign*st];
+  double sp = (dvp >= 0.0 ? 1.0 : -1.0);
+  double advp = fabs(dvp);
+  double dvm1 = sp*dvm;
+  q  = (2.0*dvp + dvm)/3.0;
+  q1 = (2.0*fabs(dvp) + sp*dvm)/3.0;
+  a = MIN(1.5*advp, 2.0*dvm1);
+  a = MIN(q1, a);
+  b = MAX(-0.5*dvm1, a);
+  c = MIN(q1, b);
+  psi = sp*MAX(0.0, c);
+  eta = r*dx;
+  eta = (dvm*dvm + dvp*dvp)/(eta*eta);
+  if (eta <= 1.0 - eps) {
+    lim = q;
+  } else if (eta >= 1.0 + eps) {
+    lim = psi;
+  } else {
+    psi = (1.0 - (eta - 1.0)/eps)*q + (1.0 + (eta - 1.0)/eps)*psi;
+    lim = 0.5*psi;
+  }
+  return v[0] + 0.5*lim;
+}
+
+/* the 3-point schemes of the same driver */
+static int ThreePoint(int lim) { return lim == ORC_LIM_LIMO3 || lim == ORC_LIM_WENO3; }
+static double Edge3(int lim, const double *F, long st, int sign, double dx) {
+  return lim == ORC_LIM_LIMO3 ? LimO3_Edge(F, st, sign, dx) : WENO3_Edge(F, st, sign, dx);
+}
+
 /* ------------------------------------------------------------------ */
 /* boundary: Src/boundary.cpp:67-322 + PeriodicBoundary 502-675         */
 /* ------------------------------------------------------------------ */
@@ -962,6 +1019,11 @@ static void Sweep(orc_t *o, int dir, double dt) {
           vR[i*nvar + nv]     = Edge5(o->c.limiter, v + i*nvar + nv, nvar, -1);
           continue;
         }
+        if (ThreePoint(o->c.limiter)) {  /* Src/States/mp5_states.cpp:164-172 */
+          vL[(i+1)*nvar + nv] = Edge3(o->c.limiter, v + i*nvar + nv, nvar, +1, o->c.dx[dir]);
+          vR[i*nvar + nv]     = Edge3(o->c.limiter, v + i*nvar + nv, nvar, -1, o->c.dx[dir]);
+          continue;
+        }
         if (o->c.limiter == ORC_LIM_PPM) {
           double dvp, dvm;
           PPM_Cell(v + i*nvar + nv, nvar, &dvp, &dvm);
@@ -977,7 +1039,7 @@ static void Sweep(orc_t *o, int dir, double dt) {
       }
     /* MP5: density and pressure edges that came out negative fall back to
        minmod PLM (Src/States/mp5_states.cpp:184-213, uniform grid) */
-    if (FivePoint(o->c.limiter)) {
+    if (FivePoint(o->c.limiter) || ThreePoint(o->c.limiter)) {
       const int qv[2] = {RHO, nvar - 1};
       int q;
       for (i = ib-1; i <= ie+1; i++)
@@ -1056,6 +1118,14 @@ static void ArrayRec(orc_t *o, int dir, int t1, int t2, int stag, const double *
     TrueIdx(dir, i, t1, t2, &ti, &tj, &tk);
     q[i] = (stag >= 0) ? o->Vs[stag][SI(o, stag, ti, tj, tk)] : Qe[EI(o, ti, tj, tk)];
   }
+  if (ThreePoint(lim)) {
+    /* LimO3 / WENO3 branch, Src/array_reconstruct.cpp:272-325 */
+    for (i = 1; i < nd-1; i++) {
+      qL[i+1] = Edge3(lim, q + i, 1, +1, o->c.dx[dir]);
+      qR[i]   = Edge3(lim, q + i, 1, -1, o->c.dx[dir]);
+    }
+    return;
+  }
   if (FivePoint(lim)) {
     /* WENOZ / MP5 branch, Src/array_reconstruct.cpp:327-384 */
     for (i = 2; i < nd-2; i++) {
@@ -1101,7 +1171,8 @@ static void ComputeEMF(orc_t *o) {
   /* Src/MHD/CT/ct_emf_average.cpp:553-559: MC for B and the scheme limiter
      for velocities with linear reconstruction; parabolic for both with PPM */
   int recV = o->c.limiter,
-      recB = (o->c.limiter == ORC_LIM_PPM || FivePoint(o->c.limiter)) ? o->c.limiter
+      recB = (o->c.limiter == ORC_LIM_PPM || FivePoint(o->c.limiter) ||
+              ThreePoint(o->c.limiter)) ? o->c.limiter
                                                                          : ORC_LIM_MC;
   int ib = o->beg[0], ie = o->end[0] + 1;
   int jb = o->beg[1], je = o->end[1] + 1;

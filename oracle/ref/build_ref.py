@@ -144,8 +144,8 @@ class RefConfig:
     def makefile(self) -> str:
         src = os.path.join(REF_ROOT, "Src")
         phys_obj, phys_dirs = _PHYS[self.physics]
-        states = {"PARABOLIC": "ppm_states", "MP5": "mp5_states",
-                  "WENOZ": "mp5_states"}.get(self.reconstruction,
+        states = {"PARABOLIC": "ppm_states", "MP5": "mp5_states", "WENOZ": "mp5_states",
+                  "LimO3": "mp5_states", "WENO3": "mp5_states"}.get(self.reconstruction,
                                                                     "plm_states")
         step = [(states if o == "plm_states" else o) for o in _STEP_OBJ]
         objs = _DEFAULT_OBJ + _MATH_OBJ + step + phys_obj

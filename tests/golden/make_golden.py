@@ -208,6 +208,27 @@ CASES = {
                                  dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
                                       ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
                                       reconstruction="WENOZ"), 6),
+    # LimO3 and WENO3 (3-point stencils of the same driver, 2 ghost cells)
+    "mhd2d_limo3_hlld_ucthlld": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=151),
+                                 dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",
+                                      ct_emf="UCT_HLLD", cfl=0.4, first_dt=1e-4,
+                                      reconstruction="LimO3"), 10),
+    "mhd3d_weno3_hlld_ucthlld_outflowz": (
+        ics.mhd3d_turbulence, dict(n=(12, 10, 9), seed=152),
+        dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="hlld", ct_emf="UCT_HLLD", cfl=0.4,
+             first_dt=1e-4, reconstruction="WENO3", bc=("periodic", "periodic", "outflow")), 6),
+    "hd2d_limo3_hllc_reflect": (ics.hd_turbulence, dict(n=(22, 18), seed=153),
+                                dict(physics="HD", ndim=2, limiter="MC_LIM", solver="hllc",
+                                     cfl=0.4, first_dt=1e-4, reconstruction="LimO3",
+                                     bc=("reflective", "periodic", "periodic")), 12),
+    "hd3d_weno3_hll_rk3": (ics.hd_turbulence, dict(n=(12, 10, 9), seed=154),
+                           dict(physics="HD", ndim=3, limiter="MC_LIM", solver="hll", cfl=0.4,
+                                first_dt=1e-4, reconstruction="WENO3", rk="RK3"), 8),
+    "rmhd3d_limo3_hlld_ucthll": (ics.rmhd3d_turbulence, dict(n=(10, 8, 8), seed=155,
+                                                             lorentz_max=5.0),
+                                 dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                      ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
+                                      reconstruction="LimO3"), 6),
     # the other PLM limiters of Src/plm_coeffs.hpp (uniform-grid forms)
     "mhd2d_flat_hlld_ucthlld": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=121),
                                 dict(physics="MHD", ndim=2, limiter="FLAT_LIM", solver="hlld",
@@ -307,8 +328,8 @@ def make_io(name: str) -> str:
 
 
 def ref_cfg_name(rc: dict) -> str:
-    lim = {"PARABOLIC": "ppm", "MP5": "mp5", "WENOZ": "wenoz"}.get(rc.get("reconstruction"),
-                                                                 rc["limiter"])
+    lim = {"PARABOLIC": "ppm", "MP5": "mp5", "WENOZ": "wenoz", "LimO3": "limo3",
+           "WENO3": "weno3"}.get(rc.get("reconstruction"), rc["limiter"])
     rk = "_rk3" if rc.get("rk") == "RK3" else ""
     return "{physics}{ndim}d_{lim}_{solver}_{ct}".format(
         ct=rc.get("ct_emf", "none"), lim=lim, **rc).lower() + rk

@@ -56,3 +56,7 @@ class Golden:
             self.limiter = "mp5"
         elif self.reconstruction == "WENOZ":
             self.limiter = "wenoz"
+        elif self.reconstruction == "LimO3":
+            self.limiter = "limo3"
+        elif self.reconstruction == "WENO3":
+            self.limiter = "weno3"

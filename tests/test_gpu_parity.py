@@ -247,10 +247,11 @@ MP5_CASES = [
 ]
 
 
-@pytest.mark.parametrize("rec", ["mp5", "wenoz"])
+@pytest.mark.parametrize("rec", ["mp5", "wenoz", "limo3", "weno3"])
 @pytest.mark.parametrize("case", range(len(MP5_CASES)))
 def test_gpu_mp5_matches_oracle_bitwise(case, rec):
-    """MP5 and WENO-Z (the same 5-point driver, different edge values)."""
+    """The schemes of the MP5 driver: MP5 and WENO-Z (5-point), LimO3 and
+    WENO3 (3-point, cell-width dependent)."""
     gen, kw, rs, ct, bc, rk, nsteps = MP5_CASES[case]
     st = gen(**kw)
     kwo = dict(limiter=rec, solver=rs, rk=rk, **bc)
@@ -270,7 +271,7 @@ def test_gpu_mp5_matches_oracle_bitwise(case, rec):
         np.testing.assert_array_equal(a, b)
 
 
-@pytest.mark.parametrize("rec", ["mp5", "wenoz"])
+@pytest.mark.parametrize("rec", ["mp5", "wenoz", "limo3", "weno3"])
 def test_mp5_mixed_form_stays_close_to_fp64(rec):
     st = ics.mhd3d_blast(n=(32, 32, 32), seed=115, radius=0.2)
     a = make_solver(st, rec, "hlld", "uct_hlld")
