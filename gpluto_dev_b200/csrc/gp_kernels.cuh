@@ -144,6 +144,7 @@ __device__ __forceinline__ R riemann(const R* vl, const R* vr, R* flux, R gamma,
                                      CTFace<R>& ct, uint32_t& err) {
   if constexpr (PHYS == PHYS_MHD) {
     if constexpr (RS == RS_HLLD) return mhd_hlld<DIR, CT>(vl, vr, flux, gamma, Bn, ct);
+    else if constexpr (RS == RS_TVDLF) return mhd_tvdlf<DIR>(vl, vr, flux, gamma, ct);
     else return mhd_hll<DIR>(vl, vr, flux, gamma, ct);
   } else if constexpr (PHYS == PHYS_RMHD) {
     if constexpr (sizeof(R) == sizeof(double)) {
@@ -165,6 +166,7 @@ __device__ __forceinline__ R riemann(const R* vl, const R* vr, R* flux, R gamma,
     }
   } else {
     if constexpr (RS == RS_HLLC) return hd_hllc<DIR>(vl, vr, flux, gamma);
+    else if constexpr (RS == RS_TVDLF) return hd_tvdlf<DIR>(vl, vr, flux, gamma);
     else return hd_hll<DIR>(vl, vr, flux, gamma);
   }
 }

@@ -157,6 +157,8 @@ static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey
       return by_lim<PHYS_MHD, 8, NDIM, RS_HLLD, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
     if (k.riemann == RS_HLL)
       return by_lim<PHYS_MHD, 8, NDIM, RS_HLL, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
+    if (k.riemann == RS_TVDLF && k.ct == CT_UCT_HLL)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_TVDLF, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
     return -1;
   }
   if (k.physics == PHYS_RMHD) {
@@ -169,6 +171,8 @@ static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey
   if (k.physics == PHYS_HD) {
     if (k.riemann == RS_HLLC) return by_lim<PHYS_HD, 5, NDIM, RS_HLLC, 0>(a, g, k.limiter, seg, s, ev);
     if (k.riemann == RS_HLL) return by_lim<PHYS_HD, 5, NDIM, RS_HLL, 0>(a, g, k.limiter, seg, s, ev);
+    if (k.riemann == RS_TVDLF)
+      return by_lim<PHYS_HD, 5, NDIM, RS_TVDLF, 0>(a, g, k.limiter, seg, s, ev);
     return -1;
   }
   return -1;

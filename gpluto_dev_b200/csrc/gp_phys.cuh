@@ -45,7 +45,7 @@ template <int LIM>
 __host__ __device__ constexpr bool five_point() { return LIM == LIM_MP5 || LIM == LIM_WENOZ; }
 template <int LIM>
 __host__ __device__ constexpr bool three_point() { return LIM == LIM_LIMO3 || LIM == LIM_WENO3; }
-enum : int { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2 };
+enum : int { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2, RS_TVDLF = 3 };
 enum : int { CT_UCT_HLL = 0, CT_UCT_HLLD = 1 };
 
 template <typename R> __device__ __forceinline__ R rsqrt_(R x);
@@ -631,6 +631,32 @@ __device__ __forceinline__ R mhd_hll(const R* vl, const R* vr, R* flux, R gamma,
   return cmax;
 }
 
+// Lax-Friedrichs (Rusanov) flux for MHD, Src/MHD/tvdlf.cpp:60-244: the
+// signal speed of the arithmetic average state; UCT_HLL face data with
+// Sl = -cmax, Sr = cmax.
+template <int DIR, typename R>
+__device__ __forceinline__ R mhd_tvdlf(const R* vl, const R* vr, R* flux, R gamma,
+                                       CTFace<R>& ct) {
+  R ul[8], ur[8], fl[8], fr[8], vLR[8], pl, pr, cmax;
+  const R gmm1 = gamma - R(1);
+  mhd_prim2cons(vl, ul, gmm1);
+  mhd_prim2cons(vr, ur, gmm1);
+#pragma unroll
+  for (int nv = 0; nv < 8; nv++) vLR[nv] = R(0.5) * (vl[nv] + vr[nv]);
+  {
+    R cminLR, cmaxLR;
+    mhd_signal_speed<DIR>(vLR, gamma * vLR[7] / vLR[RHO], cminLR, cmaxLR);
+    cmax = GP_MAX(rabs(cminLR), rabs(cmaxLR));
+  }
+  mhd_flux<DIR>(vl, ul, fl, pl);
+  mhd_flux<DIR>(vr, ur, fr, pr);
+#pragma unroll
+  for (int nv = 0; nv < 8; nv++)
+    flux[nv] = R(0.5) * (fl[nv] + fr[nv]) - R(0.5) * cmax * (ur[nv] - ul[nv]);
+  ct_store_ucthll<DIR>(vl, vr, -cmax, cmax, ct);
+  return cmax;
+}
+
 // ---------------------------------------------------------------------
 // Hydrodynamics (NVAR = 5: RHO, MX1..3, ENG)
 // ---------------------------------------------------------------------
@@ -751,6 +777,30 @@ __device__ __forceinline__ R hd_hllc(const R* vl, const R* vr, R* flux, R gamma)
 }
 
 // Src/HD/hll.cpp:95-175
+// Lax-Friedrichs flux for HD, Src/HD/tvdlf.cpp:100-190: the average state
+// takes the mean of |v_n| on the two sides.
+template <int DIR, typename R>
+__device__ __forceinline__ R hd_tvdlf(const R* vl, const R* vr, R* flux, R gamma) {
+  constexpr int VXn = VX1 + DIR;
+  R ul[5], ur[5], fL[5], fR[5], vLR[5], pl, pr, cmax;
+  hd_prim2cons(vl, ul, gamma);
+  hd_prim2cons(vr, ur, gamma);
+#pragma unroll
+  for (int nv = 0; nv < 5; nv++) vLR[nv] = R(0.5) * (vl[nv] + vr[nv]);
+  vLR[VXn] = R(0.5) * (rabs(vl[VXn]) + rabs(vr[VXn]));
+  {
+    const R a = rsqrt_(gamma * vLR[4] / vLR[RHO]);
+    const R cmaxLR = vLR[VXn] + a, cminLR = vLR[VXn] - a;
+    cmax = GP_MAX(rabs(cminLR), rabs(cmaxLR));
+  }
+  hd_flux<DIR>(vl, ul, fL, pl);
+  hd_flux<DIR>(vr, ur, fR, pr);
+#pragma unroll
+  for (int nv = 0; nv < 5; nv++)
+    flux[nv] = R(0.5) * (fL[nv] + fR[nv]) - R(0.5) * cmax * (ur[nv] - ul[nv]);
+  return cmax;
+}
+
 template <int DIR, typename R>
 __device__ __forceinline__ R hd_hll(const R* vl, const R* vr, R* flux, R gamma) {
   constexpr int VXn = VX1 + DIR;

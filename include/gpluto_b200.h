@@ -54,8 +54,9 @@ enum { GP_HD = 0, GP_MHD = 1, GP_RMHD = 2 };
    not limiters (they stand for PPM and MP5 inside the library) */
 enum { GP_LIM_FLAT = 0, GP_LIM_MINMOD = 1, GP_LIM_VANLEER = 2, GP_LIM_MC = 3,
        GP_LIM_VANALBADA = 6, GP_LIM_OSPRE = 7, GP_LIM_UMIST = 8 };
-/* [Solver] in pluto.ini (Src/MHD/set_solver.cpp:35-47) */
-enum { GP_RS_HLL = 0, GP_RS_HLLC = 1, GP_RS_HLLD = 2 };
+/* [Solver] in pluto.ini (Src/MHD/set_solver.cpp:35-47); tvdlf for MHD (with
+   UCT_HLL) and HD */
+enum { GP_RS_HLL = 0, GP_RS_HLLC = 1, GP_RS_HLLD = 2, GP_RS_TVDLF = 3 };
 /* CT_EMF_AVERAGE (Src/MHD/CT/ct.hpp:19-27) */
 enum { GP_CT_UCT_HLL = 0, GP_CT_UCT_HLLD = 1 };
 /* [Boundary] types (Src/boundary.cpp:144-310; the reference's values,

@@ -483,6 +483,53 @@ static double MHD_HLL(orc_t *o, int dir, double *vl, double *vr, double *flux, l
   return cmax;
 }
 
+/* Lax-Friedrichs (Rusanov) flux for MHD, Src/MHD/tvdlf.cpp:60-244: the
+   signal speed of the arithmetic average state, UCT_HLL face data with
+   Sl = -cmax, Sr = cmax. */
+static double MHD_TVDLF(orc_t *o, int dir, double *vl, double *vr, double *flux, long e) {
+  const double gamma = o->c.gamma;
+  int nv;
+  double ul[8], ur[8], fl[8], fr[8], vLR[8], pl, pr, cmax;
+  MHD_PrimToCons(vl, ul, gamma);
+  MHD_PrimToCons(vr, ur, gamma);
+  for (nv = 0; nv < 8; nv++) vLR[nv] = 0.5*(vl[nv] + vr[nv]);
+  {
+    double a2 = gamma*vLR[7]/vLR[RHO], cminLR, cmaxLR;
+    MHD_MaxSignalSpeed(dir, vLR, a2, &cminLR, &cmaxLR);
+    cmax = MAX(fabs(cminLR), fabs(cmaxLR));
+  }
+  MHD_Flux(dir, vl, ul, fl, &pl);
+  MHD_Flux(dir, vr, ur, fr, &pr);
+  for (nv = 0; nv < 8; nv++) flux[nv] = 0.5*(fl[nv] + fr[nv]) - 0.5*cmax*(ur[nv] - ul[nv]);
+  for (nv = 0; nv < 8; nv++) if (isnan(flux[nv])) o->err |= ERR_NAN | ERR_QUIT;
+  CT_Store_UCTHll(o, dir, vl, vr, -cmax, cmax, e);
+  return cmax;
+}
+
+/* Lax-Friedrichs flux for HD, Src/HD/tvdlf.cpp:100-190: the average state
+   takes the mean of |v_n| on the two sides. */
+static double HD_TVDLF(orc_t *o, int dir, double *vl, double *vr, double *flux) {
+  const double gamma = o->c.gamma;
+  int VXn = VX1 + dir, nv;
+  double ul[5], ur[5], fL[5], fR[5], vLR[5], pl, pr, cmax;
+  HD_PrimToCons(vl, ul, gamma);
+  HD_PrimToCons(vr, ur, gamma);
+  for (nv = 0; nv < 5; nv++) vLR[nv] = 0.5*(vl[nv] + vr[nv]);
+  vLR[VXn] = 0.5*(fabs(vl[VXn]) + fabs(vr[VXn]));
+  {
+    double a2 = gamma*vLR[4]/vLR[RHO];
+    double a = sqrt(a2);
+    double cmaxLR = vLR[VXn] + a;
+    double cminLR = vLR[VXn] - a;
+    cmax = MAX(fabs(cminLR), fabs(cmaxLR));
+  }
+  HD_Flux(dir, vl, ul, fL, &pl);
+  HD_Flux(dir, vr, ur, fR, &pr);
+  for (nv = 0; nv < 5; nv++) flux[nv] = 0.5*(fL[nv] + fR[nv]) - 0.5*cmax*(ur[nv] - ul[nv]);
+  for (nv = 0; nv < 5; nv++) if (isnan(flux[nv])) o->err |= ERR_NAN | ERR_QUIT;
+  return cmax;
+}
+
 /* Src/HD/hllc.cpp:54-260 (ideal EOS) */
 static double HD_HLLC(orc_t *o, int dir, double *vl, double *vr, double *flux) {
   const double gamma = o->c.gamma;
@@ -1078,11 +1125,13 @@ static void Sweep(orc_t *o, int dir, double dt) {
       long e = EI(o, ti, tj, tk);
       double *vl = vL + i*nvar, *vr = vR + i*nvar, *f = flux + i*nvar;
       if (o->c.physics == ORC_MHD) {
-        if (o->c.solver == ORC_HLLD) cmax[i] = MHD_HLLD(o, dir, vl, vr, f, e, Bn[i]);
-        else                         cmax[i] = MHD_HLL(o, dir, vl, vr, f, e);
+        if (o->c.solver == ORC_HLLD)       cmax[i] = MHD_HLLD(o, dir, vl, vr, f, e, Bn[i]);
+        else if (o->c.solver == ORC_TVDLF) cmax[i] = MHD_TVDLF(o, dir, vl, vr, f, e);
+        else                               cmax[i] = MHD_HLL(o, dir, vl, vr, f, e);
       } else if (o->c.physics == ORC_HD) {
-        if (o->c.solver == ORC_HLLC) cmax[i] = HD_HLLC(o, dir, vl, vr, f);
-        else                         cmax[i] = HD_HLL(o, dir, vl, vr, f);
+        if (o->c.solver == ORC_HLLC)       cmax[i] = HD_HLLC(o, dir, vl, vr, f);
+        else if (o->c.solver == ORC_TVDLF) cmax[i] = HD_TVDLF(o, dir, vl, vr, f);
+        else                               cmax[i] = HD_HLL(o, dir, vl, vr, f);
       } else {
         cmax[i] = orc_rmhd_riemann(o, dir, vl, vr, f, e);
       }

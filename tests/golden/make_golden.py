@@ -208,6 +208,21 @@ CASES = {
                                  dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
                                       ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
                                       reconstruction="WENOZ"), 6),
+    # the Lax-Friedrichs (tvdlf) solver, MHD with UCT_HLL face data and HD
+    "mhd2d_mc_tvdlf_ucthll": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=161),
+                              dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="tvdlf",
+                                   ct_emf="UCT_HLL", cfl=0.4, first_dt=1e-4), 12),
+    "mhd3d_vl_tvdlf_ucthll_outflowx": (
+        ics.mhd3d_turbulence, dict(n=(12, 10, 9), seed=162),
+        dict(physics="MHD", ndim=3, limiter="VANLEER_LIM", solver="tvdlf", ct_emf="UCT_HLL",
+             cfl=0.4, first_dt=1e-4, bc=("outflow", "periodic", "periodic")), 6),
+    "hd2d_mc_tvdlf_reflect": (ics.hd_turbulence, dict(n=(22, 18), seed=163),
+                              dict(physics="HD", ndim=2, limiter="MC_LIM", solver="tvdlf",
+                                   cfl=0.4, first_dt=1e-4,
+                                   bc=("reflective", "periodic", "periodic")), 12),
+    "hd3d_ppm_tvdlf": (ics.hd_turbulence, dict(n=(12, 10, 9), seed=164),
+                       dict(physics="HD", ndim=3, limiter="MC_LIM", solver="tvdlf", cfl=0.4,
+                            first_dt=1e-4, reconstruction="PARABOLIC"), 8),
     # LimO3 and WENO3 (3-point stencils of the same driver, 2 ghost cells)
     "mhd2d_limo3_hlld_ucthlld": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=151),
                                  dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",

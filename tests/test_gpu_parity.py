@@ -68,6 +68,10 @@ CASES = [
     (ics.mhd2d_turbulence, dict(n=(35, 19), seed=132), "ospre", "hlld", "uct_hll", 10),
     (ics.hd_turbulence, dict(n=(33, 7), seed=133), "umist", "hllc", "uct_hll", 12),
     (ics.mhd2d_turbulence, dict(n=(17, 23), seed=134), "flat", "hll", "uct_hll", 10),
+    # the Lax-Friedrichs (tvdlf) solver
+    (ics.mhd2d_turbulence, dict(n=(29, 21), seed=171), "mc", "tvdlf", "uct_hll", 10),
+    (ics.mhd3d_blast, dict(n=(13, 12, 11), seed=172, radius=0.25), "vl", "tvdlf", "uct_hll", 6),
+    (ics.hd_turbulence, dict(n=(27, 13, 11), seed=173), "ppm", "tvdlf", "uct_hll", 8),
 ]
 
 
