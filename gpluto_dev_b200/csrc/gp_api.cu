@@ -646,8 +646,13 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   if (scheme->riemann == GP_RS_TVDLF && scheme->physics == GP_RMHD)
     return fail(GP_ERR_UNSUPPORTED, "RMHD tvdlf not built");
   if (scheme->riemann == GP_RS_TVDLF && scheme->physics == GP_MHD &&
-      scheme->ct_emf != GP_CT_UCT_HLL)
+      scheme->ct_emf == GP_CT_UCT_HLLD)
     return fail(GP_ERR_UNSUPPORTED, "tvdlf needs UCT_HLL (Src/MHD/tvdlf.cpp:83-87)");
+  if (scheme->physics != GP_HD && scheme->ct_emf != GP_CT_UCT_HLL &&
+      scheme->ct_emf != GP_CT_UCT_HLLD &&
+      !(scheme->ct_emf == GP_CT_ARITHMETIC && scheme->physics == GP_MHD))
+    return fail(GP_ERR_UNSUPPORTED, "CT_EMF_AVERAGE %d not built for this physics",
+                scheme->ct_emf);
   if (scheme->riemann < GP_RS_HLL || scheme->riemann > GP_RS_TVDLF)
     return fail(GP_ERR_UNSUPPORTED, "riemann solver %d not built", scheme->riemann);
   if (scheme->physics == GP_HD && scheme->riemann == GP_RS_HLLD)

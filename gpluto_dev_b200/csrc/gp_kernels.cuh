@@ -143,9 +143,17 @@ template <int PHYS, int RS, int CT, int DIR, typename R>
 __device__ __forceinline__ R riemann(const R* vl, const R* vr, R* flux, R gamma, R Bn,
                                      CTFace<R>& ct, uint32_t& err) {
   if constexpr (PHYS == PHYS_MHD) {
-    if constexpr (RS == RS_HLLD) return mhd_hlld<DIR, CT>(vl, vr, flux, gamma, Bn, ct);
-    else if constexpr (RS == RS_TVDLF) return mhd_tvdlf<DIR>(vl, vr, flux, gamma, ct);
-    else return mhd_hll<DIR>(vl, vr, flux, gamma, ct);
+    R cm;
+    if constexpr (RS == RS_HLLD) cm = mhd_hlld<DIR, CT>(vl, vr, flux, gamma, Bn, ct);
+    else if constexpr (RS == RS_TVDLF) cm = mhd_tvdlf<DIR>(vl, vr, flux, gamma, ct);
+    else cm = mhd_hll<DIR>(vl, vr, flux, gamma, ct);
+    if constexpr (CT == CT_ARITH) {
+      // CT_Store_Arith (Src/MHD/CT/ct_store.hpp:74-93): the face's two
+      // induction fluxes, e[b][n] = -F(B_t) and e[t][n] = F(B_b)
+      ct.eb = -flux[BX1 + (DIR + 1) % 3];
+      ct.et = flux[BX1 + (DIR + 2) % 3];
+    }
+    return cm;
   } else if constexpr (PHYS == PHYS_RMHD) {
     if constexpr (sizeof(R) == sizeof(double)) {
       return rmhd_riemann<DIR, RS>(vl, vr, flux, gamma, ct, err);
@@ -1394,6 +1402,31 @@ __global__ void __launch_bounds__(EMF_TX * EMF_TY, 3)
       zb1[m] = zb1[m + 1];
       zq1[m] = zq1[m + 1];
     }
+  }
+}
+
+// Edge EMFs of CT_EMF_AVERAGE ARITHMETIC (Src/MHD/CT/ct_emf_average.cpp:36-96,
+// w = 0.25): each edge averages the four face EMFs around it, face d's two
+// components stored as ct[d][0] = e[b][d], ct[d][1] = e[t][d].
+template <int NDIM, typename R, typename CTT>
+__global__ void __launch_bounds__(256) emf_arith_kernel(StageArgs<CTT> a, Grid3 g) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, nxy = nx * ny;
+  const int ci = (int)c, i = ci % nx, j = (ci / nx) % ny, k = ci / nxy;
+  const int cxm = ci - i + wrapi(i - 1, nx), cym = ci + nx * (wrapi(j - 1, ny) - j);
+  const R w = R(0.25);
+  // Ez at (i-1/2, j-1/2, k): e[z][x] = ct[0][0], e[z][y] = ct[1][1]
+  a.Ee[2][c] = (CTT)(w * ((R)a.ct[0][0][ci] + (R)a.ct[0][0][cym] + (R)a.ct[1][1][ci] +
+                          (R)a.ct[1][1][cxm]));
+  if constexpr (NDIM == 3) {
+    const int czm = ci + nxy * (wrapi(k - 1, nz) - k);
+    // Ex at (i, j-1/2, k-1/2): e[x][z] = ct[2][1], e[x][y] = ct[1][0]
+    a.Ee[0][c] = (CTT)(w * ((R)a.ct[2][1][ci] + (R)a.ct[2][1][cym] + (R)a.ct[1][0][ci] +
+                            (R)a.ct[1][0][czm]));
+    // Ey at (i-1/2, j, k-1/2): e[y][x] = ct[0][1], e[y][z] = ct[2][0]
+    a.Ee[1][c] = (CTT)(w * ((R)a.ct[0][1][ci] + (R)a.ct[0][1][czm] + (R)a.ct[2][0][ci] +
+                            (R)a.ct[2][0][cxm]));
   }
 }
 

@@ -94,7 +94,9 @@ static void run_stage(const StageArgs<CTT>& a, const GridDims& gd, int seg, cuda
   const unsigned nb = (unsigned)((gd.n + 255) / 256);
   if constexpr (PHYS != PHYS_HD) {
     pre();
-    if constexpr (NDIM == 3 && (sizeof(RT) == 8 || five_point<LIM>())) {  // plane-staged EMF
+    if constexpr (CT == CT_ARITH) {
+      emf_arith_kernel<NDIM, RT, CTT><<<nb, 256, 0, s>>>(a, g);
+    } else if constexpr (NDIM == 3 && (sizeof(RT) == 8 || five_point<LIM>())) {  // plane-staged EMF
       using T = EmfTile<LIM, CTT>;
       cudaFuncSetAttribute(emf_tile_kernel<LIM, RT, CTT>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, T::SMEM);
@@ -150,6 +152,15 @@ static int by_lim(const StageArgs<CTT>& a, const GridDims& g, int lim, int seg, 
 template <int NDIM>
 static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey& k, int seg,
                      cudaStream_t s, cudaEvent_t* ev) {
+  if (k.physics == PHYS_MHD && k.ct == CT_ARITH) {
+    if (k.riemann == RS_HLLD)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_HLLD, CT_ARITH>(a, g, k.limiter, seg, s, ev);
+    if (k.riemann == RS_HLL)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_HLL, CT_ARITH>(a, g, k.limiter, seg, s, ev);
+    if (k.riemann == RS_TVDLF)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_TVDLF, CT_ARITH>(a, g, k.limiter, seg, s, ev);
+    return -1;
+  }
   if (k.physics == PHYS_MHD) {
     if (k.riemann == RS_HLLD && k.ct == CT_UCT_HLLD)
       return by_lim<PHYS_MHD, 8, NDIM, RS_HLLD, CT_UCT_HLLD>(a, g, k.limiter, seg, s, ev);

@@ -57,8 +57,9 @@ enum { GP_LIM_FLAT = 0, GP_LIM_MINMOD = 1, GP_LIM_VANLEER = 2, GP_LIM_MC = 3,
 /* [Solver] in pluto.ini (Src/MHD/set_solver.cpp:35-47); tvdlf for MHD (with
    UCT_HLL) and HD */
 enum { GP_RS_HLL = 0, GP_RS_HLLC = 1, GP_RS_HLLD = 2, GP_RS_TVDLF = 3 };
-/* CT_EMF_AVERAGE (Src/MHD/CT/ct.hpp:19-27) */
-enum { GP_CT_UCT_HLL = 0, GP_CT_UCT_HLLD = 1 };
+/* CT_EMF_AVERAGE (Src/MHD/CT/ct.hpp:19-27): upwind UCT_HLL / UCT_HLLD, or the
+   ARITHMETIC average of the face EMFs (MHD) */
+enum { GP_CT_UCT_HLL = 0, GP_CT_UCT_HLLD = 1, GP_CT_ARITHMETIC = 2 };
 /* [Boundary] types (Src/boundary.cpp:144-310; the reference's values,
    Src/gpluto.hpp:205-212, except periodic): outflow (zero-gradient ghost
    copy, OutflowBoundary Src/boundary.cpp:677-780), reflective,

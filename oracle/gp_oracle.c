@@ -1128,6 +1128,13 @@ static void Sweep(orc_t *o, int dir, double dt) {
         if (o->c.solver == ORC_HLLD)       cmax[i] = MHD_HLLD(o, dir, vl, vr, f, e, Bn[i]);
         else if (o->c.solver == ORC_TVDLF) cmax[i] = MHD_TVDLF(o, dir, vl, vr, f, e);
         else                               cmax[i] = MHD_HLL(o, dir, vl, vr, f, e);
+        if (o->c.ct == ORC_ARITHMETIC) {
+          /* CT_Store_Arith, Src/MHD/CT/ct_store.hpp:74-93 (replaces the
+             UCT data the solver stored) */
+          int DIRt = (dir+1)%3, DIRb = (dir+2)%3;
+          o->e[DIRb][dir][e] = -f[BX1 + DIRt];
+          o->e[DIRt][dir][e] =  f[BX1 + DIRb];
+        }
       } else if (o->c.physics == ORC_HD) {
         if (o->c.solver == ORC_HLLC)       cmax[i] = HD_HLLC(o, dir, vl, vr, f);
         else if (o->c.solver == ORC_TVDLF) cmax[i] = HD_TVDLF(o, dir, vl, vr, f);
@@ -1230,6 +1237,25 @@ static void ComputeEMF(orc_t *o) {
   double *bL = o->pqL, *bR = o->pqR, *vL = o->pvL, *vR = o->pvR;   /* scratch */
   double *qL2 = o->pflux, *qR2 = o->pcmax;
   (void)vL; (void)vR;
+
+  if (o->c.ct == ORC_ARITHMETIC) {
+    /* CT_EMF_ArithmeticAverage (Src/MHD/CT/ct_emf_average.cpp:36-96),
+       w = 0.25, each edge from the four face EMFs around it */
+    const double w = 0.25;
+    for (k = kb; k <= ke; k++)
+    for (j = jb; j <= je; j++)
+    for (i = ib; i <= ie; i++) {
+      o->Ee[2][EI(o,i,j,k)] = w*(  o->e[2][0][EI(o,i,j,k)] + o->e[2][0][EI(o,i,j-1,k)]
+                                 + o->e[2][1][EI(o,i,j,k)] + o->e[2][1][EI(o,i-1,j,k)]);
+      if (ndim == 3) {
+        o->Ee[0][EI(o,i,j,k)] = w*(  o->e[0][2][EI(o,i,j,k)] + o->e[0][2][EI(o,i,j-1,k)]
+                                   + o->e[0][1][EI(o,i,j,k)] + o->e[0][1][EI(o,i,j,k-1)]);
+        o->Ee[1][EI(o,i,j,k)] = w*(  o->e[1][0][EI(o,i,j,k)] + o->e[1][0][EI(o,i,j,k-1)]
+                                   + o->e[1][2][EI(o,i,j,k)] + o->e[1][2][EI(o,i-1,j,k)]);
+      }
+    }
+    return;
+  }
 
   /* X1a: By and -vx along x -> Ez at (i-1/2, j-1/2, k) */
   for (k = kb; k <= ke; k++)

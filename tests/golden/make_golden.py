@@ -208,6 +208,18 @@ CASES = {
                                  dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
                                       ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
                                       reconstruction="WENOZ"), 6),
+    # CT_EMF_AVERAGE ARITHMETIC (face EMFs from the induction fluxes)
+    "mhd2d_mc_hlld_arith": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=181),
+                            dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",
+                                 ct_emf="ARITHMETIC", cfl=0.4, first_dt=1e-4), 12),
+    "mhd3d_vl_hll_arith_outflowy": (
+        ics.mhd3d_turbulence, dict(n=(12, 10, 9), seed=182),
+        dict(physics="MHD", ndim=3, limiter="VANLEER_LIM", solver="hll", ct_emf="ARITHMETIC",
+             cfl=0.4, first_dt=1e-4, bc=("periodic", "outflow", "periodic")), 6),
+    "mhd2d_ppm_tvdlf_arith": (ics.mhd2d_turbulence, dict(n=(22, 18), seed=183),
+                              dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="tvdlf",
+                                   ct_emf="ARITHMETIC", cfl=0.4, first_dt=1e-4,
+                                   reconstruction="PARABOLIC"), 10),
     # the Lax-Friedrichs (tvdlf) solver, MHD with UCT_HLL face data and HD
     "mhd2d_mc_tvdlf_ucthll": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=161),
                               dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="tvdlf",

@@ -12,7 +12,8 @@ GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 LIMITER = {"MC_LIM": "mc", "VANLEER_LIM": "vl", "MINMOD_LIM": "minmod", "FLAT_LIM": "flat",
            "VANALBADA_LIM": "vanalbada", "OSPRE_LIM": "ospre", "UMIST_LIM": "umist"}
-CT = {"UCT_HLLD": "uct_hlld", "UCT_HLL": "uct_hll", "none": "uct_hll"}
+CT = {"UCT_HLLD": "uct_hlld", "UCT_HLL": "uct_hll", "ARITHMETIC": "arithmetic",
+      "none": "uct_hll"}
 
 
 def names():

@@ -72,6 +72,9 @@ CASES = [
     (ics.mhd2d_turbulence, dict(n=(29, 21), seed=171), "mc", "tvdlf", "uct_hll", 10),
     (ics.mhd3d_blast, dict(n=(13, 12, 11), seed=172, radius=0.25), "vl", "tvdlf", "uct_hll", 6),
     (ics.hd_turbulence, dict(n=(27, 13, 11), seed=173), "ppm", "tvdlf", "uct_hll", 8),
+    # CT_EMF_AVERAGE ARITHMETIC
+    (ics.mhd3d_turbulence, dict(n=(13, 11, 9), seed=191), "mc", "hlld", "arithmetic", 6),
+    (ics.mhd2d_turbulence, dict(n=(27, 19), seed=192), "vl", "tvdlf", "arithmetic", 10),
 ]
 
 
