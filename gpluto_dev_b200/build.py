@@ -29,9 +29,14 @@ BASE = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed
 # count by about a fifth.  These flags touch single precision only, so the FP64
 # accumulation, CT update and con2prim of that form stay IEEE.
 MIXED_FP32 = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
+# The stage kernels are instantiated per form and per physics (GP_PART: 0 HD,
+# 1 MHD, 2 RMHD) in six units that compile in parallel.
 UNITS = [
-    ("gp_launch_fp64.o", "gp_launch.cu", ["-DGP_MIXED=0", "-fmad=false"]),
-    ("gp_launch_mixed.o", "gp_launch.cu", ["-DGP_MIXED=1", *MIXED_FP32]),
+    *[(f"gp_launch_fp64_p{p}.o", "gp_launch.cu", ["-DGP_MIXED=0", f"-DGP_PART={p}", "-fmad=false"])
+      for p in (1, 2, 0)],
+    *[(f"gp_launch_mixed_p{p}.o", "gp_launch.cu", ["-DGP_MIXED=1", f"-DGP_PART={p}", *MIXED_FP32])
+      for p in (1, 2, 0)],
+    ("gp_launch_dispatch.o", "gp_launch_dispatch.cu", []),
     ("gp_api.o", "gp_api.cu", ["-fmad=false"]),
     ("gp_noalloc.o", "gp_noalloc.cu", ["-fmad=false"]),
 ]
@@ -64,7 +69,7 @@ def _deps() -> list:
         os.path.abspath(__file__)]  # the flags live here
 
 
-def build(verbose: bool = False, jobs: int = 3) -> str:
+def build(verbose: bool = False, jobs: int = 0) -> str:
     os.makedirs(OUT, exist_ok=True)
     newest = max(os.path.getmtime(p) for p in _deps())
     procs = []
@@ -80,11 +85,22 @@ def build(verbose: bool = False, jobs: int = 3) -> str:
         cmd = [nvcc(), *ARCH, *BASE, *flags, "-c", os.path.join(CSRC, src), "-o", o]
         if verbose:
             print(" ".join(cmd))
-        procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
-    for cmd, p in procs:
-        out, _ = p.communicate()
-        if p.returncode != 0:
-            raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + out.decode()[-6000:])
+        procs.append(cmd)
+    # at most `jobs` (default: the core count) compilers at a time, largest
+    # units first as listed
+    jobs = jobs or os.cpu_count() or 4
+    running = []
+    for cmd in procs + [None] * jobs:
+        while len(running) >= jobs or (cmd is None and running):
+            c, p = running.pop(0)
+            out, _ = p.communicate()
+            if p.returncode != 0:
+                raise RuntimeError("nvcc failed:\n" + " ".join(c) + "\n" + out.decode()[-6000:])
+            if cmd is not None:
+                break
+        if cmd is not None:
+            running.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE,
+                                                  stderr=subprocess.STDOUT)))
     dl = os.path.join(OUT, DLINK)
     if (not os.path.exists(dl)) or os.path.getmtime(dl) < max(os.path.getmtime(o) for o in rdc_objs):
         subprocess.run([nvcc(), *ARCH, "-Xcompiler", "-fPIC", "-dlink", *rdc_objs, "-o", dl],

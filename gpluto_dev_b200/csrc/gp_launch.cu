@@ -13,17 +13,26 @@
 #ifndef GP_MIXED
 #define GP_MIXED 0
 #endif
+// GP_PART selects the physics this unit instantiates (0 HD, 1 MHD, 2 RMHD:
+// the PHYS_* values), so that the build compiles the three in parallel; the
+// per-physics entry points launch_stage_{fp64,mixed}_p<part> are joined by
+// gp_launch_dispatch.cu.
+#ifndef GP_PART
+#error "compile gp_launch.cu with -DGP_PART=0, 1 or 2"
+#endif
+#define GP_CAT2(a, b) a##b
+#define GP_CAT(a, b) GP_CAT2(a, b)
 
 namespace gp {
 
 #if GP_MIXED
 using RT = float;
 using CTT = float;
-#define GP_LAUNCH_STAGE launch_stage_mixed
+#define GP_LAUNCH_STAGE GP_CAT(launch_stage_mixed_p, GP_PART)
 #else
 using RT = double;
 using CTT = double;
-#define GP_LAUNCH_STAGE launch_stage_fp64
+#define GP_LAUNCH_STAGE GP_CAT(launch_stage_fp64_p, GP_PART)
 #endif
 
 static StageArgs<CTT> make_args(const StageDesc& d) {
@@ -152,6 +161,7 @@ static int by_lim(const StageArgs<CTT>& a, const GridDims& g, int lim, int seg, 
 template <int NDIM>
 static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey& k, int seg,
                      cudaStream_t s, cudaEvent_t* ev) {
+#if GP_PART == 1
   if (k.physics == PHYS_MHD && k.ct == CT_ARITH) {
     if (k.riemann == RS_HLLD)
       return by_lim<PHYS_MHD, 8, NDIM, RS_HLLD, CT_ARITH>(a, g, k.limiter, seg, s, ev);
@@ -172,6 +182,8 @@ static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey
       return by_lim<PHYS_MHD, 8, NDIM, RS_TVDLF, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
     return -1;
   }
+#endif
+#if GP_PART == 2
   if (k.physics == PHYS_RMHD) {
     if (k.riemann == RS_HLLD && k.ct == CT_UCT_HLL)
       return by_lim<PHYS_RMHD, 8, NDIM, RS_HLLD, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
@@ -179,6 +191,8 @@ static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey
       return by_lim<PHYS_RMHD, 8, NDIM, RS_HLL, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
     return -1;
   }
+#endif
+#if GP_PART == 0
   if (k.physics == PHYS_HD) {
     if (k.riemann == RS_HLLC) return by_lim<PHYS_HD, 5, NDIM, RS_HLLC, 0>(a, g, k.limiter, seg, s, ev);
     if (k.riemann == RS_HLL) return by_lim<PHYS_HD, 5, NDIM, RS_HLL, 0>(a, g, k.limiter, seg, s, ev);
@@ -186,6 +200,7 @@ static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey
       return by_lim<PHYS_HD, 5, NDIM, RS_TVDLF, 0>(a, g, k.limiter, seg, s, ev);
     return -1;
   }
+#endif
   return -1;
 }
 
@@ -197,7 +212,7 @@ int GP_LAUNCH_STAGE(const StageDesc& d, const GridDims& g, const SchemeKey& k, i
   return -1;
 }
 
-#if !GP_MIXED
+#if !GP_MIXED && GP_PART == 1
 int launch_prim2cons(int physics, const double* V, double* U, long long n, double gamma,
                      cudaStream_t s) {
   const unsigned nb = (unsigned)((n + 255) / 256);

@@ -1,0 +1,37 @@
+// gp_launch_dispatch.cu -- joins the per-physics launch units of
+// gp_launch.cu (compiled once per form and physics, GP_MIXED x GP_PART).
+#include "gp_launch.h"
+
+namespace gp {
+
+#define GP_PART_DECL(name)                                                              \
+  int name(const StageDesc& d, const GridDims& g, const SchemeKey& k, int seg,         \
+           cudaStream_t s, cudaEvent_t* ev);
+GP_PART_DECL(launch_stage_fp64_p0)
+GP_PART_DECL(launch_stage_fp64_p1)
+GP_PART_DECL(launch_stage_fp64_p2)
+GP_PART_DECL(launch_stage_mixed_p0)
+GP_PART_DECL(launch_stage_mixed_p1)
+GP_PART_DECL(launch_stage_mixed_p2)
+
+int launch_stage_fp64(const StageDesc& d, const GridDims& g, const SchemeKey& k, int seg,
+                      cudaStream_t s, cudaEvent_t* ev) {
+  switch (k.physics) {
+    case 0: return launch_stage_fp64_p0(d, g, k, seg, s, ev);
+    case 1: return launch_stage_fp64_p1(d, g, k, seg, s, ev);
+    case 2: return launch_stage_fp64_p2(d, g, k, seg, s, ev);
+    default: return -1;
+  }
+}
+
+int launch_stage_mixed(const StageDesc& d, const GridDims& g, const SchemeKey& k, int seg,
+                       cudaStream_t s, cudaEvent_t* ev) {
+  switch (k.physics) {
+    case 0: return launch_stage_mixed_p0(d, g, k, seg, s, ev);
+    case 1: return launch_stage_mixed_p1(d, g, k, seg, s, ev);
+    case 2: return launch_stage_mixed_p2(d, g, k, seg, s, ev);
+    default: return -1;
+  }
+}
+
+}  // namespace gp
