@@ -643,8 +643,6 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   }
   if (scheme->physics == GP_MHD && scheme->riemann == GP_RS_HLLC)
     return fail(GP_ERR_UNSUPPORTED, "MHD HLLC not built");
-  if (scheme->riemann == GP_RS_TVDLF && scheme->physics == GP_RMHD)
-    return fail(GP_ERR_UNSUPPORTED, "RMHD tvdlf not built");
   if (scheme->riemann == GP_RS_TVDLF && scheme->physics == GP_MHD &&
       scheme->ct_emf == GP_CT_UCT_HLLD)
     return fail(GP_ERR_UNSUPPORTED, "tvdlf needs UCT_HLL (Src/MHD/tvdlf.cpp:83-87)");

@@ -189,6 +189,8 @@ static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey
       return by_lim<PHYS_RMHD, 8, NDIM, RS_HLLD, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
     if (k.riemann == RS_HLL && k.ct == CT_UCT_HLL)
       return by_lim<PHYS_RMHD, 8, NDIM, RS_HLL, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
+    if (k.riemann == RS_TVDLF && k.ct == CT_UCT_HLL)
+      return by_lim<PHYS_RMHD, 8, NDIM, RS_TVDLF, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
     return -1;
   }
 #endif

@@ -576,9 +576,19 @@ __device__ __forceinline__ R rmhd_riemann(const R* vl, const R* vr, R* flux, R g
     }
     Sl = GP_MIN(cmn[0], cmn[1]);
     Sr = GP_MAX(cmx[0], cmx[1]);
+    if constexpr (RS == RS_TVDLF) {
+      // Src/RMHD/tvdlf.cpp: the larger of the two states' bounds, Sl = -cmax
+      const R cL = GP_MAX(rabs(cmx[0]), rabs(cmn[0])), cR = GP_MAX(rabs(cmx[1]), rabs(cmn[1]));
+      Sr = GP_MAX(cL, cR);
+      Sl = -Sr;
+    }
   }
-  const R cmax = GP_MAX(rabs(Sl), rabs(Sr));
-  if constexpr (RS != RS_HLLD) {  // Src/RMHD/hll.cpp:180-202
+  const R cmax = RS == RS_TVDLF ? Sr : GP_MAX(rabs(Sl), rabs(Sr));
+  if constexpr (RS == RS_TVDLF) {  // Lax-Friedrichs flux
+#pragma unroll
+    for (int nv = 0; nv < 8; nv++)
+      flux[nv] = R(0.5) * (fl[nv] + fr[nv]) - R(0.5) * cmax * (ur[nv] - ul[nv]);
+  } else if constexpr (RS != RS_HLLD) {  // Src/RMHD/hll.cpp:180-202
     R bL = GP_MIN(Sl, R(0)), bR = GP_MAX(R(0), Sr);
     R scrh = R(1) / (bR - bL);
 #pragma unroll

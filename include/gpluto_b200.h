@@ -55,7 +55,7 @@ enum { GP_HD = 0, GP_MHD = 1, GP_RMHD = 2 };
 enum { GP_LIM_FLAT = 0, GP_LIM_MINMOD = 1, GP_LIM_VANLEER = 2, GP_LIM_MC = 3,
        GP_LIM_VANALBADA = 6, GP_LIM_OSPRE = 7, GP_LIM_UMIST = 8 };
 /* [Solver] in pluto.ini (Src/MHD/set_solver.cpp:35-47); tvdlf for MHD (with
-   UCT_HLL) and HD */
+   UCT_HLL or ARITHMETIC), RMHD and HD */
 enum { GP_RS_HLL = 0, GP_RS_HLLC = 1, GP_RS_HLLD = 2, GP_RS_TVDLF = 3 };
 /* CT_EMF_AVERAGE (Src/MHD/CT/ct.hpp:19-27): upwind UCT_HLL / UCT_HLLD, or the
    ARITHMETIC average of the face EMFs (MHD) */

@@ -208,6 +208,10 @@ CASES = {
                                  dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="hlld",
                                       ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4,
                                       reconstruction="WENOZ"), 6),
+    "rmhd3d_mc_tvdlf_ucthll": (ics.rmhd3d_turbulence, dict(n=(10, 8, 8), seed=165,
+                                                           lorentz_max=5.0),
+                               dict(physics="RMHD", ndim=3, limiter="MC_LIM", solver="tvdlf",
+                                    ct_emf="UCT_HLL", cfl=0.3, first_dt=1e-4), 6),
     # CT_EMF_AVERAGE ARITHMETIC (face EMFs from the induction fluxes)
     "mhd2d_mc_hlld_arith": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=181),
                             dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",

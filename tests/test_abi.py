@@ -55,7 +55,7 @@ def test_create_rejects_bad_configs_before_touching_the_device():
     assert L.gp_create(ctypes.byref(g), ctypes.byref(s), None, ctypes.byref(h)) == -2
     s = api.Scheme(riemann="tvdlf", ct_emf="uct_hlld").to_c()   # tvdlf needs UCT_HLL
     assert L.gp_create(ctypes.byref(g), ctypes.byref(s), None, ctypes.byref(h)) == -2
-    s = api.Scheme(physics=api.RMHD, riemann="tvdlf", ct_emf="uct_hll").to_c()
+    s = api.Scheme(physics=api.RMHD, riemann="hllc", ct_emf="uct_hll").to_c()
     assert L.gp_create(ctypes.byref(g), ctypes.byref(s), None, ctypes.byref(h)) == -2
 
 
