@@ -53,8 +53,9 @@ def test_create_rejects_bad_configs_before_touching_the_device():
     g.nint[2] = 1
     s.rk_stages = 4                       # RK4 is not built
     assert L.gp_create(ctypes.byref(g), ctypes.byref(s), None, ctypes.byref(h)) == -2
-    s = api.Scheme(riemann="tvdlf", ct_emf="uct_hlld").to_c()   # tvdlf needs UCT_HLL
-    assert L.gp_create(ctypes.byref(g), ctypes.byref(s), None, ctypes.byref(h)) == -2
+    for rs in ("tvdlf", "hll"):           # UCT_HLLD pairs with hlld only
+        s = api.Scheme(riemann=rs, ct_emf="uct_hlld").to_c()
+        assert L.gp_create(ctypes.byref(g), ctypes.byref(s), None, ctypes.byref(h)) == -2
     s = api.Scheme(physics=api.RMHD, riemann="hllc", ct_emf="uct_hll").to_c()
     assert L.gp_create(ctypes.byref(g), ctypes.byref(s), None, ctypes.byref(h)) == -2
 
