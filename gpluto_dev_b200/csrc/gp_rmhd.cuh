@@ -8,9 +8,11 @@
 // pressure-fix bisection fallback (Src/RMHD/rmhd_pressure_fix.cpp).
 // Expressions keep the reference's operation order.  The conservative ->
 // primitive inversion always runs in FP64 (also inside the Riemann solver of
-// the mixed form); acos/cos/sin are CUDA's, so the FP64 form agrees with the
-// reference to round-off rather than bit for bit.
+// the mixed form).  The quartic's acos/cos/sin are correctly rounded
+// (gp_crmath.cuh), so the FP64 form matches the reference wherever glibc's
+// results are correctly rounded too.
 #pragma once
+#include "gp_crmath.cuh"
 #include "gp_phys.cuh"
 
 namespace gp {
@@ -80,7 +82,9 @@ __device__ __forceinline__ void rmhd_flux(const R* v, const R* u, R h, R* flux, 
   flux[MXn] += pt;
 }
 
-// Src/RMHD/rmhd.hpp:390-452 (acos/cos/sin: CUDA's libdevice functions)
+// Src/RMHD/rmhd.hpp:390-452 (acos/cos/sin correctly rounded: the roots feed
+// discontinuous decisions, so they follow the reference's glibc results bit
+// for bit except where glibc itself is not correctly rounded)
 __device__ __forceinline__ void cubic_solve(double b, double c, double d, double* z) {
   const double one_3 = 1.0 / 3.0, one_27 = 1.0 / 27.0, sqrt3 = sqrt(3.0);
   double b2 = b * b;
@@ -91,9 +95,9 @@ __device__ __forceinline__ void cubic_solve(double b, double c, double d, double
   double arg = -1.5 * R_ / (Q * sQ);
   arg = GP_MAX(-1.0, arg);
   arg = GP_MIN(1.0, arg);
-  double theta = acos(arg) * one_3;
+  double theta = gpcr::acos_cr(arg) * one_3;   // in [0, pi/3]
   double sn, cs;
-  sincos(theta, &sn, &cs);  // one range reduction for both
+  gpcr::sincos_cr(theta, &sn, &cs);
   sn = sqrt3 * sn;
   double p = -b * one_3;
   z[0] = -sQ * (cs + sn) + p;

@@ -18,6 +18,7 @@
  * the committed fixtures in tests/golden/.
  */
 #include <math.h>
+#include <quadmath.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>

@@ -39,6 +39,7 @@ double   orc_step(void *h, double dt, uint32_t *err);
 double   orc_next_dt(double invDt_hyp, double cfl, double cfl_max_var, double dt);
 uint32_t orc_run(void *h, int nsteps, double first_dt, double *dt_hist);
 void     orc_set_ulp_nudge(int n);
+void     orc_set_cr_trig(int on);
 void     orc_set_rmhd_strict(int on);
 void     orc_prim_to_cons(int physics, double gamma, long ncell, const double *V, double *U);
 #endif

@@ -79,6 +79,12 @@ def set_ulp_nudge(n: int) -> None:
     lib().orc_set_ulp_nudge(int(n))
 
 
+def set_cr_trig(on: bool) -> None:
+    """Checker knob: correctly rounded acos/cos/sin in the RMHD quartic
+    (binary128 evaluation rounded once) instead of the C library's."""
+    lib().orc_set_cr_trig(1 if on else 0)
+
+
 def set_rmhd_strict(on: bool) -> None:
     """Checker knob: fail the RMHD HLLD star state when a Riemann state cannot
     be built (the rule the GPU kernels use); off reproduces the reference."""
