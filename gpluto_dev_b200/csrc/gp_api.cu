@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/gpluto_b200.h"
+#include "gp_checks.h"
 #include "gp_launch.h"
 
 namespace {
@@ -598,21 +599,9 @@ int check_device() {
 
 namespace gp {
 int set_last_error(int code, const char* msg) { return fail(code, "%s", msg); }
-}  // namespace gp
 
-extern "C" {
-
-const char* gp_last_error(void) { return g_err; }
-
-double gp_next_time_step(double invDt_hyp, double cfl, double cfl_max_var, double dt) {
-  double dt_new = cfl / invDt_hyp;
-  return (dt_new <= cfl_max_var * dt) ? dt_new : cfl_max_var * dt;
-}
-
-int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
-              gp_handle** out) {
-  if (!grid || !scheme || !out) return fail(GP_ERR_INVALID, "null argument");
-  *out = nullptr;
+int validate_scheme(const gp_grid_desc* grid, const gp_scheme* scheme) {
+  if (!grid || !scheme) return fail(GP_ERR_INVALID, "null argument");
   if (grid->ndim != 2 && grid->ndim != 3) return fail(GP_ERR_UNSUPPORTED, "ndim must be 2 or 3");
   if (scheme->physics != GP_MHD && scheme->physics != GP_HD && scheme->physics != GP_RMHD)
     return fail(GP_ERR_UNSUPPORTED, "physics %d not built", scheme->physics);
@@ -674,7 +663,39 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
       if (grid->nint[d] < 4)
         return fail(GP_ERR_INVALID,
                     "PPM, MP5 and WENO-Z need at least 4 cells along each direction");
-  int rc = check_device();
+  return GP_OK;
+}
+
+int cell_widths(const gp_grid_desc* grid, double dx[3]) {
+  for (int d = 0; d < 3; d++) {
+    const int nn = d < grid->ndim ? grid->nint[d] : 1;
+    dx[d] = (grid->dx[d] && d < grid->ndim) ? grid->dx[d][0]
+                                            : (grid->xend[d] - grid->xbeg[d]) / nn;
+    if (!(dx[d] > 0.0)) dx[d] = 1.0;
+  }
+  return GP_OK;
+}
+}  // namespace gp
+
+extern "C" {
+
+const char* gp_last_error(void) { return g_err; }
+
+double gp_next_time_step(double invDt_hyp, double cfl, double cfl_max_var, double dt) {
+  double dt_new = cfl / invDt_hyp;
+  return (dt_new <= cfl_max_var * dt) ? dt_new : cfl_max_var * dt;
+}
+
+int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
+              gp_handle** out) {
+  if (!grid || !scheme || !out) return fail(GP_ERR_INVALID, "null argument");
+  *out = nullptr;
+  int rc = gp::validate_scheme(grid, scheme);
+  if (rc) return rc;
+  const bool wide = scheme->reconstruction == GP_REC_PARABOLIC ||
+                    scheme->reconstruction == GP_REC_MP5 ||
+                    scheme->reconstruction == GP_REC_WENOZ;
+  rc = check_device();
   if (rc) return rc;
   gp_handle* h = new (std::nothrow) gp_handle;
   if (!h) return fail(GP_ERR_NOMEM, "host allocation");
@@ -726,12 +747,7 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
   }
   h->nvar = scheme->physics == GP_HD ? 5 : 8;
   h->ng = grid->nghost;
-  for (int d = 0; d < 3; d++) {
-    int nn = (d == 0 ? h->nx : d == 1 ? h->ny : h->nz);
-    h->dx[d] = (grid->dx[d] && d < grid->ndim) ? grid->dx[d][0]
-                                               : (grid->xend[d] - grid->xbeg[d]) / nn;
-    if (!(h->dx[d] > 0.0)) h->dx[d] = 1.0;
-  }
+  gp::cell_widths(grid, h->dx);
   // Cartesian face areas in the reference's operation order
   if (h->ndim == 2) {
     h->A[0] = 1.0 * h->dx[1];

@@ -176,7 +176,7 @@ static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey
       return by_lim<PHYS_MHD, 8, NDIM, RS_HLLD, CT_UCT_HLLD>(a, g, k.limiter, seg, s, ev);
     if (k.riemann == RS_HLLD && k.ct == CT_UCT_HLL)
       return by_lim<PHYS_MHD, 8, NDIM, RS_HLLD, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
-    if (k.riemann == RS_HLL)
+    if (k.riemann == RS_HLL && k.ct == CT_UCT_HLL)
       return by_lim<PHYS_MHD, 8, NDIM, RS_HLL, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
     if (k.riemann == RS_TVDLF && k.ct == CT_UCT_HLL)
       return by_lim<PHYS_MHD, 8, NDIM, RS_TVDLF, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);

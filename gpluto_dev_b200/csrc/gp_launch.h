@@ -54,6 +54,7 @@ int launch_prim2cons(int physics, const double* V, double* U, long long n, doubl
                      cudaStream_t s);
 // Sets the text returned by gp_last_error on this thread; returns `code`.
 int set_last_error(int code, const char* msg);
+
 // Number of kernel launches one stage issues for this scheme, and their names.
 int stage_launch_count(const SchemeKey& k);
 const char* stage_kernel_name(const SchemeKey& k, int idx);

@@ -21,6 +21,7 @@
 #include <mutex>
 
 #include "../../include/gpluto_b200.h"
+#include "gp_checks.h"
 #include "gp_launch.h"
 
 namespace {
@@ -72,41 +73,37 @@ extern "C" int gp_advance_step_noalloc(const gp_grid_desc* grid, const gp_scheme
                                        double* Uc, double* Vc, double* Vs0, double* Vs1,
                                        double* Vs2, double dt, void* stream,
                                        gp_step_out* out) {
-  if (!grid || !scheme || !Uc || !Vc) return GP_ERR_INVALID;
-  if (grid->ndim != 2 && grid->ndim != 3) return GP_ERR_UNSUPPORTED;
-  if (scheme->rk_stages != 2) return GP_ERR_UNSUPPORTED;
+  if (!grid || !scheme || !Uc || !Vc) return gp::set_last_error(GP_ERR_INVALID, "null argument");
+  // the combinations gp_create accepts, then this entry point's own limits
+  int rc = gp::validate_scheme(grid, scheme);
+  if (rc) return rc;
+  if (scheme->rk_stages != 2)
+    return gp::set_last_error(GP_ERR_UNSUPPORTED, "the no-allocation step is RK2 only");
   if (scheme->reconstruction != GP_REC_LINEAR && scheme->reconstruction != GP_REC_PARABOLIC)
-    return GP_ERR_UNSUPPORTED;
-  if (scheme->reconstruction == GP_REC_LINEAR &&
-      !((scheme->limiter >= GP_LIM_FLAT && scheme->limiter <= GP_LIM_MC) ||
-        (scheme->limiter >= GP_LIM_VANALBADA && scheme->limiter <= GP_LIM_UMIST)))
-    return GP_ERR_UNSUPPORTED;
-  if (scheme->physics != GP_HD && scheme->physics != GP_MHD && scheme->physics != GP_RMHD)
-    return GP_ERR_UNSUPPORTED;
-  if (scheme->precision != GP_FP64 && scheme->precision != GP_MIXED) return GP_ERR_INVALID;
-  if (!(dt > 0.0)) return GP_ERR_INVALID;
+    return gp::set_last_error(GP_ERR_UNSUPPORTED,
+                              "the no-allocation step takes LINEAR or PARABOLIC reconstruction");
+  if (!(dt > 0.0)) return gp::set_last_error(GP_ERR_INVALID, "dt must be positive");
   const int ndim = grid->ndim;
   const int nx = grid->nint[0], ny = grid->nint[1], nz = ndim == 3 ? grid->nint[2] : 1;
-  if (nx < 2 || ny < 2 || (ndim == 3 && nz < 2)) return GP_ERR_INVALID;
   const long long n = (long long)nx * ny * nz;
-  if (n > kMaxCells) return GP_ERR_INVALID;  // larger than the static scratch
+  if (n > kMaxCells)
+    return gp::set_last_error(GP_ERR_INVALID,
+                              "grid larger than GP_NOALLOC_MAX_CELLS (the static scratch)");
   const bool mhd = scheme->physics != GP_HD;
-  if (mhd && (!Vs0 || !Vs1 || (ndim == 3 && !Vs2))) return GP_ERR_INVALID;
+  if (mhd && (!Vs0 || !Vs1 || (ndim == 3 && !Vs2)))
+    return gp::set_last_error(GP_ERR_INVALID, "null face-field pointer");
   for (int d = 0; d < ndim; d++)
     if (grid->lbound[d] != GP_BC_PERIODIC || grid->rbound[d] != GP_BC_PERIODIC)
-      return GP_ERR_UNSUPPORTED;
+      return gp::set_last_error(GP_ERR_UNSUPPORTED,
+                                "the no-allocation step takes periodic sides only");
 
   double* base = nullptr;
-  int rc = scratch_address(&base);
-  if (rc) return rc;
+  rc = scratch_address(&base);
+  if (rc) return gp::set_last_error(rc, "cannot find the scratch array on this device");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
 
   double dx[3];
-  for (int d = 0; d < 3; d++) {
-    const int nn = d == 0 ? nx : d == 1 ? ny : nz;
-    dx[d] = (grid->xend[d] - grid->xbeg[d]) / nn;
-    if (!(dx[d] > 0.0)) dx[d] = 1.0;
-  }
+  gp::cell_widths(grid, dx);
   // carve the scratch
   Scalars* sc = reinterpret_cast<Scalars*>(base);
   double* p = base + kHeader;
@@ -157,7 +154,6 @@ extern "C" int gp_advance_step_noalloc(const gp_grid_desc* grid, const gp_scheme
   }
   gp::GridDims g{nx, ny, nz, n};
   const bool ppm = scheme->reconstruction == GP_REC_PARABOLIC;
-  if (ppm && (nx < 4 || ny < 4 || (ndim == 3 && nz < 4))) return GP_ERR_INVALID;
   gp::SchemeKey key{scheme->physics, ndim, scheme->riemann, scheme->ct_emf,
                     ppm ? 4 /* LIM_PPM */ : scheme->limiter};
   int seg = 64;
@@ -179,7 +175,7 @@ extern "C" int gp_advance_step_noalloc(const gp_grid_desc* grid, const gp_scheme
     d.Bs0[q] = d.Bs[q];
     d.Bsout[q] = (mhd && q < ndim) ? B1[q] : nullptr;
   }
-  if (launch(d) != 0) return GP_ERR_UNSUPPORTED;
+  if (launch(d) != 0) return gp::set_last_error(GP_ERR_UNSUPPORTED, "scheme not built");
   // stage 2: (U, U1, B, B1) -> (U in place, B2), then B2 -> caller's B
   d.stage = 2;
   d.w0 = d.w1 = d.wr = 0.5;  // RK2 (Src/rk_step.cpp:30-35)
@@ -190,13 +186,14 @@ extern "C" int gp_advance_step_noalloc(const gp_grid_desc* grid, const gp_scheme
     d.Bs0[q] = (mhd && q < ndim) ? Bn[q] : nullptr;
     d.Bsout[q] = (mhd && q < ndim) ? B2[q] : nullptr;
   }
-  if (launch(d) != 0) return GP_ERR_UNSUPPORTED;
+  if (launch(d) != 0) return gp::set_last_error(GP_ERR_UNSUPPORTED, "scheme not built");
   if (mhd)
     for (int q = 0; q < ndim; q++)
       if (cudaMemcpyAsync(Bn[q], B2[q], sizeof(double) * n, cudaMemcpyDeviceToDevice, s) !=
           cudaSuccess)
         return GP_ERR_CUDA;
-  if (cudaGetLastError() != cudaSuccess) return GP_ERR_CUDA;
+  // launch failures show here; peeking leaves the thread's error state as it is
+  if (cudaPeekAtLastError() != cudaSuccess) return gp::set_last_error(GP_ERR_CUDA, "launch failed");
   if (cudaMemcpyAsync(&hs, sc, sizeof(hs), cudaMemcpyDeviceToHost, s) != cudaSuccess)
     return GP_ERR_CUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return GP_ERR_CUDA;
