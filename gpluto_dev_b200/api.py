@@ -25,6 +25,7 @@ LIB_PATH = os.environ.get("GPLUTO_B200_LIB") or os.path.join(_HERE, "_build",
                                                              "libgpluto_b200.so")
 
 GP_OK, GP_ERR_INVALID, GP_ERR_QUIT, GP_ERR_NO_DEVICE, GP_ERR_IO = 0, -1, -5, -6, -7
+GP_ERR_UNSUPPORTED, GP_ERR_CUDA, GP_ERR_TIMEOUT = -2, -3, -8
 BC_PERIODIC, BC_OUTFLOW, BC_REFLECTIVE, BC_AXISYMMETRIC, BC_EQTSYMMETRIC = 0, 1, 2, 3, 4
 BC_USERDEF = 8
 HD, MHD, RMHD = 0, 1, 2

@@ -53,6 +53,8 @@ def _lib():
         L.gp_batch_set_ctas.argtypes = [P, ctypes.c_int]
         L.gp_batch_advance.argtypes = [P, ctypes.c_int]
         L.gp_batch_wait.argtypes = [P]
+        L.gp_batch_inject_wait_fault.argtypes = [P, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_longlong]
         L.gp_batch_slot_status.argtypes = [P, ctypes.c_int, ctypes.POINTER(GpSlotStatus)]
         L.gp_batch_download.argtypes = [P, ctypes.c_int, D, D, D, D, D]
         L.gp_batch_info.argtypes = [P, ctypes.POINTER(ctypes.c_size_t),
@@ -152,6 +154,13 @@ class Batch:
 
     def wait(self):
         api._check(_lib().gp_batch_wait(self._h))
+
+    def inject_wait_fault(self, slot: int, extra_need: int, spin_limit: int = 0):
+        """Test hook: from the next advance, ``slot``'s finish tiles wait for
+        ``extra_need`` EMF tiles that do not exist and a wait gives up after
+        ``spin_limit`` polls (0: the default limit); wait() then raises
+        GPError(GP_ERR_TIMEOUT).  extra_need 0 removes the fault."""
+        api._check(_lib().gp_batch_inject_wait_fault(self._h, slot, extra_need, spin_limit))
 
     def status(self, slot: int) -> SlotStatus:
         st = GpSlotStatus()

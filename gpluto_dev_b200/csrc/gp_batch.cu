@@ -32,6 +32,7 @@ namespace gp {
 namespace {
 
 constexpr long long kSpinLimit = 1LL << 22;  // ~0.3 us per poll: about a second
+constexpr uint32_t kErrWaitRanOut = 1u;      // batch error word: a wait gave up
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -86,13 +87,14 @@ __device__ __forceinline__ void batch_loop(const BatchSlot* __restrict__ slots,
     if (threadIdx.x == 0) {
       int go = s.sc->steps_left > 0 && ld_volatile(batch_err) == 0u;
       if (go && PART == 1 && t.phase == BP_FINISH && s.physics != PHYS_HD) {
-        const int need = s.need[BG_EMF];
+        const int need = s.need[BG_EMF] + (t.slot == hdr->bias_slot ? hdr->bias_need : 0);
         const int* c = &ctr->done[t.slot * BG_COUNT + BG_EMF];
+        const long long limit = hdr->spin_limit;
         long long it = 0;
         while (ld_acquire(c) < need) {
           if (ld_volatile(batch_err) != 0u) { go = 0; break; }
-          if (++it > kSpinLimit) {
-            atomicOr(batch_err, 1u);
+          if (++it > limit) {
+            atomicOr(batch_err, kErrWaitRanOut);
             go = 0;
             break;
           }
@@ -226,6 +228,8 @@ struct gp_batch {
   gp::BatchCounters* ctr_d;
   size_t ctr_bytes;
   uint32_t* err_d;
+  long long spin_limit;     // dependency-wait polls (kSpinLimit unless injected)
+  int bias_slot, bias_need; // injected dependency fault (tests), -1 / 0 = none
   BatchScalars* sc_h;  // pinned copy of every slot's scalars
   bool dirty;
   std::map<int, cudaGraphExec_t> graphs;
@@ -353,7 +357,7 @@ int rebuild_tiles(gp_batch* b) {
     b->tiles_cap = cap;
   }
   if (nt) BATCH_CUDA(cudaMemcpy(b->tiles_d, t.data(), sizeof(BatchTile) * nt, cudaMemcpyHostToDevice));
-  gp::BatchTableHeader h{nsweep, nt};
+  gp::BatchTableHeader h{nsweep, nt, b->spin_limit, b->bias_slot, b->bias_need};
   BATCH_CUDA(cudaMemcpy(b->hdr_d, &h, sizeof(h), cudaMemcpyHostToDevice));
   BATCH_CUDA(cudaMemcpy(b->slots_d, b->slots.data(), sizeof(BatchSlot) * b->max_slots,
                         cudaMemcpyHostToDevice));
@@ -408,6 +412,9 @@ int gp_batch_create(size_t pool_bytes, int max_slots, int ctas, void* stream, gp
   gp_batch* b = new (std::nothrow) gp_batch();
   if (!b) return gp::fail(GP_ERR_NOMEM, "host allocation");
   b->max_slots = max_slots;
+  b->spin_limit = gp::kSpinLimit;
+  b->bias_slot = -1;
+  b->bias_need = 0;
   b->slots.assign(max_slots, BatchSlot{});
   b->used.assign(max_slots, 0);
   b->off.assign(max_slots, 0);
@@ -673,7 +680,25 @@ int gp_batch_wait(gp_batch* b) {
       BATCH_CUDA(cudaMemcpyAsync(&b->sc_h[i], b->slots[i].sc, sizeof(BatchScalars),
                                  cudaMemcpyDeviceToHost, b->stream));
   BATCH_CUDA(cudaStreamSynchronize(b->stream));
-  if (err) return gp::fail(GP_ERR_CUDA, "a batched stage gave up waiting on a dependency");
+  if (err) {
+    // the report consumes the error word; the slots that were advancing when
+    // a wait ran out hold a partly updated state (remove or re-admit them)
+    BATCH_CUDA(cudaMemset(b->err_d, 0, sizeof(uint32_t)));
+    return gp::fail(GP_ERR_TIMEOUT, "a batched stage gave up waiting on a dependency "
+                    "(the EMF tiles of a slot did not complete within the wait limit)");
+  }
+  return GP_OK;
+}
+
+int gp_batch_inject_wait_fault(gp_batch* b, int slot, int extra_need, long long spin_limit) {
+  if (!b || extra_need < 0 || spin_limit < 0 ||
+      (extra_need > 0 && (slot < 0 || slot >= b->max_slots || !b->used[slot])))
+    return gp::fail(GP_ERR_INVALID, "bad arguments");
+  BATCH_CUDA(cudaStreamSynchronize(b->stream));
+  b->bias_slot = extra_need > 0 ? slot : -1;
+  b->bias_need = extra_need;
+  b->spin_limit = spin_limit > 0 ? spin_limit : gp::kSpinLimit;
+  b->dirty = true;  // the next advance rewrites the table header
   return GP_OK;
 }
 

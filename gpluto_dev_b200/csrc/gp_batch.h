@@ -68,6 +68,9 @@ static_assert(sizeof(StageArgs<double>) == sizeof(StageArgs<float>), "StageArgs 
 struct BatchTableHeader {
   int nsweep;
   int ntiles;
+  long long spin_limit;  // polls before a dependency wait gives up
+  int bias_slot;         // fault injection (tests): this slot's EMF count
+  int bias_need;         //   must reach need + bias_need; -1 / 0 = off
 };
 
 // Queue heads of the two launches and per-slot group counters; cleared

@@ -45,7 +45,8 @@ enum gp_status {
   GP_ERR_NOMEM = -4,        /* device allocation failed */
   GP_ERR_QUIT = -5,         /* a kernel raised ERR_QUIT (the reference would QuitPLUTO) */
   GP_ERR_NO_DEVICE = -6,    /* no CUDA device: this library has no CPU path */
-  GP_ERR_IO = -7            /* an output or restart file is missing, short or unwritable */
+  GP_ERR_IO = -7,           /* an output or restart file is missing, short or unwritable */
+  GP_ERR_TIMEOUT = -8       /* a batched stage's bounded dependency wait ran out */
 };
 
 /* PHYSICS (definitions.hpp) */
@@ -257,8 +258,9 @@ int gp_advance_step_noalloc(const gp_grid_desc *grid, const gp_scheme *scheme,
    its own dt sequence (NextTimeStep on the device, exactly as
    gp_advance_steps) and its own step budget; a slot whose budget is spent,
    or that raised ERR_QUIT, stops advancing.  Built schemes: ideal MHD with
-   PLM-MC + HLLD + UCT_HLLD and HD with PLM-MC + HLLC, 2-D and 3-D, FP64 or
-   mixed per slot, periodic boundaries.  The reference advances one grid per
+   PLM-MC + HLLD + UCT_HLLD, relativistic MHD with PLM-MC + HLLD + UCT_HLL
+   (its Riemann solver in FP64 in both forms) and HD with PLM-MC + HLLC,
+   2-D and 3-D, FP64 or mixed per slot, RK2, periodic boundaries.  The reference advances one grid per
    process; this has no reference counterpart beyond the step it repeats.
    --------------------------------------------------------------------- */
 typedef struct gp_batch gp_batch;
@@ -304,8 +306,17 @@ int gp_batch_remove(gp_batch *b, int slot);
 /* Enqueue `nsteps` steps of every slot with budget left (asynchronous; the
    graph for this step count is captured on first use). */
 int gp_batch_advance(gp_batch *b, int nsteps);
-/* Wait for the enqueued steps and refresh every slot's status. */
+/* Wait for the enqueued steps and refresh every slot's status.  Returns
+   GP_ERR_TIMEOUT when a finish tile's bounded wait for its slot's EMF tiles
+   ran out (the launch then skips every later tile and ends; the slots being
+   advanced hold a partly updated state and should be removed); the report
+   clears the condition. */
 int gp_batch_wait(gp_batch *b);
+/* Host-side fault injection for tests (no reference counterpart): from the
+   next gp_batch_advance, slot `slot`'s finish tiles wait for `extra_need`
+   more EMF tiles than exist, and a wait gives up after `spin_limit` polls
+   (0: the default, about a second).  extra_need 0 removes the fault. */
+int gp_batch_inject_wait_fault(gp_batch *b, int slot, int extra_need, long long spin_limit);
 int gp_batch_slot_status(const gp_batch *b, int slot, gp_slot_status *st);
 /* Copy a slot's state to the host (interior layout; any pointer may be NULL). */
 int gp_batch_download(gp_batch *b, int slot, double *Uc, double *Vc, double *Vs0,
