@@ -3,7 +3,8 @@
 Test infrastructure only.  For one scheme configuration this writes a
 ``definitions.hpp``, a ``pluto.ini`` and a short Makefile of our own into
 ``oracle/_ref/<name>/`` and compiles the reference sources in place under
-``/root/reference/Src`` (never copied) together with ``oracle/ref/init.cpp``,
+``$GP_REFERENCE_ROOT/Src`` (never copied; by default the ``reference``
+directory beside this repository) together with ``oracle/ref/init.cpp``,
 using the flags of the reference's serial build ``Config/linux.g++.defs``
 (``g++ -O3 -std=c++17``).  The object lists follow
 ``Src/Templates/default_objects.mk``, ``Src/MHD/makefile``,
@@ -23,8 +24,9 @@ import sys
 
 import numpy as np
 
-REF_ROOT = os.environ.get("GP_REFERENCE_ROOT", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
+REF_ROOT = os.path.abspath(os.environ.get(
+    "GP_REFERENCE_ROOT", os.path.join(HERE, "..", "..", "..", "reference")))
 OUT_ROOT = os.path.join(os.path.dirname(HERE), "_ref")
 
 _DEFAULT_OBJ = """arrays array_reconstruct bin_io boundary cmd_line_opt data2sweep

@@ -1,6 +1,7 @@
 """Generate the golden parity fixtures from the reference gPLUTO serial build.
 
-Run in a container that has the reference tree (default /root/reference):
+Run in a container that has the reference tree (``GP_REFERENCE_ROOT``, by
+default ``../reference`` beside the repository):
 
     python tests/golden/make_golden.py [name ...]
 
