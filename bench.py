@@ -15,10 +15,18 @@ state alone is ~2.5 GB), so no L2 flush is needed between steps.
 Multi-GPU: replicas only (one independent grid per rank, no data-path
 collective); value = zone updates of all ranks / max-over-ranks time.
 
+The default line also carries the CPU baseline (the reference serial build,
+one thread, on this same 256^3 grid: one timed step after one untimed, run
+beside the GPU measurements) and two short legs of the other workloads: the
+batched ensemble (all 512 grids, K steps) and the serving loop (64 requests
+at 8 requests/s: p50/p99 latency and Mzone-updates/s).
+
 ``--impl reference`` times the reference gPLUTO serial build (compiled from
-the reference sources into oracle/_ref by __graft_entry__.build()) on all
-host cores, one independent process per core, each step a bounded sample:
-one RK2 step of a 64^3 grid of the same scheme per process.
+the reference sources into oracle/_ref by __graft_entry__.build()) on this
+same workload, the 256^3 blast: as many concurrent single-thread processes
+as the host's cores and memory hold (at most 16; ~18 GB each), each one
+untimed and one timed RK2 step of the full grid -- a bounded sample, since
+one step takes the reference 40-60 s on one core.
 
 ``--workload ensemble`` (default 200 steps): 512 independent 2-D ideal-MHD
 grids (sides log-uniform 64..512, square and 2:1, half FP64 / half mixed,
@@ -66,7 +74,6 @@ KERNEL_BYTES = {
     ("emf", 1): 192, ("emf", 2): 192,
     ("finish", 1): 384, ("finish", 2): 448,
 }
-REF_SAMPLE_N = 64
 REF_BINARY = os.path.join(ROOT, "oracle", "_ref", "mhd3d_mc_lim_hlld_uct_hlld", "pluto")
 
 
@@ -140,51 +147,73 @@ def _ref_available() -> bool:
     return os.path.exists(REF_BINARY)
 
 
-def run_reference_sample(nproc: int, nsteps_timed: int, nwarm: int, n=REF_SAMPLE_N):
-    """Run `nproc` concurrent reference processes on n^3 blast grids.
+REF_RSS_256 = 18 << 30     # resident bytes of one reference process at 256^3 (measured)
 
-    Returns (Mzone-updates/s aggregate, mean s/step, cores, kind, sample text)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle", "ref"))
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from gpluto_dev_b200 import ics
-    total = nwarm + nsteps_timed
-    if _ref_available():
+
+def _mem_available() -> int:
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+class ReferenceRun:
+    """`nproc` concurrent reference processes (serial build, one thread
+    each), every one advancing the bench's own 256^3 grid: `nwarm` untimed
+    steps, then `ntimed` timed ones (the wall stamps the problem file logs
+    before every step).  Started at construction, collected by result()."""
+
+    def __init__(self, st, nproc: int, nwarm: int, ntimed: int):
+        sys.path.insert(0, os.path.join(ROOT, "oracle", "ref"))
+        from gpluto_dev_b200 import ics
         import build_ref as br
-        cfg = br.RefConfig(name="bench", physics="MHD", ndim=3, n=(n, n, n), limiter="MC_LIM",
-                           solver="hlld", ct_emf="UCT_HLLD", cfl=0.4, first_dt=FIRST_DT)
-        with tempfile.TemporaryDirectory() as tmp:
-            procs = []
-            for r in range(nproc):
-                d = os.path.join(tmp, f"p{r}")
-                os.makedirs(d)
-                open(os.path.join(d, "pluto.ini"), "w").write(cfg.ini())
-                icp = os.path.join(d, "ic.bin")
-                ics.write_ic(icp, ics.mhd3d_blast(n=(n, n, n), seed=1 + r))
-                env = dict(os.environ, GPLUTO_FTZ_DAZ="0", GP_IC_FILE=icp,
-                           GP_DUMP_STEP=str(total + 1), GP_DUMP_FILE=os.path.join(d, "out.dump"))
-                procs.append((d, subprocess.Popen([REF_BINARY, "-no-write", "-maxsteps",
-                                                   str(total + 1)], cwd=d, env=env,
-                                                  stdout=subprocess.DEVNULL,
-                                                  stderr=subprocess.DEVNULL)))
-            per = []
-            for d, p in procs:
-                p.wait()
-                dm = br.read_dump(os.path.join(d, "out.dump"))
-                w = dm.wall
-                per.append((w[nwarm + nsteps_timed] - w[nwarm]) / nsteps_timed)
-        kind = "reference"
-    else:  # C restatement of the reference (oracle port), one process per core
-        import oracle as orc
-        from concurrent.futures import ProcessPoolExecutor
-        import multiprocessing as mp
-        with ProcessPoolExecutor(nproc, mp_context=mp.get_context("spawn")) as ex:
-            per = list(ex.map(_oracle_worker, [(n, total, nwarm, r) for r in range(nproc)]))
-        kind = "port"
-    zones = n ** 3
-    value = sum(zones / t for t in per) / 1e6
-    sample = (f"{nproc} concurrent single-thread processes, each one {n}^3 grid of the same "
-              f"scheme, {nsteps_timed} timed RK2 steps after {nwarm} warm-up")
-    return value, statistics.mean(per), nproc, kind, sample
+        self.br, self.nwarm, self.ntimed, self.ncell = br, nwarm, ntimed, st.ncells
+        total = nwarm + ntimed
+        nx, ny, nz = st.shape
+        cfg = br.RefConfig(name="bench", physics="MHD", ndim=3, n=(nx, ny, nz),
+                           limiter="MC_LIM", solver="hlld", ct_emf="UCT_HLLD", cfl=0.4,
+                           first_dt=FIRST_DT)
+        self.tmp = tempfile.TemporaryDirectory()
+        icp = os.path.join(self.tmp.name, "ic.bin")
+        ics.write_ic(icp, st)
+        self.procs = []
+        for r in range(nproc):
+            d = os.path.join(self.tmp.name, f"p{r}")
+            os.makedirs(d)
+            open(os.path.join(d, "pluto.ini"), "w").write(cfg.ini())
+            env = dict(os.environ, GPLUTO_FTZ_DAZ="0", GP_IC_FILE=icp,
+                       GP_DUMP_STEP=str(total), GP_DUMP_FILE=os.path.join(d, "out.dump"))
+            self.procs.append((d, subprocess.Popen(
+                [REF_BINARY, "-no-write", "-maxsteps", str(total)], cwd=d, env=env,
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)))
+
+    def result(self):
+        """(Mzone-updates/s summed over processes, mean s/step)."""
+        per = []
+        for d, p in self.procs:
+            p.wait()
+            w = self.br.read_dump(os.path.join(d, "out.dump")).wall
+            per.append((w[self.nwarm + self.ntimed] - w[self.nwarm]) / self.ntimed)
+        self.tmp.cleanup()
+        return sum(self.ncell / t for t in per) / 1e6, statistics.mean(per)
+
+
+def reference_processes(cap: int) -> int:
+    """Concurrent 256^3 reference processes the host can hold: one per core,
+    at most `cap`, and no more than 80% of the available memory allows."""
+    cores = os.cpu_count() or 1
+    by_mem = max(1, int(0.8 * _mem_available() // REF_RSS_256))
+    return max(1, min(cores, by_mem, cap))
+
+
+def _oracle_rate(n, nwarm, ntimed):
+    """The oracle port on one n^3 blast grid, one thread (when the reference
+    build is absent)."""
+    t = _oracle_worker((n, nwarm + ntimed, nwarm, 0))
+    return n ** 3 / t / 1e6, t
 
 
 def _oracle_worker(args):
@@ -213,24 +242,39 @@ def config_block(n=N):
 
 
 def impl_reference(args):
+    """The reference serial build on the bench's own workload (the seeded
+    256^3 blast, the same scheme): as many concurrent single-thread
+    processes as the host's cores and memory hold (at most 16), each one
+    untimed step then one timed step -- a bounded sample, since one step of
+    this grid takes the reference about 40-60 s on one core."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    ncores = os.cpu_count() or 1
-    nproc = max(1, min(ncores, 64))
-    value, sps, cores, kind, sample = run_reference_sample(nproc, args.steps, args.warmup)
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+    from gpluto_dev_b200 import ics
+    n = args.n
+    st = ics.mhd3d_blast(n=(n, n, n), seed=1)
+    if _ref_available():
+        nproc = reference_processes(16)
+        v, sps = ReferenceRun(st, nproc, 1, 1).result()
+        kind, cores = "reference", nproc
+        sample = (f"{nproc} concurrent single-thread processes of the reference serial build, "
+                  f"each advancing the {n}^3 blast grid of this workload (seed 1): 1 untimed "
+                  f"RK2 step, then 1 timed step; Mzone-updates/s summed over processes")
+    else:
+        v, sps = _oracle_rate(n, 1, 1)
+        kind, cores = "port", 1
+        sample = f"the C oracle on the {n}^3 blast grid, one thread, 1 timed step after 1"
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC,
+            "n_gpus": args.gpus, "steps": 1, "warmup": 1, "steps_requested": args.steps,
             "ms_per_step": sps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_block(),
-            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind,
+            "config": config_block(n),
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": kind,
                              "sample": sample},
-            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
-
 
 
 def mixed_error(make_solver, nsteps, st):
@@ -330,6 +374,13 @@ def impl_ours(args):
         sch = api.Scheme(physics=api.MHD, precision=precision, gamma=st.gamma, **SCHEME)
         return api.Solver.from_state(st, sch)
 
+    # ---- CPU baseline: the reference serial build on this same grid, one
+    # core, started now so that it runs beside the GPU measurements ------
+    ref_run = None
+    want_cpu = rank == 0 and world == 1 and not args.no_cpu
+    if want_cpu and _ref_available():
+        ref_run = ReferenceRun(st, 1, 1, 1)
+
     # ---- plain FP64 form: timed region ---------------------------------
     s64 = solver(api.FP64)
     dt = FIRST_DT
@@ -380,7 +431,7 @@ def impl_ours(args):
     # ---- mixed FP32-flux form ------------------------------------------
     mixed = None
     if not args.no_mixed:
-        del s64
+        s64 = None
         torch.cuda.empty_cache()
         smx = solver(api.MIXED)
         d2, _, _ = smx.run(args.warmup, FIRST_DT, history=False)
@@ -411,11 +462,36 @@ def impl_ours(args):
     # device -> host download of the same arrays.
     e2e = None if args.no_e2e else measure_e2e(solver, ncell, args.steps, ranks)
 
+    # ---- the other two workloads, short: the batched ensemble (all 512
+    # grids, K steps) and the serving loop (64 requests at one rate) -------
+    legs = {}
+    if world == 1 and not args.no_legs:
+        s64 = None
+        torch.cuda.empty_cache()
+        ens = ensemble_leg(args, ranks, args.steps, 3, with_e2e=False, with_cpu=False)
+        legs["ensemble"] = {k: ens[k] for k in ("value", "unit", "steps", "ms_per_step",
+                                               "roofline", "err_bits", "steps_done_min",
+                                               "ctas")}
+        legs["ensemble"]["workload"] = ens["config"]["workload"]
+        legs["ensemble"]["cells_total"] = ens["config"]["cells_total"]
+        torch.cuda.empty_cache()
+        sweep, table, _, work = serve_leg(args, [SERVE_DEFAULT_RATE], args.requests)
+        legs["serve"] = dict(sweep[0], workload=f"serve_poisson_{args.requests}req",
+                             work_zone_updates=work)
+
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        nproc = max(1, min(os.cpu_count() or 1, 16))
-        v, sps, cores, kind, sample = run_reference_sample(nproc, 2, 1)
-        cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample}
+    if want_cpu:
+        if ref_run is not None:
+            v, sps = ref_run.result()
+            cpu = {"value": v, "unit": METRIC, "cores": 1, "kind": "reference",
+                   "sample": f"the reference serial build (one thread) on this workload's own "
+                             f"{n}^3 grid: 1 untimed RK2 step, then 1 timed step",
+                   "s_per_step": sps}
+        else:
+            v, sps = _oracle_rate(n, 1, 1)
+            cpu = {"value": v, "unit": METRIC, "cores": 1, "kind": "port",
+                   "sample": f"the C oracle (one thread) on this workload's {n}^3 grid: 1 "
+                             f"timed RK2 step after 1", "s_per_step": sps}
 
     ranks.close()
     if rank != 0:
@@ -428,7 +504,7 @@ def impl_ours(args):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clocks,
             "forms": {"fp64": {"value": value, "ms_per_step": ms_step}, "mixed": mixed},
-            "kernels": per_kernel, "err_bits": out.err_bits}
+            "kernels": per_kernel, "err_bits": out.err_bits, **legs}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -531,16 +607,16 @@ def _oracle_grid_worker(a):
     return (time.perf_counter() - t0) / 2
 
 
-def impl_ensemble(args):
+def ensemble_leg(args, ranks, steps, warmup, with_e2e=True, with_cpu=True, tune=True):
+    """The batched ensemble (every rank its own set of grids): autotune on a
+    sample, warm-up, `steps` timed steps of all grids; returns the fields of
+    its JSON line."""
     import torch
     from gpluto_dev_b200 import autotune, replicas, workloads
     from gpluto_dev_b200 import batch as gb
 
-    ranks = replicas.init("nccl")          # replicas: one grid (set) per GPU
     world, rank, local = ranks.world, ranks.rank, ranks.local
-    torch.cuda.set_device(local)
     barrier = ranks.barrier
-
     members = workloads.ensemble(args.grids, seed0=replicas.replica_seed(0, rank, args.grids))
     cells = sum(m.state.ncells for m in members)
     stream = torch.cuda.Stream()
@@ -548,7 +624,7 @@ def impl_ensemble(args):
 
     # ---- autotune tile shapes per size bin on a sample (every 4th grid) ----
     trials = []
-    if args.no_tune:
+    if not tune:
         table = autotune.default_table()
     else:
         sample = members[::4]
@@ -562,10 +638,10 @@ def impl_ensemble(args):
 
     # ---- the run: all grids, warm-up then K timed steps -----------------
     b = gb.Batch(pool, len(members), stream=stream.cuda_stream)
-    slots = [b.add(m.state, m.scheme, FIRST_DT, args.warmup + args.steps,
+    slots = [b.add(m.state, m.scheme, FIRST_DT, warmup + steps,
                    autotune.shape_for(table, 2, m.state.ncells)) for m in members]
     autotune.apply(b, table, {s: (2, m.state.ncells) for s, m in zip(slots, members)})
-    b.advance(args.warmup)
+    b.advance(warmup)
     b.wait()
     clock = ClockSampler(local)
     barrier()
@@ -574,7 +650,7 @@ def impl_ensemble(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     stream.synchronize()
     e0.record(stream)
-    b.advance(args.steps)
+    b.advance(steps)
     e1.record(stream)
     b.wait()
     clocks = clock.stop()
@@ -590,9 +666,9 @@ def impl_ensemble(args):
     ctas = b.info()["ctas"]
     b.close()
     del b
-    value = replicas.whole_job_rate(world, cells, args.steps, t_ms)
+    value = replicas.whole_job_rate(world, cells, steps, t_ms)
     peak, peak_kind = peaks()
-    achieved = ENSEMBLE_ALG_BYTES_ZONE * cells * args.steps / (t_ms * 1e-3) / 1e9
+    achieved = ENSEMBLE_ALG_BYTES_ZONE * cells * steps / (t_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": "batch_sweep_kernel + batch_cell_kernel (all grids)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": None,
@@ -602,14 +678,14 @@ def impl_ensemble(args):
 
     # ---- end to end: admission from host arrays, K steps, download -------
     e2e = None
-    if not args.no_e2e:
+    if with_e2e:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         b = gb.Batch(pool, len(members), stream=stream.cuda_stream)
-        sl = [b.add(m.state, m.scheme, FIRST_DT, args.steps,
+        sl = [b.add(m.state, m.scheme, FIRST_DT, steps,
                     autotune.shape_for(table, 2, m.state.ncells)) for m in members]
         autotune.apply(b, table, {s: (2, m.state.ncells) for s, m in zip(sl, members)})
-        b.advance(args.steps)
+        b.advance(steps)
         b.wait()
         nout = 0
         for s in sl:
@@ -619,27 +695,37 @@ def impl_ensemble(args):
         b.close()
         nin = sum((m.state.V.size + sum(x.size for x in m.state.Bs)) * 8 for m in members)
         te = ranks.max_over_ranks(te)
-        e2e = {"value": world * cells * args.steps / te / 1e6, "unit": METRIC,
-               "h2d_bytes_per_step": nin / args.steps, "d2h_bytes_per_step": nout / args.steps,
-               "steps": args.steps,
+        e2e = {"value": world * cells * steps / te / 1e6, "unit": METRIC,
+               "h2d_bytes_per_step": nin / steps, "d2h_bytes_per_step": nout / steps,
+               "steps": steps,
                "path": "gp_batch_add of every grid from host arrays, gp_batch_advance(K), "
                        "gp_batch_download of every grid; bytes amortised over K steps"}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if with_cpu and rank == 0 and world == 1:
         cpu, _ = ensemble_cpu_baseline(args, max(1, min(os.cpu_count() or 1, 16)))
+    return {"value": value, "unit": METRIC, "steps": steps, "warmup": warmup,
+            "ms_per_step": t_ms / steps, "config": ensemble_config(args, table),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": 4 * steps, "clocks": clocks, "ctas": ctas, "err_bits": err,
+            "steps_done_min": min(done), "autotune_trials": len(trials)}
 
+
+def impl_ensemble(args):
+    import torch
+    from gpluto_dev_b200 import replicas
+
+    ranks = replicas.init("nccl")          # replicas: one grid (set) per GPU
+    torch.cuda.set_device(ranks.local)
+    leg = ensemble_leg(args, ranks, args.steps, args.warmup, with_e2e=not args.no_e2e,
+                       with_cpu=not args.no_cpu, tune=not args.no_tune)
+    world, rank = ranks.world, ranks.rank
     ranks.close()
     if rank != 0:
         return 0
-    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
-            "data": "synthetic (seeded 2-D turbulence ensemble)",
-            "config": ensemble_config(args, table), "roofline": roofline,
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 4 * args.steps,
-            "clocks": clocks, "ctas": ctas, "err_bits": err,
-            "steps_done_min": min(done), "autotune_trials": len(trials)}
+    line = {"metric": METRIC, "n_gpus": world, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32",
+            "data": "synthetic (seeded 2-D turbulence ensemble)", **leg}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -817,21 +903,18 @@ def run_reference_grids_rmhd(states, nsteps_timed, nwarm):
 # serving: Poisson arrivals, continuous batching, p50/p99 latency vs rate
 # --------------------------------------------------------------------------
 SERVE_RATES = (2.0, 4.0, 8.0, 16.0)
+SERVE_DEFAULT_RATE = 8.0     # requests/s of the serving leg in the default line
 
 
-def impl_serve(args):
+def serve_leg(args, rates, nreq):
+    """The serving loop on a Poisson stream of `nreq` requests at each rate
+    in `rates` (requests/s); returns (sweep rows, tile table, clocks)."""
     import torch
     from gpluto_dev_b200 import autotune, serve, workloads
     from gpluto_dev_b200 import batch as gb
 
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:          # replicas only: the serving sweep runs on one GPU
-        return 0
-    nreq = args.requests
     base = workloads.requests(nreq, 1.0, seed=7)          # unit-rate arrival times
     states = [q.state() for q in base]                    # request payloads, built up front
-    work = sum(q.cells * q.nsteps for q in base)
     stream = torch.cuda.Stream()
     # tile shapes per size bin, tuned on a sample of the requests
     sample = list(range(0, nreq, max(1, nreq // 16)))
@@ -845,7 +928,7 @@ def impl_serve(args):
     sweep = []
     clock = ClockSampler(0)
     clock.start()
-    for lam in args.rates:
+    for lam in rates:
         jobs = [serve.Job(q.rid, q.arrival / lam, st, q.scheme(), q.nsteps)
                 for q, st in zip(base, states)]
         srv = serve.Server(pool_bytes=args.hbm_budget, max_slots=1024, chunk=args.chunk,
@@ -863,21 +946,36 @@ def impl_serve(args):
             row["err_bits"] |= j.status.err_bits
         sweep.append(row)
     clocks = clock.stop()
+    work = sum(q.cells * q.nsteps for q in base)
+    return sweep, table, clocks, work
+
+
+def serve_config(args, nreq, rates, work, table):
+    return {"workload": f"serve_poisson_{nreq}req", "requests": nreq,
+            "rates_per_s": list(rates),
+            "mix": "2-D/3-D ideal MHD (PLM-MC/HLLD/UCT_HLLD) or HD (PLM-MC/HLLC), "
+                   "cells log-uniform 32^2..128^3, steps log-uniform 50..2000, FP64 or mixed",
+            "hbm_budget_bytes": args.hbm_budget, "chunk_steps": args.chunk,
+            "work_zone_updates": work, "tile_table": table,
+            "launch": "per chunk: CUDA graph of chunk x RK2 steps, 2 persistent launches per "
+                      "stage over all active requests"}
+
+
+def impl_serve(args):
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:          # replicas only: the serving sweep runs on one GPU
+        return 0
+    nreq = args.requests
+    sweep, table, clocks, work = serve_leg(args, args.rates, nreq)
     # headline value: p99 latency at the highest rate of the sweep
     head = sweep[-1]
     line = {"metric": "p99 serve latency", "value": head["p99_s"], "unit": "s",
             "n_gpus": 1, "steps": None, "warmup": None, "ms_per_step": None,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64+f32", "data": "synthetic (seeded serving stream)",
-            "config": {"workload": f"serve_poisson_{nreq}req",
-                       "requests": nreq, "rates_per_s": list(args.rates),
-                       "mix": "2-D/3-D ideal MHD (PLM-MC/HLLD/UCT_HLLD) or HD (PLM-MC/HLLC), "
-                              "cells log-uniform 32^2..128^3, steps log-uniform 50..2000, "
-                              "FP64 or mixed",
-                       "hbm_budget_bytes": args.hbm_budget, "chunk_steps": args.chunk,
-                       "work_zone_updates": work, "tile_table": table,
-                       "launch": "per chunk: CUDA graph of chunk x RK2 steps, 2 persistent "
-                                 "launches per stage over all active requests"},
+            "config": serve_config(args, nreq, args.rates, work, table),
             "throughput_Mzone_updates_per_s": head["Mzone_updates_per_s"],
             "sweep": sweep, "clocks": clocks,
             "e2e": {"value": head["Mzone_updates_per_s"], "unit": METRIC,
@@ -908,6 +1006,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--error-steps", type=int, default=100)
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the short ensemble and serving legs of the default line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
