@@ -29,13 +29,14 @@ BASE = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed
 # count by about a fifth.  These flags touch single precision only, so the FP64
 # accumulation, CT update and con2prim of that form stay IEEE.
 MIXED_FP32 = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
-# The stage kernels are instantiated per form and per physics (GP_PART: 0 HD,
-# 1 MHD, 2 RMHD) in six units that compile in parallel.
+# The stage kernels are instantiated per form and per scheme group (GP_PART:
+# 0 HD, 1 MHD with HLLD/HLL, 2 RMHD, 3 MHD with Lax-Friedrichs/HLLC) in eight
+# units that compile in parallel.
 UNITS = [
     *[(f"gp_launch_fp64_p{p}.o", "gp_launch.cu", ["-DGP_MIXED=0", f"-DGP_PART={p}", "-fmad=false"])
-      for p in (1, 2, 0)],
+      for p in (1, 2, 3, 0)],
     *[(f"gp_launch_mixed_p{p}.o", "gp_launch.cu", ["-DGP_MIXED=1", f"-DGP_PART={p}", *MIXED_FP32])
-      for p in (1, 2, 0)],
+      for p in (1, 2, 3, 0)],
     ("gp_launch_dispatch.o", "gp_launch_dispatch.cu", []),
     ("gp_api.o", "gp_api.cu", ["-fmad=false"]),
     ("gp_noalloc.o", "gp_noalloc.cu", ["-fmad=false"]),

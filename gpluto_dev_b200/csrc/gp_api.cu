@@ -630,12 +630,10 @@ int validate_scheme(const gp_grid_desc* grid, const gp_scheme* scheme) {
         return fail(GP_ERR_UNSUPPORTED, "non-uniform grid along %d", d);
     }
   }
-  if (scheme->physics == GP_MHD && scheme->riemann == GP_RS_HLLC)
-    return fail(GP_ERR_UNSUPPORTED, "MHD HLLC not built");
   if (scheme->physics == GP_MHD && scheme->ct_emf == GP_CT_UCT_HLLD &&
       scheme->riemann != GP_RS_HLLD)
     return fail(GP_ERR_UNSUPPORTED, "UCT_HLLD pairs with hlld only (Src/MHD/hll.cpp:73-77, "
-                "Src/MHD/tvdlf.cpp:83-87)");
+                "Src/MHD/tvdlf.cpp:83-87, Src/MHD/hllc.cpp:79-83)");
   if (scheme->physics != GP_HD && scheme->ct_emf != GP_CT_UCT_HLL &&
       scheme->ct_emf != GP_CT_UCT_HLLD &&
       !(scheme->ct_emf == GP_CT_ARITHMETIC && scheme->physics == GP_MHD))

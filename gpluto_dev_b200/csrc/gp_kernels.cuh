@@ -146,6 +146,7 @@ __device__ __forceinline__ R riemann(const R* vl, const R* vr, R* flux, R gamma,
     R cm;
     if constexpr (RS == RS_HLLD) cm = mhd_hlld<DIR, CT>(vl, vr, flux, gamma, Bn, ct);
     else if constexpr (RS == RS_TVDLF) cm = mhd_tvdlf<DIR>(vl, vr, flux, gamma, ct);
+    else if constexpr (RS == RS_HLLC) cm = mhd_hllc<DIR>(vl, vr, flux, gamma, ct);
     else cm = mhd_hll<DIR>(vl, vr, flux, gamma, ct);
     if constexpr (CT == CT_ARITH) {
       // CT_Store_Arith (Src/MHD/CT/ct_store.hpp:74-93): the face's two

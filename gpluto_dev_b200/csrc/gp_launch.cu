@@ -13,12 +13,12 @@
 #ifndef GP_MIXED
 #define GP_MIXED 0
 #endif
-// GP_PART selects the physics this unit instantiates (0 HD, 1 MHD, 2 RMHD:
-// the PHYS_* values), so that the build compiles the three in parallel; the
-// per-physics entry points launch_stage_{fp64,mixed}_p<part> are joined by
-// gp_launch_dispatch.cu.
+// GP_PART selects the schemes this unit instantiates (0 HD, 1 MHD with
+// HLLD/HLL, 2 RMHD, 3 MHD with Lax-Friedrichs/HLLC), so that the build
+// compiles the four in parallel; the entry points
+// launch_stage_{fp64,mixed}_p<part> are joined by gp_launch_dispatch.cu.
 #ifndef GP_PART
-#error "compile gp_launch.cu with -DGP_PART=0, 1 or 2"
+#error "compile gp_launch.cu with -DGP_PART=0, 1, 2 or 3"
 #endif
 #define GP_CAT2(a, b) a##b
 #define GP_CAT(a, b) GP_CAT2(a, b)
@@ -162,13 +162,12 @@ template <int NDIM>
 static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey& k, int seg,
                      cudaStream_t s, cudaEvent_t* ev) {
 #if GP_PART == 1
+  // MHD with the HLLD and HLL solvers
   if (k.physics == PHYS_MHD && k.ct == CT_ARITH) {
     if (k.riemann == RS_HLLD)
       return by_lim<PHYS_MHD, 8, NDIM, RS_HLLD, CT_ARITH>(a, g, k.limiter, seg, s, ev);
     if (k.riemann == RS_HLL)
       return by_lim<PHYS_MHD, 8, NDIM, RS_HLL, CT_ARITH>(a, g, k.limiter, seg, s, ev);
-    if (k.riemann == RS_TVDLF)
-      return by_lim<PHYS_MHD, 8, NDIM, RS_TVDLF, CT_ARITH>(a, g, k.limiter, seg, s, ev);
     return -1;
   }
   if (k.physics == PHYS_MHD) {
@@ -178,8 +177,23 @@ static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey
       return by_lim<PHYS_MHD, 8, NDIM, RS_HLLD, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
     if (k.riemann == RS_HLL && k.ct == CT_UCT_HLL)
       return by_lim<PHYS_MHD, 8, NDIM, RS_HLL, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
+    return -1;
+  }
+#endif
+#if GP_PART == 3
+  // MHD with the Lax-Friedrichs and HLLC solvers (UCT_HLL or ARITHMETIC)
+  if (k.physics == PHYS_MHD && k.ct == CT_ARITH) {
+    if (k.riemann == RS_TVDLF)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_TVDLF, CT_ARITH>(a, g, k.limiter, seg, s, ev);
+    if (k.riemann == RS_HLLC)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_HLLC, CT_ARITH>(a, g, k.limiter, seg, s, ev);
+    return -1;
+  }
+  if (k.physics == PHYS_MHD) {
     if (k.riemann == RS_TVDLF && k.ct == CT_UCT_HLL)
       return by_lim<PHYS_MHD, 8, NDIM, RS_TVDLF, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
+    if (k.riemann == RS_HLLC && k.ct == CT_UCT_HLL)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_HLLC, CT_UCT_HLL>(a, g, k.limiter, seg, s, ev);
     return -1;
   }
 #endif

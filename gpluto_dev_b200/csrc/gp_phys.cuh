@@ -631,6 +631,77 @@ __device__ __forceinline__ R mhd_hll(const R* vl, const R* vr, R* flux, R gamma,
   return cmax;
 }
 
+// HLLC solver for MHD, Src/MHD/hllc.cpp:52-363: one intermediate state on
+// each side of the contact, built from the HLL average (no HLL switch
+// without multi-D shock flattening); UCT_HLL face data (the caller replaces
+// them by the induction fluxes for CT_EMF_AVERAGE ARITHMETIC).
+template <int DIR, typename R>
+__device__ __forceinline__ R mhd_hllc(const R* vl, const R* vr, R* flux, R gamma,
+                                      CTFace<R>& ct) {
+  constexpr int VXn = VX1 + DIR;
+  constexpr int MXn = MX1 + DIR, MXt = MX1 + (DIR + 1) % 3, MXb = MX1 + (DIR + 2) % 3;
+  constexpr int BXn = BX1 + DIR, BXt = BX1 + (DIR + 1) % 3, BXb = BX1 + (DIR + 2) % 3;
+  R ul[8], ur[8], fl[8], fr[8], Sl, Sr, pl, pr;
+  const R gmm1 = gamma - R(1);
+  mhd_prim2cons(vl, ul, gmm1);
+  mhd_prim2cons(vr, ur, gmm1);
+  R a2L = gamma * vl[7] / vl[RHO];
+  R a2R = gamma * vr[7] / vr[RHO];
+  {
+    R sl_min, sl_max, sr_min, sr_max;
+    mhd_signal_speed<DIR>(vl, a2L, sl_min, sl_max);
+    mhd_signal_speed<DIR>(vr, a2R, sr_min, sr_max);
+    Sl = GP_MIN(sl_min, sr_min);
+    Sr = GP_MAX(sl_max, sr_max);
+  }
+  R cmax = GP_MAX(rabs(Sl), rabs(Sr));
+  mhd_flux<DIR>(vl, ul, fl, pl);
+  mhd_flux<DIR>(vr, ur, fr, pr);
+  if (Sl >= R(0)) {
+#pragma unroll
+    for (int nv = 0; nv < 8; nv++) flux[nv] = fl[nv];
+  } else if (Sr <= R(0)) {
+#pragma unroll
+    for (int nv = 0; nv < 8; nv++) flux[nv] = fr[nv];
+  } else {
+    R Uhll[8], Fhll[8], us[8];
+    const R scrh = R(1) / (Sr - Sl);
+#pragma unroll
+    for (int nv = 0; nv < 8; nv++) {
+      Uhll[nv] = Sr * ur[nv] - Sl * ul[nv] + fl[nv] - fr[nv];
+      Uhll[nv] *= scrh;
+      Fhll[nv] = Sl * Sr * (ur[nv] - ul[nv]) + Sr * fl[nv] - Sl * fr[nv];
+      Fhll[nv] *= scrh;
+    }
+    const R Bxs = Uhll[BXn], Bys = Uhll[BXt], Bzs = Uhll[BXb];
+    const R vxs = Uhll[MXn] / Uhll[RHO];
+    // only the state on the side of the contact the face sees is built
+    const bool left = vxs > R(0);
+    const R* v = left ? vl : vr;
+    const R* u = left ? ul : ur;
+    const R* f = left ? fl : fr;
+    const R S = left ? Sl : Sr;
+    const R p = left ? pl : pr;
+    const R vx = v[VXn];
+    R vB = v[VX1] * v[BX1] + v[VX1 + 1] * v[BX2] + v[VX1 + 2] * v[BX3];
+    R vBs = Uhll[BX1] * Uhll[MX1] + Uhll[BX2] * Uhll[MX2] + Uhll[BX3] * Uhll[MX3];
+    vBs /= Uhll[RHO];
+    us[RHO] = u[RHO] * (S - vx) / (S - vxs);
+    const R ps = Fhll[MXn] + Bxs * Bxs - Fhll[RHO] * vxs;
+    us[7] = (u[7] * (S - vx) + ps * vxs - p * vx - Bxs * vBs + v[BXn] * vB) / (S - vxs);
+    us[MXn] = us[RHO] * vxs;
+    us[MXt] = (u[MXt] * (S - vx) - (Bxs * Bys - v[BXn] * v[BXt])) / (S - vxs);
+    us[MXb] = (u[MXb] * (S - vx) - (Bxs * Bzs - v[BXn] * v[BXb])) / (S - vxs);
+    us[BXn] = Bxs;
+    us[BXt] = Bys;
+    us[BXb] = Bzs;
+#pragma unroll
+    for (int nv = 0; nv < 8; nv++) flux[nv] = f[nv] + S * (us[nv] - u[nv]);
+  }
+  ct_store_ucthll<DIR>(vl, vr, Sl, Sr, ct);
+  return cmax;
+}
+
 // Lax-Friedrichs (Rusanov) flux for MHD, Src/MHD/tvdlf.cpp:60-244: the
 // signal speed of the arithmetic average state; UCT_HLL face data with
 // Sl = -cmax, Sr = cmax.

@@ -484,6 +484,76 @@ static double MHD_HLL(orc_t *o, int dir, double *vl, double *vr, double *flux, l
   return cmax;
 }
 
+/* HLLC for MHD, Src/MHD/hllc.cpp:52-363 (no HLL switch without multi-D
+   shock flattening; UCT_HLL face data, or the caller's arithmetic store). */
+static double MHD_HLLC(orc_t *o, int dir, double *vl, double *vr, double *flux, long e) {
+  const double gamma = o->c.gamma;
+  const int VXn = VX1 + dir;
+  const int MXn = MX1 + dir, MXt = MX1 + (dir+1)%3, MXb = MX1 + (dir+2)%3;
+  const int BXn = BX1 + dir, BXt = BX1 + (dir+1)%3, BXb = BX1 + (dir+2)%3;
+  int nv;
+  double ul[8], ur[8], fl[8], fr[8], Sl, Sr, pl, pr;
+  MHD_PrimToCons(vl, ul, gamma);
+  MHD_PrimToCons(vr, ur, gamma);
+  double a2L = gamma*vl[7]/vl[RHO];
+  double a2R = gamma*vr[7]/vr[RHO];
+  {
+    double sl_min, sl_max, sr_min, sr_max;
+    MHD_MaxSignalSpeed(dir, vl, a2L, &sl_min, &sl_max);
+    MHD_MaxSignalSpeed(dir, vr, a2R, &sr_min, &sr_max);
+    Sl = MIN(sl_min, sr_min);
+    Sr = MAX(sl_max, sr_max);
+  }
+  double cmax = MAX(fabs(Sl), fabs(Sr));
+  MHD_Flux(dir, vl, ul, fl, &pl);
+  MHD_Flux(dir, vr, ur, fr, &pr);
+  if (Sl >= 0.0) {
+    for (nv = 0; nv < 8; nv++) flux[nv] = fl[nv];
+  } else if (Sr <= 0.0) {
+    for (nv = 0; nv < 8; nv++) flux[nv] = fr[nv];
+  } else {
+    double Uhll[8], Fhll[8], usl[8], usr[8];
+    double scrh = 1.0/(Sr - Sl);
+    for (nv = 0; nv < 8; nv++) {
+      Uhll[nv]  = Sr*ur[nv] - Sl*ul[nv] + fl[nv] - fr[nv];
+      Uhll[nv] *= scrh;
+      Fhll[nv]  = Sl*Sr*(ur[nv] - ul[nv]) + Sr*fl[nv] - Sl*fr[nv];
+      Fhll[nv] *= scrh;
+    }
+    double Bxs = Uhll[BXn], Bys = Uhll[BXt], Bzs = Uhll[BXb];
+    double vxL = vl[VXn], vxR = vr[VXn];
+    double vxs = Uhll[MXn]/Uhll[RHO];
+    {
+      double vBL = vl[VX1]*vl[BX1] + vl[VX1+1]*vl[BX2] + vl[VX1+2]*vl[BX3];
+      double vBR = vr[VX1]*vr[BX1] + vr[VX1+1]*vr[BX2] + vr[VX1+2]*vr[BX3];
+      double vBs = Uhll[BX1]*Uhll[MX1] + Uhll[BX2]*Uhll[MX2] + Uhll[BX3]*Uhll[MX3];
+      vBs /= Uhll[RHO];
+      usl[RHO] = ul[RHO]*(Sl - vxL)/(Sl - vxs);
+      usr[RHO] = ur[RHO]*(Sr - vxR)/(Sr - vxs);
+      double ps = Fhll[MXn] + Bxs*Bxs - Fhll[RHO]*vxs;
+      usl[7] = (ul[7]*(Sl - vxL) + ps*vxs - pl*vxL - Bxs*vBs + vl[BXn]*vBL)/(Sl - vxs);
+      usr[7] = (ur[7]*(Sr - vxR) + ps*vxs - pr*vxR - Bxs*vBs + vr[BXn]*vBR)/(Sr - vxs);
+    }
+    usl[MXn] = usl[RHO]*vxs;
+    usr[MXn] = usr[RHO]*vxs;
+    usl[MXt] = (ul[MXt]*(Sl - vxL) - (Bxs*Bys - vl[BXn]*vl[BXt]))/(Sl - vxs);
+    usr[MXt] = (ur[MXt]*(Sr - vxR) - (Bxs*Bys - vr[BXn]*vr[BXt]))/(Sr - vxs);
+    usl[MXb] = (ul[MXb]*(Sl - vxL) - (Bxs*Bzs - vl[BXn]*vl[BXb]))/(Sl - vxs);
+    usr[MXb] = (ur[MXb]*(Sr - vxR) - (Bxs*Bzs - vr[BXn]*vr[BXb]))/(Sr - vxs);
+    usl[BXn] = usr[BXn] = Bxs;
+    usl[BXt] = usr[BXt] = Bys;
+    usl[BXb] = usr[BXb] = Bzs;
+    if (vxs > 0.0) {
+      for (nv = 0; nv < 8; nv++) flux[nv] = fl[nv] + Sl*(usl[nv] - ul[nv]);
+    } else {
+      for (nv = 0; nv < 8; nv++) flux[nv] = fr[nv] + Sr*(usr[nv] - ur[nv]);
+    }
+  }
+  for (nv = 0; nv < 8; nv++) if (isnan(flux[nv])) o->err |= ERR_NAN | ERR_QUIT;
+  CT_Store_UCTHll(o, dir, vl, vr, Sl, Sr, e);
+  return cmax;
+}
+
 /* Lax-Friedrichs (Rusanov) flux for MHD, Src/MHD/tvdlf.cpp:60-244: the
    signal speed of the arithmetic average state, UCT_HLL face data with
    Sl = -cmax, Sr = cmax. */
@@ -1128,6 +1198,7 @@ static void Sweep(orc_t *o, int dir, double dt) {
       if (o->c.physics == ORC_MHD) {
         if (o->c.solver == ORC_HLLD)       cmax[i] = MHD_HLLD(o, dir, vl, vr, f, e, Bn[i]);
         else if (o->c.solver == ORC_TVDLF) cmax[i] = MHD_TVDLF(o, dir, vl, vr, f, e);
+        else if (o->c.solver == ORC_HLLC)  cmax[i] = MHD_HLLC(o, dir, vl, vr, f, e);
         else                               cmax[i] = MHD_HLL(o, dir, vl, vr, f, e);
         if (o->c.ct == ORC_ARITHMETIC) {
           /* CT_Store_Arith, Src/MHD/CT/ct_store.hpp:74-93 (replaces the

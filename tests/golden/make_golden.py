@@ -225,6 +225,22 @@ CASES = {
                               dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="tvdlf",
                                    ct_emf="ARITHMETIC", cfl=0.4, first_dt=1e-4,
                                    reconstruction="PARABOLIC"), 10),
+    # HLLC for MHD (Src/MHD/hllc.cpp): UCT_HLL and ARITHMETIC face data
+    "mhd2d_mc_hllc_ucthll": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=191),
+                             dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hllc",
+                                  ct_emf="UCT_HLL", cfl=0.4, first_dt=1e-4), 12),
+    "mhd3d_vl_hllc_arith_outflowx": (
+        ics.mhd3d_turbulence, dict(n=(12, 10, 9), seed=192),
+        dict(physics="MHD", ndim=3, limiter="VANLEER_LIM", solver="hllc", ct_emf="ARITHMETIC",
+             cfl=0.4, first_dt=1e-4, bc=("outflow", "periodic", "periodic")), 6),
+    "mhd2d_ppm_hllc_ucthll_rk3": (ics.mhd2d_turbulence, dict(n=(22, 18), seed=193),
+                                  dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hllc",
+                                       ct_emf="UCT_HLL", cfl=0.4, first_dt=1e-4,
+                                       reconstruction="PARABOLIC", rk="RK3"), 10),
+    "mhd3d_blast_mc_hllc_ucthll_reflect": (
+        ics.mhd3d_blast, dict(n=(14, 12, 10), seed=194, radius=0.25),
+        dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="hllc", ct_emf="UCT_HLL", cfl=0.4,
+             first_dt=1e-4, bc=("reflective", "reflective", "reflective")), 8),
     # the Lax-Friedrichs (tvdlf) solver, MHD with UCT_HLL face data and HD
     "mhd2d_mc_tvdlf_ucthll": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=161),
                               dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="tvdlf",

@@ -71,6 +71,8 @@ MIXED_SCHEMES = [
      dict(), 2, 30),
     (ics.mhd3d_turbulence, dict(n=(36, 32, 28), seed=126), "ospre", "hlld", "uct_hlld",
      dict(), 2, 12),
+    (ics.mhd3d_turbulence, dict(n=(36, 32, 28), seed=127), "mc", "hllc", "uct_hll",
+     dict(), 2, 12),
 ]
 
 

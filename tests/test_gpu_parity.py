@@ -75,6 +75,11 @@ CASES = [
     # CT_EMF_AVERAGE ARITHMETIC
     (ics.mhd3d_turbulence, dict(n=(13, 11, 9), seed=191), "mc", "hlld", "arithmetic", 6),
     (ics.mhd2d_turbulence, dict(n=(27, 19), seed=192), "vl", "tvdlf", "arithmetic", 10),
+    # HLLC for MHD (UCT_HLL and ARITHMETIC face data)
+    (ics.mhd3d_turbulence, dict(n=(17, 13, 11), seed=195), "mc", "hllc", "uct_hll", 6),
+    (ics.mhd2d_turbulence, dict(n=(31, 23), seed=196), "ppm", "hllc", "arithmetic", 10),
+    (ics.mhd3d_blast, dict(n=(15, 14, 13), seed=197, radius=0.25), "minmod", "hllc",
+     "uct_hll", 6),
 ]
 
 
