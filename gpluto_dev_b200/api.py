@@ -35,7 +35,7 @@ LIMITERS = {"flat": 0, "minmod": 1, "vl": 2, "vanleer": 2, "mc": 3, "ppm": 3, "m
             "wenoz": 3, "limo3": 3, "weno3": 3, "vanalbada": 6, "ospre": 7, "umist": 8}
 RECONSTRUCTION = {"ppm": 1, "mp5": 2, "wenoz": 3, "limo3": 4, "weno3": 5}
 SOLVERS = {"hll": 0, "hllc": 1, "hlld": 2, "tvdlf": 3}
-CT_AVG = {"uct_hll": 0, "uct_hlld": 1, "arithmetic": 2}
+CT_AVG = {"uct_hll": 0, "uct_hlld": 1, "arithmetic": 2, "ct_contact": 3}
 FP64, MIXED = 0, 1
 LAYOUT_INTERIOR, LAYOUT_REFERENCE = 0, 1
 ERR_QUIT = 1 << 15

@@ -636,7 +636,8 @@ int validate_scheme(const gp_grid_desc* grid, const gp_scheme* scheme) {
                 "Src/MHD/tvdlf.cpp:83-87, Src/MHD/hllc.cpp:79-83)");
   if (scheme->physics != GP_HD && scheme->ct_emf != GP_CT_UCT_HLL &&
       scheme->ct_emf != GP_CT_UCT_HLLD &&
-      !(scheme->ct_emf == GP_CT_ARITHMETIC && scheme->physics == GP_MHD))
+      !((scheme->ct_emf == GP_CT_ARITHMETIC || scheme->ct_emf == GP_CT_CONTACT) &&
+        scheme->physics == GP_MHD))
     return fail(GP_ERR_UNSUPPORTED, "CT_EMF_AVERAGE %d not built for this physics",
                 scheme->ct_emf);
   if (scheme->riemann < GP_RS_HLL || scheme->riemann > GP_RS_TVDLF)

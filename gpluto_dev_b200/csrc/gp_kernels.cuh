@@ -148,11 +148,18 @@ __device__ __forceinline__ R riemann(const R* vl, const R* vr, R* flux, R gamma,
     else if constexpr (RS == RS_TVDLF) cm = mhd_tvdlf<DIR>(vl, vr, flux, gamma, ct);
     else if constexpr (RS == RS_HLLC) cm = mhd_hllc<DIR>(vl, vr, flux, gamma, ct);
     else cm = mhd_hll<DIR>(vl, vr, flux, gamma, ct);
-    if constexpr (CT == CT_ARITH) {
+    if constexpr (CT == CT_ARITH || CT == CT_CONTACT) {
       // CT_Store_Arith (Src/MHD/CT/ct_store.hpp:74-93): the face's two
       // induction fluxes, e[b][n] = -F(B_t) and e[t][n] = F(B_b)
       ct.eb = -flux[BX1 + (DIR + 1) % 3];
       ct.et = flux[BX1 + (DIR + 2) % 3];
+      if constexpr (CT == CT_CONTACT) {
+        // the sign of the mass flux (zero within eps_CT_CONTACT = 1e-6,
+        // Src/MHD/CT/ct.hpp:110), kept as the weight the corner
+        // integration gives the left cell (Src/MHD/CT/ct_emf_average.cpp:137-143)
+        const R fr = flux[RHO];
+        ct.aL = fr > R(1.e-6) ? R(1) : (fr < R(-1.e-6) ? R(0) : R(0.5));
+      }
     }
     return cm;
   } else if constexpr (PHYS == PHYS_RMHD) {
@@ -1428,6 +1435,70 @@ __global__ void __launch_bounds__(256) emf_arith_kernel(StageArgs<CTT> a, Grid3 
     // Ey at (i-1/2, j, k-1/2): e[y][x] = ct[0][1], e[y][z] = ct[2][0]
     a.Ee[1][c] = (CTT)(w * ((R)a.ct[0][1][ci] + (R)a.ct[0][1][czm] + (R)a.ct[2][0][ci] +
                             (R)a.ct[2][0][cxm]));
+  }
+}
+
+// CT_EMF_AVERAGE CT_CONTACT (Src/MHD/CT/ct_emf.cpp:220-245): per edge the
+// four face EMFs summed (CT_EMF_ArithmeticAverage with w = 1), the terms of
+// CT_EMF_IntegrateToCorner (Src/MHD/CT/ct_emf_average.cpp:115-290; Gardiner
+// & Stone 2005, eqs. 41-50) -- derivatives of E between the faces and the
+// cell-centred field -v x B, each taken from the upwind cell of the face's
+// contact (weights in ct[d][2]) -- then times 1/4, in the reference's
+// operation order.  Thread per cell, its three edges.
+template <int NDIM, typename R, typename CTT>
+__global__ void __launch_bounds__(256) emf_contact_kernel(StageArgs<CTT> a, Grid3 g) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, nxy = nx * ny;
+  const long long n = g.n;
+  const int ci = (int)c, i = ci % nx, j = (ci / nx) % ny, k = ci / nxy;
+  const int dx = wrapi(i - 1, nx) - i, dy = nx * (wrapi(j - 1, ny) - j);
+  const int dz = NDIM == 3 ? nxy * (wrapi(k - 1, nz) - k) : 0;
+  const double* V = a.V;
+  // cell-centred inductive field (CT_ComputeCenterEMF, Src/MHD/CT/ct_emf.cpp:333-367)
+  auto ecc = [&](int comp, int q) -> R {
+    const R vx1 = (R)V[VX1 * n + q], vx2 = (R)V[(VX1 + 1) * n + q], vx3 = (R)V[(VX1 + 2) * n + q];
+    const R bx1 = (R)V[BX1 * n + q], bx2 = (R)V[BX2 * n + q], bx3 = (R)V[BX3 * n + q];
+    if (comp == 0) return (vx3 * bx2 - vx2 * bx3);
+    if (comp == 1) return (vx1 * bx3 - vx3 * bx1);
+    return (vx2 * bx1 - vx1 * bx2);
+  };
+  auto f = [&](int d, int r, int q) -> R { return (R)a.ct[d][r][q]; };
+  const R one = R(1);
+  {  // Ez at (i-1/2, j-1/2, k): e[z][x] = ct[0][0], e[z][y] = ct[1][1]
+    const int c0 = ci, cxm = ci + dx, cym = ci + dy, cxym = ci + dx + dy;
+    R E = one * (f(0, 0, c0) + f(0, 0, cym) + f(1, 1, c0) + f(1, 1, cxm));
+    const R wS = f(0, 2, cym), wN = f(0, 2, c0);
+    E += wS * (f(1, 1, cxm) - ecc(2, cxym)) + (one - wS) * (f(1, 1, c0) - ecc(2, cym)) -
+         wN * (ecc(2, cxm) - f(1, 1, cxm)) - (one - wN) * (ecc(2, c0) - f(1, 1, c0));
+    const R wW = f(1, 2, cxm), wE = f(1, 2, c0);
+    E += wW * (f(0, 0, cym) - ecc(2, cxym)) + (one - wW) * (f(0, 0, c0) - ecc(2, cxm)) -
+         wE * (ecc(2, cym) - f(0, 0, cym)) - (one - wE) * (ecc(2, c0) - f(0, 0, c0));
+    a.Ee[2][c] = (CTT)(E * R(0.25));
+  }
+  if constexpr (NDIM == 3) {
+    {  // Ex at (i, j-1/2, k-1/2): e[x][z] = ct[2][1], e[x][y] = ct[1][0]
+      const int c0 = ci, cym = ci + dy, czm = ci + dz, cyzm = ci + dy + dz;
+      R E = one * (f(2, 1, c0) + f(2, 1, cym) + f(1, 0, c0) + f(1, 0, czm));
+      const R wS = f(1, 2, czm), wN = f(1, 2, c0);
+      E += wS * (f(2, 1, cym) - ecc(0, cyzm)) + (one - wS) * (f(2, 1, c0) - ecc(0, czm)) -
+           wN * (ecc(0, cym) - f(2, 1, cym)) - (one - wN) * (ecc(0, c0) - f(2, 1, c0));
+      const R wW = f(2, 2, cym), wE = f(2, 2, c0);
+      E += wW * (f(1, 0, czm) - ecc(0, cyzm)) + (one - wW) * (f(1, 0, c0) - ecc(0, cym)) -
+           wE * (ecc(0, czm) - f(1, 0, czm)) - (one - wE) * (ecc(0, c0) - f(1, 0, c0));
+      a.Ee[0][c] = (CTT)(E * R(0.25));
+    }
+    {  // Ey at (i-1/2, j, k-1/2): e[y][x] = ct[0][1], e[y][z] = ct[2][0]
+      const int c0 = ci, cxm = ci + dx, czm = ci + dz, cxzm = ci + dx + dz;
+      R E = one * (f(0, 1, c0) + f(0, 1, czm) + f(2, 0, c0) + f(2, 0, cxm));
+      const R wS = f(2, 2, cxm), wN = f(2, 2, c0);
+      E += wS * (f(0, 1, czm) - ecc(1, cxzm)) + (one - wS) * (f(0, 1, c0) - ecc(1, cxm)) -
+           wN * (ecc(1, czm) - f(0, 1, czm)) - (one - wN) * (ecc(1, c0) - f(0, 1, c0));
+      const R wW = f(0, 2, czm), wE = f(0, 2, c0);
+      E += wW * (f(2, 0, cxm) - ecc(1, cxzm)) + (one - wW) * (f(2, 0, c0) - ecc(1, czm)) -
+           wE * (ecc(1, cxm) - f(2, 0, cxm)) - (one - wE) * (ecc(1, c0) - f(2, 0, c0));
+      a.Ee[1][c] = (CTT)(E * R(0.25));
+    }
   }
 }
 

@@ -105,6 +105,8 @@ static void run_stage(const StageArgs<CTT>& a, const GridDims& gd, int seg, cuda
     pre();
     if constexpr (CT == CT_ARITH) {
       emf_arith_kernel<NDIM, RT, CTT><<<nb, 256, 0, s>>>(a, g);
+    } else if constexpr (CT == CT_CONTACT) {
+      emf_contact_kernel<NDIM, RT, CTT><<<nb, 256, 0, s>>>(a, g);
     } else if constexpr (NDIM == 3 && (sizeof(RT) == 8 || five_point<LIM>())) {  // plane-staged EMF
       using T = EmfTile<LIM, CTT>;
       cudaFuncSetAttribute(emf_tile_kernel<LIM, RT, CTT>,
@@ -163,6 +165,13 @@ static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey
                      cudaStream_t s, cudaEvent_t* ev) {
 #if GP_PART == 1
   // MHD with the HLLD and HLL solvers
+  if (k.physics == PHYS_MHD && k.ct == CT_CONTACT) {
+    if (k.riemann == RS_HLLD)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_HLLD, CT_CONTACT>(a, g, k.limiter, seg, s, ev);
+    if (k.riemann == RS_HLL)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_HLL, CT_CONTACT>(a, g, k.limiter, seg, s, ev);
+    return -1;
+  }
   if (k.physics == PHYS_MHD && k.ct == CT_ARITH) {
     if (k.riemann == RS_HLLD)
       return by_lim<PHYS_MHD, 8, NDIM, RS_HLLD, CT_ARITH>(a, g, k.limiter, seg, s, ev);
@@ -181,7 +190,14 @@ static int by_scheme(const StageArgs<CTT>& a, const GridDims& g, const SchemeKey
   }
 #endif
 #if GP_PART == 3
-  // MHD with the Lax-Friedrichs and HLLC solvers (UCT_HLL or ARITHMETIC)
+  // MHD with the Lax-Friedrichs and HLLC solvers (UCT_HLL, ARITHMETIC or CT_CONTACT)
+  if (k.physics == PHYS_MHD && k.ct == CT_CONTACT) {
+    if (k.riemann == RS_TVDLF)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_TVDLF, CT_CONTACT>(a, g, k.limiter, seg, s, ev);
+    if (k.riemann == RS_HLLC)
+      return by_lim<PHYS_MHD, 8, NDIM, RS_HLLC, CT_CONTACT>(a, g, k.limiter, seg, s, ev);
+    return -1;
+  }
   if (k.physics == PHYS_MHD && k.ct == CT_ARITH) {
     if (k.riemann == RS_TVDLF)
       return by_lim<PHYS_MHD, 8, NDIM, RS_TVDLF, CT_ARITH>(a, g, k.limiter, seg, s, ev);

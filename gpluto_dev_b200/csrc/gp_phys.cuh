@@ -46,7 +46,7 @@ __host__ __device__ constexpr bool five_point() { return LIM == LIM_MP5 || LIM =
 template <int LIM>
 __host__ __device__ constexpr bool three_point() { return LIM == LIM_LIMO3 || LIM == LIM_WENO3; }
 enum : int { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2, RS_TVDLF = 3 };
-enum : int { CT_UCT_HLL = 0, CT_UCT_HLLD = 1, CT_ARITH = 2 };
+enum : int { CT_UCT_HLL = 0, CT_UCT_HLLD = 1, CT_ARITH = 2, CT_CONTACT = 3 };
 
 template <typename R> __device__ __forceinline__ R rsqrt_(R x);
 template <> __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }

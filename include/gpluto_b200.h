@@ -55,12 +55,15 @@ enum { GP_HD = 0, GP_MHD = 1, GP_RMHD = 2 };
    not limiters (they stand for PPM and MP5 inside the library) */
 enum { GP_LIM_FLAT = 0, GP_LIM_MINMOD = 1, GP_LIM_VANLEER = 2, GP_LIM_MC = 3,
        GP_LIM_VANALBADA = 6, GP_LIM_OSPRE = 7, GP_LIM_UMIST = 8 };
-/* [Solver] in pluto.ini (Src/MHD/set_solver.cpp:35-47); tvdlf for MHD (with
-   UCT_HLL or ARITHMETIC), RMHD and HD */
+/* [Solver] in pluto.ini (Src/MHD/set_solver.cpp:35-47); hll, hllc and tvdlf
+   for MHD take UCT_HLL, ARITHMETIC or CT_CONTACT (UCT_HLLD needs hlld);
+   hllc is HD and MHD only */
 enum { GP_RS_HLL = 0, GP_RS_HLLC = 1, GP_RS_HLLD = 2, GP_RS_TVDLF = 3 };
-/* CT_EMF_AVERAGE (Src/MHD/CT/ct.hpp:19-27): upwind UCT_HLL / UCT_HLLD, or the
-   ARITHMETIC average of the face EMFs (MHD) */
-enum { GP_CT_UCT_HLL = 0, GP_CT_UCT_HLLD = 1, GP_CT_ARITHMETIC = 2 };
+/* CT_EMF_AVERAGE (Src/MHD/CT/ct.hpp:19-27): upwind UCT_HLL / UCT_HLLD, the
+   ARITHMETIC average of the face EMFs, or CT_CONTACT (that average with the
+   contact-upwinded corner terms, Src/MHD/CT/ct_emf.cpp:220-245); the last
+   two for MHD */
+enum { GP_CT_UCT_HLL = 0, GP_CT_UCT_HLLD = 1, GP_CT_ARITHMETIC = 2, GP_CT_CONTACT = 3 };
 /* [Boundary] types (Src/boundary.cpp:144-310; the reference's values,
    Src/gpluto.hpp:205-212, except periodic): outflow (zero-gradient ghost
    copy, OutflowBoundary Src/boundary.cpp:677-780), reflective,

@@ -57,6 +57,7 @@ typedef struct {
   /* CT face data, indexed on a (nt+1)^3 box */
   int ne[3];
   double *e[3][3], *aL[3], *aR[3], *dL[3], *dR[3], *Ee[3];
+  double *sv[3];   /* CT_CONTACT: sign of the face's mass flux */
   /* pencil buffers */
   int pmax;
   double *pv, *pvL, *pvR, *pflux, *pcmax, *pBn, *pq, *pqL, *pqR;
@@ -1200,12 +1201,15 @@ static void Sweep(orc_t *o, int dir, double dt) {
         else if (o->c.solver == ORC_TVDLF) cmax[i] = MHD_TVDLF(o, dir, vl, vr, f, e);
         else if (o->c.solver == ORC_HLLC)  cmax[i] = MHD_HLLC(o, dir, vl, vr, f, e);
         else                               cmax[i] = MHD_HLL(o, dir, vl, vr, f, e);
-        if (o->c.ct == ORC_ARITHMETIC) {
+        if (o->c.ct == ORC_ARITHMETIC || o->c.ct == ORC_CT_CONTACT) {
           /* CT_Store_Arith, Src/MHD/CT/ct_store.hpp:74-93 (replaces the
-             UCT data the solver stored) */
+             UCT data the solver stored); CT_CONTACT adds the sign of the
+             mass flux, zero within eps_CT_CONTACT = 1e-6 (ct.hpp:110) */
           int DIRt = (dir+1)%3, DIRb = (dir+2)%3;
           o->e[DIRb][dir][e] = -f[BX1 + DIRt];
           o->e[DIRt][dir][e] =  f[BX1 + DIRb];
+          if (o->c.ct == ORC_CT_CONTACT)
+            o->sv[dir][e] = f[RHO] > 1.e-6 ? 1.0 : (f[RHO] < -1.e-6 ? -1.0 : 0.0);
         }
       } else if (o->c.physics == ORC_HD) {
         if (o->c.solver == ORC_HLLC)       cmax[i] = HD_HLLC(o, dir, vl, vr, f);
@@ -1294,6 +1298,87 @@ static void ArrayRec(orc_t *o, int dir, int t1, int t2, int stag, const double *
   }
 }
 
+/* CT_CONTACT helpers: the cell-centred inductive field E = -v x B of
+   CT_ComputeCenterEMF (Src/MHD/CT/ct_emf.cpp:333-367) and the upwind weight
+   of a face's contact sign (Src/MHD/CT/ct_emf_average.cpp:137-143). */
+static double Ecc(orc_t *o, int comp, int i, int j, int k) {
+  double vx1 = *VC(o, o->Vc, VX1, i, j, k), vx2 = *VC(o, o->Vc, VX1+1, i, j, k);
+  double vx3 = *VC(o, o->Vc, VX1+2, i, j, k);
+  double Bx1 = *VC(o, o->Vc, BX1, i, j, k), Bx2 = *VC(o, o->Vc, BX2, i, j, k);
+  double Bx3 = *VC(o, o->Vc, BX3, i, j, k);
+  if (comp == 0) return (vx3*Bx2 - vx2*Bx3);
+  if (comp == 1) return (vx1*Bx3 - vx3*Bx1);
+  return (vx2*Bx1 - vx1*Bx2);
+}
+static double ContactW(double s) { return s != 0.0 ? (s > 0.0 ? 1.0 : 0.0) : 0.5; }
+
+/* CT_ComputeEMF with CT_EMF_AVERAGE CT_CONTACT (Src/MHD/CT/ct_emf.cpp:220-245):
+   the four face EMFs summed (CT_EMF_ArithmeticAverage with w = 1), the
+   upwinded derivative terms of CT_EMF_IntegrateToCorner
+   (Src/MHD/CT/ct_emf_average.cpp:115-290, Gardiner & Stone 2005), then
+   times 1/4.  Each edge in one pass, in the reference's operation order. */
+static void ContactEMF(orc_t *o, int ib, int ie, int jb, int je, int kb, int ke) {
+  const int ndim = o->c.ndim;
+  int i, j, k;
+  double **e0 = o->e[0], **e1 = o->e[1], **e2 = o->e[2];
+#define EE(A, ii, jj, kk) (A)[EI(o, ii, jj, kk)]
+  for (k = kb; k <= ke; k++)
+  for (j = jb; j <= je; j++)
+  for (i = ib; i <= ie; i++) {
+    double wS, wN, wW, wE, E;
+    /* Ez at (i-1/2, j-1/2, k) */
+    E = 1.0*(  EE(e2[0], i, j, k) + EE(e2[0], i, j-1, k)
+             + EE(e2[1], i, j, k) + EE(e2[1], i-1, j, k));
+    wS = ContactW(EE(o->sv[0], i, j-1, k));
+    wN = ContactW(EE(o->sv[0], i, j, k));
+    E +=   wS*(EE(e2[1], i-1, j, k) - Ecc(o, 2, i-1, j-1, k))
+         + (1.0-wS)*(EE(e2[1], i, j, k) - Ecc(o, 2, i, j-1, k))
+         - wN*(Ecc(o, 2, i-1, j, k) - EE(e2[1], i-1, j, k))
+         - (1.0-wN)*(Ecc(o, 2, i, j, k) - EE(e2[1], i, j, k));
+    wW = ContactW(EE(o->sv[1], i-1, j, k));
+    wE = ContactW(EE(o->sv[1], i, j, k));
+    E +=   wW*(EE(e2[0], i, j-1, k) - Ecc(o, 2, i-1, j-1, k))
+         + (1.0-wW)*(EE(e2[0], i, j, k) - Ecc(o, 2, i-1, j, k))
+         - wE*(Ecc(o, 2, i, j-1, k) - EE(e2[0], i, j-1, k))
+         - (1.0-wE)*(Ecc(o, 2, i, j, k) - EE(e2[0], i, j, k));
+    EE(o->Ee[2], i, j, k) = E*0.25;
+    if (ndim < 3) continue;
+    /* Ex at (i, j-1/2, k-1/2) */
+    E = 1.0*(  EE(e0[2], i, j, k) + EE(e0[2], i, j-1, k)
+             + EE(e0[1], i, j, k) + EE(e0[1], i, j, k-1));
+    wS = ContactW(EE(o->sv[1], i, j, k-1));
+    wN = ContactW(EE(o->sv[1], i, j, k));
+    E +=   wS*(EE(e0[2], i, j-1, k) - Ecc(o, 0, i, j-1, k-1))
+         + (1.0-wS)*(EE(e0[2], i, j, k) - Ecc(o, 0, i, j, k-1))
+         - wN*(Ecc(o, 0, i, j-1, k) - EE(e0[2], i, j-1, k))
+         - (1.0-wN)*(Ecc(o, 0, i, j, k) - EE(e0[2], i, j, k));
+    wW = ContactW(EE(o->sv[2], i, j-1, k));
+    wE = ContactW(EE(o->sv[2], i, j, k));
+    E +=   wW*(EE(e0[1], i, j, k-1) - Ecc(o, 0, i, j-1, k-1))
+         + (1.0-wW)*(EE(e0[1], i, j, k) - Ecc(o, 0, i, j-1, k))
+         - wE*(Ecc(o, 0, i, j, k-1) - EE(e0[1], i, j, k-1))
+         - (1.0-wE)*(Ecc(o, 0, i, j, k) - EE(e0[1], i, j, k));
+    EE(o->Ee[0], i, j, k) = E*0.25;
+    /* Ey at (i-1/2, j, k-1/2) */
+    E = 1.0*(  EE(e1[0], i, j, k) + EE(e1[0], i, j, k-1)
+             + EE(e1[2], i, j, k) + EE(e1[2], i-1, j, k));
+    wS = ContactW(EE(o->sv[2], i-1, j, k));
+    wN = ContactW(EE(o->sv[2], i, j, k));
+    E +=   wS*(EE(e1[0], i, j, k-1) - Ecc(o, 1, i-1, j, k-1))
+         + (1.0-wS)*(EE(e1[0], i, j, k) - Ecc(o, 1, i-1, j, k))
+         - wN*(Ecc(o, 1, i, j, k-1) - EE(e1[0], i, j, k-1))
+         - (1.0-wN)*(Ecc(o, 1, i, j, k) - EE(e1[0], i, j, k));
+    wW = ContactW(EE(o->sv[0], i, j, k-1));
+    wE = ContactW(EE(o->sv[0], i, j, k));
+    E +=   wW*(EE(e1[2], i-1, j, k) - Ecc(o, 1, i-1, j, k-1))
+         + (1.0-wW)*(EE(e1[2], i, j, k) - Ecc(o, 1, i, j, k-1))
+         - wE*(Ecc(o, 1, i-1, j, k) - EE(e1[2], i-1, j, k))
+         - (1.0-wE)*(Ecc(o, 1, i, j, k) - EE(e1[2], i, j, k));
+    EE(o->Ee[1], i, j, k) = E*0.25;
+  }
+#undef EE
+}
+
 static void ComputeEMF(orc_t *o) {
   const int ndim = o->c.ndim;
   /* Src/MHD/CT/ct_emf_average.cpp:553-559: MC for B and the scheme limiter
@@ -1310,6 +1395,10 @@ static void ComputeEMF(orc_t *o) {
   double *qL2 = o->pflux, *qR2 = o->pcmax;
   (void)vL; (void)vR;
 
+  if (o->c.ct == ORC_CT_CONTACT) {
+    ContactEMF(o, ib, ie, jb, je, kb, ke);
+    return;
+  }
   if (o->c.ct == ORC_ARITHMETIC) {
     /* CT_EMF_ArithmeticAverage (Src/MHD/CT/ct_emf_average.cpp:36-96),
        w = 0.25, each edge from the four face EMFs around it */
@@ -1690,6 +1779,7 @@ void *orc_create(const orc_cfg *cfg) {
       o->dL[d] = calloc(ne, sizeof(double));
       o->dR[d] = calloc(ne, sizeof(double));
       o->Ee[d] = calloc(ne, sizeof(double));
+      o->sv[d] = calloc(ne, sizeof(double));
       for (e = 0; e < 3; e++) o->e[d][e] = calloc(ne, sizeof(double));
     }
   }
@@ -1716,6 +1806,7 @@ void orc_destroy(void *h) {
   for (d = 0; d < 3; d++) {
     free(o->Vs[d]); free(o->Bs0[d]); free(o->Rs[d]);
     free(o->aL[d]); free(o->aR[d]); free(o->dL[d]); free(o->dR[d]); free(o->Ee[d]);
+    free(o->sv[d]);
     for (e = 0; e < 3; e++) free(o->e[d][e]);
   }
   free(o->pv); free(o->pvL); free(o->pvR); free(o->pflux); free(o->pcmax);

@@ -14,7 +14,7 @@ enum { ORC_LIM_FLAT = 0, ORC_LIM_MINMOD = 1, ORC_LIM_VL = 2, ORC_LIM_MC = 3,
        ORC_LIM_WENOZ = 9 /* RECONSTRUCTION WENOZ (no slope limiter) */,
        ORC_LIM_LIMO3 = 10, ORC_LIM_WENO3 = 11 /* RECONSTRUCTION LimO3 / WENO3 */ };
 enum { ORC_HLL = 0, ORC_HLLC = 1, ORC_HLLD = 2, ORC_TVDLF = 3 };
-enum { ORC_UCT_HLL = 0, ORC_UCT_HLLD = 1, ORC_ARITHMETIC = 2 };
+enum { ORC_UCT_HLL = 0, ORC_UCT_HLLD = 1, ORC_ARITHMETIC = 2, ORC_CT_CONTACT = 3 };
 
 typedef struct {
   int physics, ndim;

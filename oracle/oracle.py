@@ -18,7 +18,7 @@ HD, MHD, RMHD = 0, 1, 2
 LIM = {"flat": 0, "minmod": 1, "vl": 2, "vanleer": 2, "mc": 3, "ppm": 4, "mp5": 5,
        "vanalbada": 6, "ospre": 7, "umist": 8, "wenoz": 9, "limo3": 10, "weno3": 11}
 SOLVER = {"hll": 0, "hllc": 1, "hlld": 2, "tvdlf": 3}
-CT = {"uct_hll": 0, "uct_hlld": 1, "arithmetic": 2}
+CT = {"uct_hll": 0, "uct_hlld": 1, "arithmetic": 2, "ct_contact": 3}
 
 
 class OrcCfg(ctypes.Structure):

@@ -225,6 +225,25 @@ CASES = {
                               dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="tvdlf",
                                    ct_emf="ARITHMETIC", cfl=0.4, first_dt=1e-4,
                                    reconstruction="PARABOLIC"), 10),
+    # CT_EMF_AVERAGE CT_CONTACT (face EMFs + contact-upwinded corner terms)
+    "mhd2d_mc_hlld_contact": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=201),
+                              dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hlld",
+                                   ct_emf="CT_CONTACT", cfl=0.4, first_dt=1e-4), 12),
+    "mhd3d_mc_hlld_contact": (ics.mhd3d_turbulence, dict(n=(12, 10, 9), seed=202),
+                              dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="hlld",
+                                   ct_emf="CT_CONTACT", cfl=0.4, first_dt=1e-4), 8),
+    "mhd3d_vl_hll_contact_outflowy": (
+        ics.mhd3d_turbulence, dict(n=(12, 10, 9), seed=203),
+        dict(physics="MHD", ndim=3, limiter="VANLEER_LIM", solver="hll", ct_emf="CT_CONTACT",
+             cfl=0.4, first_dt=1e-4, bc=("periodic", "outflow", "periodic")), 6),
+    "mhd2d_ppm_hllc_contact_rk3": (ics.mhd2d_turbulence, dict(n=(22, 18), seed=204),
+                                   dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hllc",
+                                        ct_emf="CT_CONTACT", cfl=0.4, first_dt=1e-4,
+                                        reconstruction="PARABOLIC", rk="RK3"), 10),
+    "mhd3d_blast_mc_tvdlf_contact_reflect": (
+        ics.mhd3d_blast, dict(n=(14, 12, 10), seed=205, radius=0.25),
+        dict(physics="MHD", ndim=3, limiter="MC_LIM", solver="tvdlf", ct_emf="CT_CONTACT",
+             cfl=0.4, first_dt=1e-4, bc=("reflective", "reflective", "reflective")), 6),
     # HLLC for MHD (Src/MHD/hllc.cpp): UCT_HLL and ARITHMETIC face data
     "mhd2d_mc_hllc_ucthll": (ics.mhd2d_turbulence, dict(n=(24, 20), seed=191),
                              dict(physics="MHD", ndim=2, limiter="MC_LIM", solver="hllc",

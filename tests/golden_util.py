@@ -13,6 +13,7 @@ GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 LIMITER = {"MC_LIM": "mc", "VANLEER_LIM": "vl", "MINMOD_LIM": "minmod", "FLAT_LIM": "flat",
            "VANALBADA_LIM": "vanalbada", "OSPRE_LIM": "ospre", "UMIST_LIM": "umist"}
 CT = {"UCT_HLLD": "uct_hlld", "UCT_HLL": "uct_hll", "ARITHMETIC": "arithmetic",
+      "CT_CONTACT": "ct_contact",
       "none": "uct_hll"}
 
 

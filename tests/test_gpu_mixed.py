@@ -73,6 +73,8 @@ MIXED_SCHEMES = [
      dict(), 2, 12),
     (ics.mhd3d_turbulence, dict(n=(36, 32, 28), seed=127), "mc", "hllc", "uct_hll",
      dict(), 2, 12),
+    (ics.mhd3d_turbulence, dict(n=(36, 32, 28), seed=128), "mc", "hlld", "ct_contact",
+     dict(), 2, 12),
 ]
 
 

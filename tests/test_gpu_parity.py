@@ -75,6 +75,11 @@ CASES = [
     # CT_EMF_AVERAGE ARITHMETIC
     (ics.mhd3d_turbulence, dict(n=(13, 11, 9), seed=191), "mc", "hlld", "arithmetic", 6),
     (ics.mhd2d_turbulence, dict(n=(27, 19), seed=192), "vl", "tvdlf", "arithmetic", 10),
+    # CT_EMF_AVERAGE CT_CONTACT on odd sizes
+    (ics.mhd3d_turbulence, dict(n=(13, 11, 9), seed=206), "vl", "hlld", "ct_contact", 6),
+    (ics.mhd2d_turbulence, dict(n=(29, 17), seed=207), "mc", "hllc", "ct_contact", 10),
+    (ics.mhd3d_blast, dict(n=(15, 13, 11), seed=208, radius=0.25), "ppm", "tvdlf",
+     "ct_contact", 6),
     # HLLC for MHD (UCT_HLL and ARITHMETIC face data)
     (ics.mhd3d_turbulence, dict(n=(17, 13, 11), seed=195), "mc", "hllc", "uct_hll", 6),
     (ics.mhd2d_turbulence, dict(n=(31, 23), seed=196), "ppm", "hllc", "arithmetic", 10),
