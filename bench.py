@@ -354,6 +354,35 @@ def measure_e2e(make_solver, ncell, steps, ranks):
             "path": "gp_upload_state(reference layout, pinned host) + gp_advance_step + "
                     "gp_download_state(reference layout) per step"}
 
+def fp64_roofline(per_kernel, top, ncell, ms_step, clocks):
+    """The FP64 pipe as the roof of the FP64 form: FP64 flops per cell of
+    each kernel (2 x DFMA + DADD + DMUL thread instructions counted by ncu on
+    the same kernels, profiles/fp64_ops.json) x cells / the kernel's CUDA-event
+    time, against the hardware's DFMA rate (ncu's peak_sustained DFMA thread
+    instructions per cycle, x 2 flop) at the SM clock sampled in the run."""
+    path = os.path.join(ROOT, "profiles", "fp64_ops.json")
+    if not os.path.exists(path):
+        return None
+    ops = json.load(open(path))
+    mhz = (clocks or {}).get("sm_mhz") or ops["sm_mhz_nominal"]
+    peak = 2.0 * ops["dfma_per_cycle"] * mhz * 1e6 / 1e12
+    per = ops["flop_per_cell"]
+
+    def key(k):
+        return f"{k['kernel']}_stage{k['stage']}" if k["kernel"] == "finish" else k["kernel"]
+    step_flop = sum(per.get(key(k), 0.0) for k in per_kernel) * ncell
+    top_flop = per.get(key(top), 0.0) * ncell
+    ach = top_flop / (top["ms"] * 1e-3) / 1e12
+    step_ach = step_flop / (ms_step * 1e-3) / 1e12
+    return {"bound": "fp64", "kernel": f"{top['kernel']} (stage {top['stage']})",
+            "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+            "flop_per_cell": per.get(key(top)),
+            "pipe_active_pct_ncu": ops.get("pipe_active_pct", {}).get(key(top)),
+            "peak_kind": "hardware DFMA rate (ncu peak_sustained) at the sampled SM clock",
+            "step": {"flop_per_zone_update": step_flop / ncell, "achieved": step_ach,
+                     "frac": step_ach / peak}}
+
+
 # --------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------
@@ -427,6 +456,9 @@ def impl_ours(args):
                 "alg_bytes_per_launch": top_bytes, "launch_ms": top["ms"],
                 "step": {"alg_bytes_per_zone_update": ALG_BYTES_ZONE, "achieved": step_gbs,
                          "frac": step_gbs / peak}}
+    fp64 = fp64_roofline(per_kernel, top, ncell, ms_step, clocks)
+    if fp64 is not None:
+        roofline["fp64"] = fp64
 
     # ---- mixed FP32-flux form ------------------------------------------
     mixed = None

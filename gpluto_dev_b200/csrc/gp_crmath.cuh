@@ -27,15 +27,21 @@
 //
 // The double-double value is rounded once; the result is the correctly
 // rounded one unless the exact value lies within ~2^-47 ulp of a rounding
-// midpoint.  The functions compile for the host as well, where the CPU tests
-// check them against binary128 on dense argument sweeps.
+// midpoint.  That full-accuracy path is the slow path: each function first
+// evaluates a fast form (the three leading terms exact, the rest in double,
+// error below 2^-68 absolute or 2^-63 relative) and returns its rounding when
+// every value within twice that error rounds the same way (Ziv's strategy,
+// as in CRlibm); about one call in a thousand defers to the slow path.  The functions compile for the host as well, where the
+// CPU tests check them against binary128 on dense argument sweeps.
 #pragma once
 #include <math.h>
 
 #if defined(__CUDACC__)
 #define GP_CR_FN __host__ __device__ __forceinline__
+#define GP_CR_SLOW static __host__ __device__ __noinline__
 #else
 #define GP_CR_FN static inline
+#define GP_CR_SLOW static
 #endif
 
 namespace gpcr {
@@ -111,15 +117,21 @@ GP_CR_FN dd dd_mul_d(dd a, double b) {
     {0x1.cdf604a1cadcep-1, -0x1.6b50757f2fa40p-56, 0x1.b9865639d0596p-2, -0x1.931bd06786cb9p-56}, \
   }
 
+// Global rather than constant memory: the lanes of a warp index different
+// entries, which the constant cache would serialise.
 #if defined(__CUDACC__)
-static __constant__ double kSinCosTable[19][4] = GP_CR_TABLE;
+static __device__ const double kSinCosTable[19][4] = GP_CR_TABLE;
 #endif
 static const double kSinCosTableHost[19][4] = GP_CR_TABLE;
+
+GP_CR_FN double sincos_tab(int j, int k) {
 #if defined(__CUDA_ARCH__)
-#define GP_CR_TAB kSinCosTable
+  return __ldg(&kSinCosTable[j][k]);
 #else
-#define GP_CR_TAB kSinCosTableHost
+  return kSinCosTableHost[j][k];
 #endif
+}
+#define GP_CR_TAB_J(j, k) sincos_tab(j, k)
 
 // double-double sin and cos of x in [0, 1.125]
 GP_CR_FN void sincos_dd(double x, dd& s, dd& c) {
@@ -141,14 +153,25 @@ GP_CR_FN void sincos_dd(double x, dd& s, dd& c) {
   pc = dd_add(dd_mul(z, pc), {0x1.5555555555555p-5, 0x1.5555555555555p-59});
   pc = dd_add(dd_mul(z, pc), {-0.5, 0.0});
   const dd cr = dd_add_d(dd_mul(z, pc), 1.0);
-  const dd sj = {GP_CR_TAB[j][0], GP_CR_TAB[j][1]};
-  const dd cj = {GP_CR_TAB[j][2], GP_CR_TAB[j][3]};
+  const dd sj = {GP_CR_TAB_J(j, 0), GP_CR_TAB_J(j, 1)};
+  const dd cj = {GP_CR_TAB_J(j, 2), GP_CR_TAB_J(j, 3)};
   s = dd_add(dd_mul(sj, cr), dd_mul(cj, sr));
   c = dd_add(dd_mul(cj, cr), dd_neg(dd_mul(sj, sr)));
 }
 
-// correctly rounded sin(x) and cos(x), 0 <= x <= 1.125
-GP_CR_FN void sincos_cr(double x, double* sn, double* cs) {
+// ---------------------------------------------------------------------
+// Full-accuracy paths (relative error ~2^-100), out of line: taken only when
+// the fast paths below cannot decide the rounding.
+// ---------------------------------------------------------------------
+#if defined(GP_CR_COUNT_SLOW) && !defined(__CUDA_ARCH__)
+extern long gp_cr_slow_calls;  // host test builds: how often the fast path defers
+#define GP_CR_NOTE_SLOW() (++gp_cr_slow_calls)
+#else
+#define GP_CR_NOTE_SLOW() ((void)0)
+#endif
+
+GP_CR_SLOW void sincos_slow(double x, double* sn, double* cs) {
+  GP_CR_NOTE_SLOW();
   dd s, c;
   sincos_dd(x, s, c);
   *sn = s.hi + s.lo;
@@ -167,8 +190,8 @@ GP_CR_FN dd asin_dd(dd s) {
   return two_sum(y0, delta);
 }
 
-// correctly rounded acos(x), -1 <= x <= 1
-GP_CR_FN double acos_cr(double x) {
+GP_CR_SLOW double acos_slow(double x) {
+  GP_CR_NOTE_SLOW();
   const dd kPi = {0x1.921fb54442d18p+1, 0x1.1a62633145c07p-53};
   const dd kPi2 = {0x1.921fb54442d18p+0, 0x1.1a62633145c07p-54};
   if (fabs(x) <= 0.5) {
@@ -182,6 +205,138 @@ GP_CR_FN double acos_cr(double x) {
   y = {2.0 * y.hi, 2.0 * y.lo};
   if (x < 0.0) y = dd_add(kPi, dd_neg(y));
   return y.hi + y.lo;
+}
+
+// ---------------------------------------------------------------------
+// Fast paths (Ziv's strategy): evaluate with a proven error bound, and
+// return the double nearest to the result only when every value within that
+// bound rounds to it; otherwise fall back to the full-accuracy path.
+// ---------------------------------------------------------------------
+
+// The double nearest to y when every value within err of y rounds the same
+// way (y = hi + lo normalised; rounding is monotonic, so both ends suffice).
+GP_CR_FN bool round_certain(dd y, double err, double* out) {
+  const double a = y.hi + (y.lo + err);
+  const double b = y.hi + (y.lo - err);
+  *out = a;
+  return a == b;
+}
+
+// sin and cos of x in [0, 1.125] as unevaluated sums.  With j = round(16 x),
+// r = x - j/16 (exact, |r| <= 1/32), z = r^2 = zh + zl (exact),
+// cm = cos r - 1 = -zh/2 + cml and sm = sin r - r:
+//   sin x = Sj + Cj r + Sj (-zh/2) + [rest], cos x = Cj - Sj r + Cj (-zh/2) + [rest]
+// where the three leading terms are formed exactly (Dekker products, Knuth
+// sums) and the rest (below 2^-17) in double.  Error: for j >= 1 below 2^-68
+// absolute for both (the double products Cj*sm, Sj*sm and sm's own rounding
+// dominate: |sm| <= 2^-17.6, three roundings); for j = 0 (x < 1/32, Sj = 0,
+// Cj = 1) sin x = r + sm to 2^-63 relative and cos x = 1 - zh/2 + cml to
+// 2^-75.  Measured against binary128 on 4 million arguments: 2^-68.7
+// absolute (j >= 1, sin and cos), 2^-64.2 relative (j = 0, sin).  Returned
+// with the bounds the rounding test uses: 2^-67 absolute, 2^-62 relative.
+GP_CR_FN void sincos_fast(double x, dd& s, dd& c, double& es, double& ec) {
+  const int j = (int)(x * 16.0 + 0.5);
+  const double r = x - (double)j * 0.0625;
+  const dd z = two_prod(r, r);
+  const double zh = z.hi;
+  // cm = -z/2 + z^2 (1/4! - z/6! + z^2/8! - z^3/10!)
+  const double q = fma(zh, fma(zh, fma(zh, -0x1.27e4fb7789f5cp-22, 0x1.a01a01a01a01ap-16),
+                               -0x1.6c16c16c16c17p-10),
+                       0x1.5555555555555p-5);
+  const double cmh = -0.5 * zh;                    // exact
+  const double cml = fma(zh * zh, q, -0.5 * z.lo);
+  // sm = r z (-1/3! + z (1/5! - z/7! + z^2/9!))
+  const double p = fma(zh, fma(zh, fma(zh, 0x1.71de3a556c734p-19, -0x1.a01a01a01a01ap-13),
+                               0x1.1111111111111p-7),
+                       -0x1.5555555555555p-3);
+  const double sm = r * fma(zh, p, z.lo * -0x1.5555555555555p-3);
+  const double Sh = GP_CR_TAB_J(j, 0), Sl = GP_CR_TAB_J(j, 1);
+  const double Ch = GP_CR_TAB_J(j, 2), Cl = GP_CR_TAB_J(j, 3);
+  {  // sin
+    const dd a = two_prod(Ch, r);
+    const dd b = two_prod(Sh, cmh);
+    const dd t1 = two_sum(Sh, a.hi);
+    const dd t2 = two_sum(t1.hi, b.hi);
+    double rest = a.lo + b.lo;
+    rest += Sl;
+    rest += Sh * cml;
+    rest += Cl * r;
+    rest += Sl * cmh;
+    rest += Cl * sm;
+    rest += t1.lo + t2.lo;
+    rest += Ch * sm;
+    s = fast_two_sum(t2.hi, rest);
+  }
+  {  // cos
+    const dd a = two_prod(Sh, r);
+    const dd b = two_prod(Ch, cmh);
+    const dd t1 = two_sum(Ch, -a.hi);
+    const dd t2 = two_sum(t1.hi, b.hi);
+    double rest = b.lo - a.lo;
+    rest += Cl;
+    rest += Ch * cml;
+    rest -= Sl * r;
+    rest += Cl * cmh;
+    rest -= Sl * sm;
+    rest += t1.lo + t2.lo;
+    rest -= Sh * sm;
+    c = fast_two_sum(t2.hi, rest);
+  }
+  es = j == 0 ? 0x1p-62 * fabs(s.hi) : 0x1p-67;
+  ec = 0x1p-67;
+}
+
+// correctly rounded sin(x) and cos(x), 0 <= x <= 1.125
+GP_CR_FN void sincos_cr(double x, double* sn, double* cs) {
+  dd s, c;
+  double es, ec;
+  sincos_fast(x, s, c, es, ec);
+  const bool ok = round_certain(s, es, sn) & round_certain(c, ec, cs);
+  if (!ok) sincos_slow(x, sn, cs);
+}
+
+// correctly rounded acos(x), -1 <= x <= 1: the Newton step of asin_dd on the
+// fast sin (its error carried through: |d asin / d sin| = 1/cos <= 1.16 on
+// [-1/2, 1/2], doubled where acos = 2 asin), then the rounding test.
+GP_CR_FN double acos_cr(double x) {
+  const double kPih = 0x1.921fb54442d18p+1, kPil = 0x1.1a62633145c07p-53;
+  const double kPi2h = 0x1.921fb54442d18p+0, kPi2l = 0x1.1a62633145c07p-54;
+  const bool mid = fabs(x) <= 0.5;
+  double sh, sl;
+  if (mid) {
+    sh = x;
+    sl = 0.0;
+  } else {
+    const double t = (x > 0.0 ? 1.0 - x : 1.0 + x) * 0.5;   // exact
+    sh = sqrt(t);
+    sl = sh > 0.0 ? fma(-sh, sh, t) / (2.0 * sh) : 0.0;
+  }
+  const double y0 = asin(sh);
+  dd sy, cy;
+  double es, ec;
+  sincos_fast(fabs(y0), sy, cy, es, ec);
+  if (y0 < 0.0) sy = dd_neg(sy);
+  // s - sin(y0): the high parts are within a few ulps (exact difference)
+  const double e = (sh - sy.hi) + (sl - sy.lo);
+  const double delta = e / cy.hi;
+  dd y;
+  double err = 1.25 * es;
+  if (mid) {
+    const dd t = two_sum(kPi2h, -y0);
+    y = fast_two_sum(t.hi, (t.lo - delta) + kPi2l);
+  } else if (x > 0.0) {
+    y = fast_two_sum(2.0 * y0, 2.0 * delta);
+    err *= 2.0;
+  } else {
+    const dd t = two_sum(kPih, -2.0 * y0);
+    y = fast_two_sum(t.hi, (t.lo - 2.0 * delta) + kPil);
+    err *= 2.0;
+  }
+  // + the Newton step's own terms (quadratic in a few ulps, relative)
+  err += 0x1p-98 * fabs(y.hi);
+  double r;
+  if (round_certain(y, err, &r)) return r;
+  return acos_slow(x);
 }
 
 }  // namespace gpcr

@@ -203,6 +203,9 @@ __device__ __forceinline__ void cell_update(const StageArgs<CTT>& a, long long n
       if (!rhs_var<PHYS, NDIM>(nv)) continue;
       du[nv * n + c] = (CTT)(-dtdx * ((double)Fr[nv] - (double)Fl[nv]));
     }
+    // stored in every stage although only stage 1's CFL maximum reads it
+    // (Src/update_stage.cpp:422-435): a store conditional on the stage made
+    // the FP64 y/z sweeps 40% slower at 256^3
     a.Cdt[(long long)dir * n + c] = (CTT)(0.5 * ((double)cml + (double)cmr) / a.dx[dir]);
   } else {
     // mixed form: the stored difference is FP32, so it is formed in FP32
@@ -217,12 +220,17 @@ __device__ __forceinline__ void cell_update(const StageArgs<CTT>& a, long long n
   }
 }
 
-template <typename R, typename CTT>
+// Face data for the edge EMFs: the two face EMFs and, for the upwind
+// averages, the four weights; CT_CONTACT keeps one weight (the contact's),
+// ARITHMETIC none.
+template <int CT, typename R, typename CTT>
 __device__ __forceinline__ void store_ct(const StageArgs<CTT>& a, int dir, long long f,
                                          const CTFace<R>& ct) {
   a.ct[dir][0][f] = (CTT)ct.eb;
   a.ct[dir][1][f] = (CTT)ct.et;
+  if constexpr (CT == CT_ARITH) return;
   a.ct[dir][2][f] = (CTT)ct.aL;
+  if constexpr (CT == CT_CONTACT) return;
   a.ct[dir][3][f] = (CTT)ct.aR;
   a.ct[dir][4][f] = (CTT)ct.dL;
   a.ct[dir][5][f] = (CTT)ct.dR;
@@ -364,7 +372,7 @@ __device__ __forceinline__ void sweep_x_row_ppm(const StageArgs<CTT>& a, const G
       if (act && rhs_var<PHYS, NDIM>(nv) && isnan(F[nv])) fe |= ERR_NAN | ERR_QUIT;
     if (fe && face_counts(g, 0, f, 1, row % g.ny, 2, row / g.ny)) err |= fe;
     if constexpr (PHYS != PHYS_HD) {
-      if (act) store_ct(a, 0, rb + f, ct);
+      if (act) store_ct<CT>(a, 0, rb + f, ct);
     }
     R Fm1[NV];
 #pragma unroll
@@ -538,7 +546,7 @@ __device__ __forceinline__ void sweep_x_row_mp5(const StageArgs<CTT>& a, const G
       if (act && rhs_var<PHYS, NDIM>(nv) && isnan(F[nv])) fe |= ERR_NAN | ERR_QUIT;
     if (fe && face_counts(g, 0, f, 1, row % g.ny, 2, row / g.ny)) err |= fe;
     if constexpr (PHYS != PHYS_HD) {
-      if (act) store_ct(a, 0, rb + f, ct);
+      if (act) store_ct<CT>(a, 0, rb + f, ct);
     }
     R Fm1[NV];
 #pragma unroll
@@ -717,7 +725,7 @@ __device__ __forceinline__ void sweep_x_row(const StageArgs<CTT>& a, const Grid3
       if (act && rhs_var<PHYS, NDIM>(nv) && isnan(F[nv])) fe |= ERR_NAN | ERR_QUIT;
     if (fe && face_counts(g, 0, f, 1, row % g.ny, 2, row / g.ny)) err |= fe;
     if constexpr (PHYS != PHYS_HD) {
-      if (act) store_ct(a, 0, rb + f, ct);
+      if (act) store_ct<CT>(a, 0, rb + f, ct);
     }
     // flux of face f-1 and cell update of cell f-1
     R Fm1[NV];
@@ -854,7 +862,7 @@ __device__ __forceinline__ void sweep_m_col_ppm(const StageArgs<CTT>& a, const G
         if (rhs_var<PHYS, NDIM>(nv) && isnan(F[nv])) fe |= ERR_NAN | ERR_QUIT;
       if (fe && face_counts(g, DIR, m, 0, i, DIR == 1 ? 2 : 1, t)) err |= fe;
       if constexpr (PHYS != PHYS_HD) {
-        if (m < m1) store_ct(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
+        if (m < m1) store_ct<CT>(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
       }
       if (m > m0)
         cell_update<PHYS, NV, NDIM>(a, n, base + (long long)(m - 1) * stride, Fp, F, cmp, cm,
@@ -946,7 +954,7 @@ __device__ __forceinline__ void sweep_m_col_mp5(const StageArgs<CTT>& a, const G
         if (rhs_var<PHYS, NDIM>(nv) && isnan(F[nv])) fe |= ERR_NAN | ERR_QUIT;
       if (fe && face_counts(g, DIR, m, 0, i, DIR == 1 ? 2 : 1, t)) err |= fe;
       if constexpr (PHYS != PHYS_HD) {
-        if (m < m1) store_ct(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
+        if (m < m1) store_ct<CT>(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
       }
       if (m > m0)
         cell_update<PHYS, NV, NDIM>(a, n, base + (long long)(m - 1) * stride, Fp, F, cmp, cm,
@@ -1070,7 +1078,7 @@ __device__ __forceinline__ void sweep_m_col(const StageArgs<CTT>& a, const Grid3
         if (rhs_var<PHYS, NDIM>(nv) && isnan(F[nv])) fe |= ERR_NAN | ERR_QUIT;
       if (fe && face_counts(g, DIR, m, 0, i, DIR == 1 ? 2 : 1, t)) err |= fe;
       if constexpr (PHYS != PHYS_HD) {
-        if (m < m1) store_ct(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
+        if (m < m1) store_ct<CT>(a, DIR, base + (long long)gidx(m, nd, g.outflow, DIR) * stride, ct);
       }
       if (m > m0)
         cell_update<PHYS, NV, NDIM>(a, n, base + (long long)(m - 1) * stride, Fp, F, cmp, cm,
@@ -1809,8 +1817,10 @@ __device__ __forceinline__ double finish_cell(const StageArgs<CTT>& a, const Gri
       if (a.stage == 1) u[nv] = u0 + Rc;
       else u[nv] = a.w0 * u0 + a.w1 * a.Uc[nv * n + c] + a.wr * Rc;
     }
-    cdt = (double)a.Cdt[c] + (double)a.Cdt[n + c];
-    if (NDIM == 3) cdt = cdt + (double)a.Cdt[2 * n + c];
+    if (a.stage == 1) {  // the CFL maximum is a stage-1 quantity
+      cdt = (double)a.Cdt[c] + (double)a.Cdt[n + c];
+      if (NDIM == 3) cdt = cdt + (double)a.Cdt[2 * n + c];
+    }
     if constexpr (PHYS != PHYS_HD) {
       // 32-bit wrapped offsets of the index and its two successors along
       // each direction, formed once (grids hold fewer than 2^31 cells)

@@ -2,9 +2,16 @@
 // binary128 evaluations of the same functions (libquadmath) rounded once.
 #include <quadmath.h>
 #include <stddef.h>
+#define GP_CR_COUNT_SLOW 1
 #include "../gpluto_dev_b200/csrc/gp_crmath.cuh"
 
+namespace gpcr {
+long gp_cr_slow_calls = 0;
+}
+
 extern "C" {
+long crm_slow_calls(void) { return gpcr::gp_cr_slow_calls; }
+
 // which: 0 acos, 1 sin, 2 cos
 void crm_eval(int which, const double* x, double* ours, double* quad, size_t n) {
   for (size_t i = 0; i < n; i++) {

@@ -27,6 +27,7 @@ def crm():
     L = ctypes.CDLL(so)
     P = ctypes.POINTER(ctypes.c_double)
     L.crm_eval.argtypes = [ctypes.c_int, P, P, P, ctypes.c_size_t]
+    L.crm_slow_calls.restype = ctypes.c_long
 
     def ev(which, x):
         x = np.ascontiguousarray(x, dtype=np.float64)
@@ -34,6 +35,7 @@ def crm():
         L.crm_eval(which, x.ctypes.data_as(P), a.ctypes.data_as(P), b.ctypes.data_as(P),
                    x.size)
         return a, b
+    ev.slow_calls = L.crm_slow_calls
     return ev
 
 
@@ -80,3 +82,15 @@ def test_agrees_with_mpmath(crm):
     for a, so, co in zip(xs, s, c):
         assert float(mpmath.sin(mpmath.mpf(float(a)))) == so
         assert float(mpmath.cos(mpmath.mpf(float(a)))) == co
+
+
+def test_fast_path_decides_nearly_every_call(crm):
+    """The slow (full double-double) path runs only where the fast form
+    cannot decide the rounding: well under 1% of the calls the quartic makes."""
+    x = _acos_args(200_000, 9)
+    before = crm.slow_calls()
+    crm(0, x)                                   # acos
+    theta = np.arccos(x) / 3.0
+    crm(1, theta)                               # sin and cos share one slow call
+    slow = crm.slow_calls() - before
+    assert slow < 0.005 * 2 * x.size, slow
