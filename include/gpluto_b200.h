@@ -247,8 +247,12 @@ int gp_data_minmax(gp_handle *h, double *vmin, double *vmax, double *mach_max);
    GP_NOALLOC_MAX_CELLS cells return GP_ERR_INVALID.  The first call on a
    device looks up that array's device address (cudaGetSymbolAddress), so
    make it before any stream capture.  All calls share the array: calls
-   that overlap on the GPU race.  Returns a gp_status (no gp_last_error
-   text); `out` as for gp_advance_step. */
+   that overlap on the GPU race.  It accepts what gp_create accepts (same
+   checks, same cell widths: Grid::dx when given) restricted to RK2,
+   LINEAR or PARABOLIC reconstruction and periodic sides on every
+   direction; anything else returns GP_ERR_UNSUPPORTED.  Returns a
+   gp_status with the reason in gp_last_error(); `out` as for
+   gp_advance_step. */
 int gp_advance_step_noalloc(const gp_grid_desc *grid, const gp_scheme *scheme,
                             double *Uc, double *Vc, double *Vs0, double *Vs1, double *Vs2,
                             double dt, void *stream, gp_step_out *out);
