@@ -39,6 +39,7 @@ grids first.  value = zone updates of all grids / device time.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -348,11 +349,35 @@ def measure_e2e(make_solver, ncell, steps, ranks):
     te = time.perf_counter() - t0
     te = ranks.max_over_ranks(te)
     nbytes = (hU.numel() + hV.numel() + sum(b.numel() for b in hB if b is not None)) * 8
+    # resident use: the state goes up once and comes back
+    # once; every step is one gp_advance_step whose gp_step_out (error bits,
+    # invDt_hyp, next dt) the host reads -- all inside the timed region
+    kr = max(1, steps)
+    out = api.GpStepOut()
+    torch.cuda.synchronize()
+    ranks.barrier()
+    t0 = time.perf_counter()
+    api._check(L.gp_upload_state(se._h, api.LAYOUT_REFERENCE, api._dp(hU), api._dp(hV),
+                                 api._dp(hB[0]), api._dp(hB[1]), api._dp(hB[2])))
+    de = FIRST_DT
+    for _ in range(kr):
+        api._check(L.gp_advance_step(se._h, de, ctypes.byref(out)))
+        de = out.dt_next
+    dl()
+    torch.cuda.synchronize()
+    tr = ranks.max_over_ranks(time.perf_counter() - t0)
     se.close()
     return {"value": ranks.world * ncell * k / te / 1e6, "unit": METRIC,
             "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": k,
             "path": "gp_upload_state(reference layout, pinned host) + gp_advance_step + "
-                    "gp_download_state(reference layout) per step"}
+                    "gp_download_state(reference layout) per step",
+            "resident": {"value": ranks.world * ncell * kr / tr / 1e6, "unit": METRIC,
+                         "steps": kr, "h2d_bytes_per_step": nbytes / kr + 8,
+                         "d2h_bytes_per_step": nbytes / kr + ctypes.sizeof(out),
+                         "path": "state up once (pinned, reference layout), K x "
+                                 "gp_advance_step with its gp_step_out read by the host, "
+                                 "state down once; the drop-in driver's loop between "
+                                 "outputs"}}
 
 def fp64_roofline(per_kernel, top, ncell, ms_step, clocks):
     """The FP64 pipe as the roof of the FP64 form: FP64 flops per cell of
