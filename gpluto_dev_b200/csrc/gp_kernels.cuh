@@ -1918,8 +1918,16 @@ __device__ __forceinline__ void block_invdt_max(unsigned long long* bits, double
   }
 }
 
+// Resident 256-thread blocks per SM: the mixed form's 4-byte loads need
+// more requests in flight per byte than the FP64 form's to keep HBM busy.
+// Measured at 256^3: mixed 4 blocks 1.01/1.04 ms (stage 1/2), 5 blocks the
+// same, 6 blocks (40 registers) 0.92/0.97 ms, 8 blocks 1.12/1.17 ms; the
+// FP64 finish gains nothing from 6 (1.02/1.12 against 1.04/1.08 ms).
+template <typename CTT>
+__host__ __device__ constexpr int finish_minb() { return sizeof(CTT) == 4 ? 6 : 4; }
+
 template <int PHYS, int NV, int NDIM, typename CTT>
-__global__ void __launch_bounds__(256) finish_kernel(StageArgs<CTT> a, Grid3 g) {
+__global__ void __launch_bounds__(256, finish_minb<CTT>()) finish_kernel(StageArgs<CTT> a, Grid3 g) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const double cdt = finish_cell<PHYS, NV, NDIM, CTT>(a, g, c);
   if (a.stage == 1) block_invdt_max(a.invdt_bits, cdt);
