@@ -15,8 +15,8 @@ into ``oracle/_ref/dropin_<name>/``:
 
 then compiles it with every other source taken from the reference tree in
 place, plus ``oracle/ref/gp_dropin.cpp`` (ours), and links
-``gpluto_dev_b200/_build/libgpluto_b200.so`` (run-time path set to that
-directory).  The copy of main.cpp stays in the git-ignored build directory.
+``gpluto_dev_b200/_build/libgpluto_b200.so`` (run-time path relative to the
+binary).  The copy of main.cpp stays in the git-ignored build directory.
 
 ``run_dbl`` runs a binary (this one or the plain reference build) on a
 seeded initial condition with ``.dbl`` output every ``every`` steps and
@@ -67,8 +67,10 @@ def makefile(cfg: "br.RefConfig") -> str:
         elif line.startswith("INCS "):
             line += f" -I{INC_DIR}"
         elif line.startswith("LDFLAGS "):
-            line = (f"LDFLAGS = -L{LIB_DIR} -lgpluto_b200 -Wl,-rpath,{LIB_DIR} "
-                    f"-Wl,-rpath,/root/repo/gpluto_dev_b200/_build -lm")
+            # run-time path relative to the binary (oracle/_ref/<dir>/pluto),
+            # so that the driver finds the library wherever the tree is copied
+            line = (f"LDFLAGS = -L{LIB_DIR} -lgpluto_b200 "
+                    "-Wl,-rpath,'$$ORIGIN/../../../gpluto_dev_b200/_build' -lm")
         lines.append(line)
     return "\n".join(lines) + "\n"
 
