@@ -286,6 +286,42 @@ GP_CR_FN void sincos_fast(double x, dd& s, dd& c, double& es, double& ec) {
   ec = 0x1p-67;
 }
 
+// sin(x) as in sincos_fast (same terms, same bound es) and cos(x) to double
+// precision only: the Newton step of acos_cr divides by it, where relative
+// accuracy 2^-50 is ample.
+GP_CR_FN void sin_fast_cos_d(double x, dd& s, double& es, double& cd) {
+  const int j = (int)(x * 16.0 + 0.5);
+  const double r = x - (double)j * 0.0625;
+  const dd z = two_prod(r, r);
+  const double zh = z.hi;
+  const double q = fma(zh, fma(zh, fma(zh, -0x1.27e4fb7789f5cp-22, 0x1.a01a01a01a01ap-16),
+                               -0x1.6c16c16c16c17p-10),
+                       0x1.5555555555555p-5);
+  const double cmh = -0.5 * zh;
+  const double cml = fma(zh * zh, q, -0.5 * z.lo);
+  const double p = fma(zh, fma(zh, fma(zh, 0x1.71de3a556c734p-19, -0x1.a01a01a01a01ap-13),
+                               0x1.1111111111111p-7),
+                       -0x1.5555555555555p-3);
+  const double sm = r * fma(zh, p, z.lo * -0x1.5555555555555p-3);
+  const double Sh = GP_CR_TAB_J(j, 0), Sl = GP_CR_TAB_J(j, 1);
+  const double Ch = GP_CR_TAB_J(j, 2), Cl = GP_CR_TAB_J(j, 3);
+  const dd a = two_prod(Ch, r);
+  const dd b = two_prod(Sh, cmh);
+  const dd t1 = two_sum(Sh, a.hi);
+  const dd t2 = two_sum(t1.hi, b.hi);
+  double rest = a.lo + b.lo;
+  rest += Sl;
+  rest += Sh * cml;
+  rest += Cl * r;
+  rest += Sl * cmh;
+  rest += Cl * sm;
+  rest += t1.lo + t2.lo;
+  rest += Ch * sm;
+  s = fast_two_sum(t2.hi, rest);
+  es = j == 0 ? 0x1p-62 * fabs(s.hi) : 0x1p-67;
+  cd = Ch + (Ch * (cmh + cml) - Sh * (r + sm));
+}
+
 // correctly rounded sin(x) and cos(x), 0 <= x <= 1.125
 GP_CR_FN void sincos_cr(double x, double* sn, double* cs) {
   dd s, c;
@@ -312,13 +348,13 @@ GP_CR_FN double acos_cr(double x) {
     sl = sh > 0.0 ? fma(-sh, sh, t) / (2.0 * sh) : 0.0;
   }
   const double y0 = asin(sh);
-  dd sy, cy;
-  double es, ec;
-  sincos_fast(fabs(y0), sy, cy, es, ec);
+  dd sy;
+  double es, cy;
+  sin_fast_cos_d(fabs(y0), sy, es, cy);
   if (y0 < 0.0) sy = dd_neg(sy);
   // s - sin(y0): the high parts are within a few ulps (exact difference)
   const double e = (sh - sy.hi) + (sl - sy.lo);
-  const double delta = e / cy.hi;
+  const double delta = e / cy;
   dd y;
   double err = 1.25 * es;
   if (mid) {
