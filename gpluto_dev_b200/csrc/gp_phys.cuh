@@ -355,6 +355,12 @@ __device__ __forceinline__ void mhd_flux(const R* v, const R* u, R* f, R& pt) {
   f[MXn] += pt;
 }
 
+// Total pressure of mhd_flux (the same expression, so the same value)
+template <typename R>
+__device__ __forceinline__ R mhd_ptot(const R* v) {
+  return v[7] + R(0.5) * (v[BX1] * v[BX1] + v[BX2] * v[BX2] + v[BX3] * v[BX3]);
+}
+
 // Src/MHD/mhd.hpp:241-277 with a^2 = gamma p/rho (Src/eos.hpp:96)
 template <int DIR, typename R>
 __device__ __forceinline__ void mhd_signal_speed(const R* v, R a2, R& cmin, R& cmax) {
@@ -452,7 +458,7 @@ __device__ __forceinline__ R mhd_hlld(const R* vl, const R* vr, R* flux, R gamma
   constexpr int VXn = VX1 + DIR, VXt = VX1 + (DIR + 1) % 3, VXb = VX1 + (DIR + 2) % 3;
   constexpr int MXn = MX1 + DIR, MXt = MX1 + (DIR + 1) % 3, MXb = MX1 + (DIR + 2) % 3;
   constexpr int BXn = BX1 + DIR, BXt = BX1 + (DIR + 1) % 3, BXb = BX1 + (DIR + 2) % 3;
-  R ul[8], ur[8], fl[8], fr[8], usl[8], usr[8];
+  R ul[8], ur[8], usl[8], usr[8];
   R Sl, Sr, ptl, ptr;
   const R gmm1 = gamma - R(1);
   mhd_prim2cons(vl, ul, gmm1);
@@ -467,8 +473,11 @@ __device__ __forceinline__ R mhd_hlld(const R* vl, const R* vr, R* flux, R gamma
     Sr = GP_MAX(sl_max, sr_max);
   }
   R cmax = GP_MAX(rabs(Sl), rabs(Sr));
-  mhd_flux<DIR>(vl, ul, fl, ptl);
-  mhd_flux<DIR>(vr, ur, fr, ptr);
+  // The physical fluxes are formed where a region's flux uses them (one
+  // side outside the HLL fallback), so they are not live across the star
+  // states; every value is the one the reference computes up front.
+  ptl = mhd_ptot(vl);
+  ptr = mhd_ptot(vr);
 
   R dul, dur, Bx, Bx1, sBx, pts, SM;
   {
@@ -491,12 +500,11 @@ __device__ __forceinline__ R mhd_hlld(const R* vl, const R* vr, R* flux, R gamma
   R S1L = SM - rabs(Bx) / sqrL;
   R S1R = SM + rabs(Bx) / sqrR;
 
+  R pt_;
   if (Sl >= R(0)) {
-#pragma unroll
-    for (int nv = 0; nv < 8; nv++) flux[nv] = fl[nv];
+    mhd_flux<DIR>(vl, ul, flux, pt_);
   } else if (Sr <= R(0)) {
-#pragma unroll
-    for (int nv = 0; nv < 8; nv++) flux[nv] = fr[nv];
+    mhd_flux<DIR>(vr, ur, flux, pt_);
   } else if (!switch_to_hll) {
     int switch_to_hllc = 0;
     if ((S1L - Sl) < R(1.e-4) * (SM - Sl)) switch_to_hllc = 1;
@@ -513,8 +521,13 @@ __device__ __forceinline__ R mhd_hlld(const R* vl, const R* vr, R* flux, R gamma
       usr[BXb] = ur[BXb] * scrhR;
     } else {
       R scrh = R(1) / (Sr - Sl);
-      R Ut = (Sr * ur[BXt] - Sl * ul[BXt] + fl[BXt] - fr[BXt]) * scrh;
-      R Ub = (Sr * ur[BXb] - Sl * ul[BXb] + fl[BXb] - fr[BXb]) * scrh;
+      // mhd_flux's transverse induction components
+      const R flt = vl[BXt] * vl[VXn] - vl[BXn] * vl[VXt];
+      const R frt = vr[BXt] * vr[VXn] - vr[BXn] * vr[VXt];
+      const R flb = vl[BXb] * vl[VXn] - vl[BXn] * vl[VXb];
+      const R frb = vr[BXb] * vr[VXn] - vr[BXn] * vr[VXb];
+      R Ut = (Sr * ur[BXt] - Sl * ul[BXt] + flt - frt) * scrh;
+      R Ub = (Sr * ur[BXb] - Sl * ul[BXb] + flb - frb) * scrh;
       usl[BXn] = usr[BXn] = Bx1;
       usl[BXt] = usr[BXt] = Ut;
       usl[BXb] = usr[BXb] = Ub;
@@ -542,9 +555,13 @@ __device__ __forceinline__ R mhd_hlld(const R* vl, const R* vr, R* flux, R gamma
     usr[7] /= Sr - SM;
 
     if (S1L >= R(0)) {
+      R fl[8];
+      mhd_flux<DIR>(vl, ul, fl, pt_);
 #pragma unroll
       for (int nv = 0; nv < 8; nv++) flux[nv] = fl[nv] + Sl * (usl[nv] - ul[nv]);
     } else if (S1R <= R(0)) {
+      R fr[8];
+      mhd_flux<DIR>(vr, ur, fr, pt_);
 #pragma unroll
       for (int nv = 0; nv < 8; nv++) flux[nv] = fr[nv] + Sr * (usr[nv] - ur[nv]);
     } else {
@@ -575,16 +592,23 @@ __device__ __forceinline__ R mhd_hlld(const R* vl, const R* vr, R* flux, R gamma
       ussl[7] = usl[7] - sqrL * scrhL * sBx;
       ussr[7] = usr[7] + sqrR * scrhR * sBx;
       if (SM >= R(0)) {
+        R fl[8];
+        mhd_flux<DIR>(vl, ul, fl, pt_);
 #pragma unroll
         for (int nv = 0; nv < 8; nv++)
           flux[nv] = fl[nv] + S1L * (ussl[nv] - usl[nv]) + Sl * (usl[nv] - ul[nv]);
       } else {
+        R fr[8];
+        mhd_flux<DIR>(vr, ur, fr, pt_);
 #pragma unroll
         for (int nv = 0; nv < 8; nv++)
           flux[nv] = fr[nv] + S1R * (ussr[nv] - usr[nv]) + Sr * (usr[nv] - ur[nv]);
       }
     }
   } else {
+    R fl[8], fr[8];
+    mhd_flux<DIR>(vl, ul, fl, pt_);
+    mhd_flux<DIR>(vr, ur, fr, pt_);
     R scrh = R(1) / (Sr - Sl);
 #pragma unroll
     for (int nv = 0; nv < 8; nv++) {
