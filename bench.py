@@ -323,11 +323,17 @@ def mixed_error(make_solver, nsteps, st):
 
 
 def measure_e2e(make_solver, ncell, steps, ranks):
-    """End to end through the C ABI with host buffers.
+    """End to end through the C ABI with host buffers (pinned), three ways.
 
-    Per step: host (pinned) -> device upload of the full reference-layout
-    state (Uc, Vc, Vs with ghost zones, as Data holds it), one AdvanceStep,
-    device -> host download of the same arrays."""
+    The headline is the drop-in driver's loop (oracle/ref/gp_dropin.cpp
+    around the reference's Src/main.cpp:444-463): the full reference-layout
+    state (Uc, Vc, Vs with ghost zones, as Data holds it) goes up once;
+    every step is one gp_advance_step (dt from the host, gp_step_out back)
+    followed by gp_download_state of the whole state into the host arrays,
+    so that output, analysis and the log read the new state.
+    `roundtrip` also uploads the whole state before every step (Data
+    changed on the host between steps); `resident` downloads it once after
+    K steps (the loop between outputs)."""
     import torch
     from gpluto_dev_b200 import api
     se = make_solver(api.FP64)
@@ -337,56 +343,76 @@ def measure_e2e(make_solver, ncell, steps, ranks):
     hB = [torch.empty(f, dtype=torch.float64, pin_memory=True) for f in fshapes]
     hB += [None] * (3 - len(hB))
     L = api.lib()
+    out = api.GpStepOut()
+
+    def up():
+        api._check(L.gp_upload_state(se._h, api.LAYOUT_REFERENCE, api._dp(hU), api._dp(hV),
+                                     api._dp(hB[0]), api._dp(hB[1]), api._dp(hB[2])))
 
     def dl():
         api._check(L.gp_download_state(se._h, api.LAYOUT_REFERENCE, api._dp(hU), api._dp(hV),
                                        api._dp(hB[0]), api._dp(hB[1]), api._dp(hB[2])))
 
+    def timed(fn):
+        torch.cuda.synchronize()
+        ranks.barrier()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return ranks.max_over_ranks(time.perf_counter() - t0)
+
     dl()
-    k = max(1, min(steps, 10))
-    de = FIRST_DT
-    torch.cuda.synchronize()
-    ranks.barrier()
-    t0 = time.perf_counter()
-    for _ in range(k):
-        api._check(L.gp_upload_state(se._h, api.LAYOUT_REFERENCE, api._dp(hU), api._dp(hV),
-                                     api._dp(hB[0]), api._dp(hB[1]), api._dp(hB[2])))
-        o = se.AdvanceStep(de)
-        de = api.NextTimeStep(o.invDt_hyp, 0.4, 1.1, de)
-        dl()
-    torch.cuda.synchronize()
-    te = time.perf_counter() - t0
-    te = ranks.max_over_ranks(te)
     nbytes = (hU.numel() + hV.numel() + sum(b.numel() for b in hB if b is not None)) * 8
-    # resident use: the state goes up once and comes back
-    # once; every step is one gp_advance_step whose gp_step_out (error bits,
-    # invDt_hyp, next dt) the host reads -- all inside the timed region
-    kr = max(1, steps)
-    out = api.GpStepOut()
-    torch.cuda.synchronize()
-    ranks.barrier()
-    t0 = time.perf_counter()
-    api._check(L.gp_upload_state(se._h, api.LAYOUT_REFERENCE, api._dp(hU), api._dp(hV),
-                                 api._dp(hB[0]), api._dp(hB[1]), api._dp(hB[2])))
-    de = FIRST_DT
-    for _ in range(kr):
-        api._check(L.gp_advance_step(se._h, de, ctypes.byref(out)))
-        de = out.dt_next
-    dl()
-    torch.cuda.synchronize()
-    tr = ranks.max_over_ranks(time.perf_counter() - t0)
+    so = ctypes.sizeof(out)
+
+    k = max(1, steps)   # drop-in loop
+
+    def dropin():
+        up()
+        de = FIRST_DT
+        for _ in range(k):
+            api._check(L.gp_advance_step(se._h, de, ctypes.byref(out)))
+            de = out.dt_next
+            dl()
+    td = timed(dropin)
+
+    kt = max(1, min(steps, 10))   # whole state both ways every step
+
+    def roundtrip():
+        de = FIRST_DT
+        for _ in range(kt):
+            up()
+            api._check(L.gp_advance_step(se._h, de, ctypes.byref(out)))
+            de = out.dt_next
+            dl()
+    tt = timed(roundtrip)
+
+    def resident():
+        up()
+        de = FIRST_DT
+        for _ in range(k):
+            api._check(L.gp_advance_step(se._h, de, ctypes.byref(out)))
+            de = out.dt_next
+        dl()
+    tr = timed(resident)
     se.close()
-    return {"value": ranks.world * ncell * k / te / 1e6, "unit": METRIC,
-            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": k,
-            "path": "gp_upload_state(reference layout, pinned host) + gp_advance_step + "
-                    "gp_download_state(reference layout) per step",
-            "resident": {"value": ranks.world * ncell * kr / tr / 1e6, "unit": METRIC,
-                         "steps": kr, "h2d_bytes_per_step": nbytes / kr + 8,
-                         "d2h_bytes_per_step": nbytes / kr + ctypes.sizeof(out),
+    return {"value": ranks.world * ncell * k / td / 1e6, "unit": METRIC,
+            "h2d_bytes_per_step": nbytes / k + 8, "d2h_bytes_per_step": nbytes + so,
+            "steps": k,
+            "path": "state up once (gp_upload_state, reference layout, pinned host); per "
+                    "step gp_advance_step (dt in, gp_step_out back) + gp_download_state "
+                    "(reference layout) into the host Data arrays: the drop-in driver's loop",
+            "roundtrip": {"value": ranks.world * ncell * kt / tt / 1e6, "unit": METRIC,
+                          "steps": kt, "h2d_bytes_per_step": nbytes + 8,
+                          "d2h_bytes_per_step": nbytes + so,
+                          "path": "gp_upload_state + gp_advance_step + gp_download_state "
+                                  "(reference layout, pinned host) every step"},
+            "resident": {"value": ranks.world * ncell * k / tr / 1e6, "unit": METRIC,
+                         "steps": k, "h2d_bytes_per_step": nbytes / k + 8,
+                         "d2h_bytes_per_step": nbytes / k + so,
                          "path": "state up once (pinned, reference layout), K x "
                                  "gp_advance_step with its gp_step_out read by the host, "
-                                 "state down once; the drop-in driver's loop between "
-                                 "outputs"}}
+                                 "state down once: the drop-in loop between outputs"}}
 
 def fp64_roofline(per_kernel, top, ncell, ms_step, clocks):
     """The FP64 pipe as the roof of the FP64 form: FP64 flops per cell of
