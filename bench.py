@@ -2,7 +2,7 @@
 """Throughput of the B200 Godunov step on the 3-D 256^3 ideal-MHD blast.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload mhd3d_blast|ensemble]
+                    [--workload mhd3d_blast|ensemble|serve|rmhd]
 
 Workload (one "step" = one full RK2 step of the grid): 3-D ideal MHD, 256^3
 periodic on [0,1]^3, PLM with the MC limiter, HLLD, UCT_HLLD constrained
@@ -17,9 +17,11 @@ collective); value = zone updates of all ranks / max-over-ranks time.
 
 The default line also carries the CPU baseline (the reference serial build,
 one thread, on this same 256^3 grid: one timed step after one untimed, run
-beside the GPU measurements) and two short legs of the other workloads: the
-batched ensemble (all 512 grids, K steps) and the serving loop (64 requests
-at 8 requests/s: p50/p99 latency and Mzone-updates/s).
+beside the GPU measurements), the end-to-end rate through the C ABI with
+host buffers in the drop-in driver's loop, and three short legs of the
+other workloads: the batched ensemble (all 512 grids, K steps), the serving
+loop (64 requests at 8 requests/s: p50/p99 latency and Mzone-updates/s) and
+the 3-D RMHD 192^3 grid (FP64 and mixed, min(K, 10) steps).
 
 ``--impl reference`` times the reference gPLUTO serial build (compiled from
 the reference sources into oracle/_ref by __graft_entry__.build()) on this
@@ -556,14 +558,11 @@ def impl_ours(args):
     if mixed is not None:
         mixed["error_vs_fp64"] = mixed_error(solver, args.error_steps, st)
 
-    # ---- end to end through the C ABI with host buffers ------------------
-    # Per step: host (pinned) -> device upload of the full reference-layout
-    # state (Uc, Vc, Vs with ghost zones, as Data holds it), one AdvanceStep,
-    # device -> host download of the same arrays.
+    # ---- end to end through the C ABI with host buffers (measure_e2e) ----
     e2e = None if args.no_e2e else measure_e2e(solver, ncell, args.steps, ranks)
 
-    # ---- the other two workloads, short: the batched ensemble (all 512
-    # grids, K steps) and the serving loop (64 requests at one rate) -------
+    # ---- the other workloads, short: the batched ensemble (all 512 grids,
+    # K steps), the serving loop (64 requests at one rate) and RMHD 192^3 ---
     legs = {}
     if world == 1 and not args.no_legs:
         s64 = None
@@ -578,6 +577,8 @@ def impl_ours(args):
         sweep, table, _, work = serve_leg(args, [SERVE_DEFAULT_RATE], args.requests)
         legs["serve"] = dict(sweep[0], workload=f"serve_poisson_{args.requests}req",
                              work_zone_updates=work)
+        torch.cuda.empty_cache()
+        legs["rmhd"] = rmhd_leg(min(args.steps, 10), 3)
 
     cpu = None
     if want_cpu:
@@ -855,14 +856,12 @@ RMHD_ALG_BYTES_ZONE = 696   # 440 + 4 x 64: the stored primitives read and writt
 REF_BINARY_RMHD = os.path.join(ROOT, "oracle", "_ref", "rmhd3d_mc_lim_hlld_uct_hll", "pluto")
 
 
-def impl_rmhd(args):
+def rmhd_forms(n, steps, warmup, clock=None, profile=True):
+    """The RMHD n^3 workload's FP64 and mixed forms, each timed over `steps`
+    RK2 steps after `warmup` (CUDA events on the library's stream).  Returns
+    (forms, state, solver factory, clocks sampled during the FP64 steps)."""
     import torch
     from gpluto_dev_b200 import api, ics
-
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    if int(os.environ.get("RANK", "0")) != 0:
-        return 0
-    n = args.n if args.n != N else RMHD_N
     st = ics.rmhd3d_turbulence(n=(n, n, n), seed=1)
     ncell = n ** 3
 
@@ -872,30 +871,54 @@ def impl_rmhd(args):
         return api.Solver.from_state(st, sch)
 
     forms = {}
-    clock = ClockSampler(0)
     clocks = None
     for prec, name in ((api.FP64, "fp64"), (api.MIXED, "mixed")):
         s = solver(prec)
-        dt, _, _ = s.run(args.warmup, 1e-4, history=False)
+        dt, _, _ = s.run(warmup, 1e-4, history=False)
         torch.cuda.synchronize()
-        if name == "fp64":
+        if name == "fp64" and clock is not None:
             clock.start()
             time.sleep(0.25)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        _, _, out = s.run(args.steps, dt, history=False)
+        _, _, out = s.run(steps, dt, history=False)
         e1.record()
         torch.cuda.synchronize()
-        if name == "fp64":
+        if name == "fp64" and clock is not None:
             clocks = clock.stop()
-        ms = e0.elapsed_time(e1) / args.steps
-        prof, _ = s.profile(2, dt)
-        forms[name] = {"value": ncell / ms / 1e3, "ms_per_step": ms, "err_bits": out.err_bits,
-                       "kernels": [{"kernel": k, "stage": g, "ms": t} for k, g, t in prof]}
+        ms = e0.elapsed_time(e1) / steps
+        forms[name] = {"value": ncell / ms / 1e3, "ms_per_step": ms, "err_bits": out.err_bits}
+        if profile:
+            prof, _ = s.profile(2, dt)
+            forms[name]["kernels"] = [{"kernel": k, "stage": g, "ms": t} for k, g, t in prof]
         s.close()
         del s
         torch.cuda.empty_cache()
     forms["mixed"]["speedup_vs_fp64"] = forms["mixed"]["value"] / forms["fp64"]["value"]
+    return forms, st, solver, clocks
+
+
+def rmhd_leg(steps, warmup):
+    """Short RMHD leg of the default line: the 192^3 workload's two forms."""
+    forms, _, _, _ = rmhd_forms(RMHD_N, steps, warmup, profile=False)
+    return {"value": forms["fp64"]["value"], "unit": METRIC, "steps": steps,
+            "ms_per_step": forms["fp64"]["ms_per_step"], "err_bits": forms["fp64"]["err_bits"],
+            "mixed": {k: forms["mixed"][k] for k in ("value", "ms_per_step", "speedup_vs_fp64",
+                                                     "err_bits")},
+            "workload": f"3d_rmhd_{RMHD_N}^3",
+            "scheme": "PLM-MC + RMHD HLLD + UCT_HLL + RK2, CFL 0.3, gamma 4/3"}
+
+
+def impl_rmhd(args):
+    import torch
+    from gpluto_dev_b200 import api, ics
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    n = args.n if args.n != N else RMHD_N
+    ncell = n ** 3
+    forms, st, solver, clocks = rmhd_forms(n, args.steps, args.warmup, ClockSampler(0))
     # error of the mixed form against FP64 after 100 steps on FP64's dt sequence
     a = solver(api.FP64)
     _, hist, _ = a.run(args.error_steps, 1e-4)
