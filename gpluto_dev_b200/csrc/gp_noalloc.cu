@@ -132,7 +132,7 @@ extern "C" int gp_advance_step_noalloc(const gp_grid_desc* grid, const gp_scheme
   hs.dt = dt;
   for (int d = 0; d < 3; d++) hs.dtdx[d] = dt / dx[d];
   if (cudaMemcpyAsync(sc, &hs, sizeof(hs), cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return GP_ERR_CUDA;
+    return gp::set_last_error(GP_ERR_CUDA, "cannot write the step scalars");
 
   gp::StageDesc d;
   std::memset(&d, 0, sizeof(d));
@@ -191,12 +191,13 @@ extern "C" int gp_advance_step_noalloc(const gp_grid_desc* grid, const gp_scheme
     for (int q = 0; q < ndim; q++)
       if (cudaMemcpyAsync(Bn[q], B2[q], sizeof(double) * n, cudaMemcpyDeviceToDevice, s) !=
           cudaSuccess)
-        return GP_ERR_CUDA;
+        return gp::set_last_error(GP_ERR_CUDA, "cannot copy the new face field back");
   // launch failures show here; peeking leaves the thread's error state as it is
   if (cudaPeekAtLastError() != cudaSuccess) return gp::set_last_error(GP_ERR_CUDA, "launch failed");
   if (cudaMemcpyAsync(&hs, sc, sizeof(hs), cudaMemcpyDeviceToHost, s) != cudaSuccess)
-    return GP_ERR_CUDA;
-  if (cudaStreamSynchronize(s) != cudaSuccess) return GP_ERR_CUDA;
+    return gp::set_last_error(GP_ERR_CUDA, "cannot read the step scalars");
+  if (cudaStreamSynchronize(s) != cudaSuccess)
+    return gp::set_last_error(GP_ERR_CUDA, "the step failed on the device");
   // invDt_hyp = max(C_dt)/dim (Src/update_stage.cpp:422-435), NextTimeStep
   double inv;
   std::memcpy(&inv, &hs.invdt_bits, sizeof(inv));
