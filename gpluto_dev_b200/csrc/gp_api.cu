@@ -766,13 +766,34 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
                          : scheme->reconstruction == GP_REC_LIMO3   ? 10  /* LIM_LIMO3 */
                          : scheme->reconstruction == GP_REC_WENO3   ? 11  /* LIM_WENO3 */
                                                                     : scheme->limiter};
-  // pencil segment for the marching sweeps: enough threads to fill 148 SMs
+  // pencil segment for the marching sweeps: enough threads to fill 148 SMs,
+  // then, among that length and its halves down to a quarter, the one whose
+  // y and z sweeps take the fewest (waves of resident blocks) x (cells a
+  // block marches, + 2 for its start-up): a last wave that fills few SMs
+  // costs a whole wave.  At 256^3 the FP64 sweeps (4 blocks per SM) take
+  // 32 (y/z 1.33 -> 1.29 ms against 64), the mixed ones (5 per SM) keep 64.
   {
     long long cols = (long long)h->px * (h->ndim == 3 ? h->pz : 1);
     int nd = h->py;
     int seg = 64;
     while (seg > 4 && cols * ((nd + seg - 1) / seg) < 148LL * 1024) seg /= 2;
-    h->seg = seg;
+    const long long resident =
+        148LL * gp::sweep_m_blocks_per_sm(scheme->physics, h->mixed);
+    const long long bx = (h->px + 127) / 128;   // SWEEP_THREADS columns per block
+    auto cost = [&](int S) {
+      long long c = 0;
+      const long long by = bx * (h->ndim == 3 ? h->pz : 1) * ((h->py + S - 1) / S);
+      c += (by + resident - 1) / resident * (S + 2);
+      if (h->ndim == 3) {
+        const long long bz = bx * h->py * ((h->pz + S - 1) / S);
+        c += (bz + resident - 1) / resident * (S + 2);
+      }
+      return c;
+    };
+    int best = seg;
+    for (int S = seg / 2; S >= 4 && S >= seg / 4; S /= 2)
+      if (cost(S) < cost(best)) best = S;
+    h->seg = best;
   }
   const size_t cell = sizeof(double) * h->pn;
   const size_t ctb = (h->mixed ? sizeof(float) : sizeof(double)) * h->pn;

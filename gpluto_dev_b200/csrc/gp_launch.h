@@ -55,6 +55,10 @@ int launch_prim2cons(int physics, const double* V, double* U, long long n, doubl
 // Sets the text returned by gp_last_error on this thread; returns `code`.
 int set_last_error(int code, const char* msg);
 
+// Resident blocks per SM the y/z marching sweeps are compiled for
+// (SWEEP_THREADS threads each).
+int sweep_m_blocks_per_sm(int physics, bool mixed);
+
 // Number of kernel launches one stage issues for this scheme, and their names.
 int stage_launch_count(const SchemeKey& k);
 const char* stage_kernel_name(const SchemeKey& k, int idx);

@@ -1,8 +1,17 @@
 // gp_launch_dispatch.cu -- joins the per-physics launch units of
 // gp_launch.cu (compiled once per form and physics, GP_MIXED x GP_PART).
+#include "gp_kernels.cuh"
 #include "gp_launch.h"
 
 namespace gp {
+
+int sweep_m_blocks_per_sm(int physics, bool mixed) {
+  if (physics == PHYS_RMHD)
+    return mixed ? sweep_m_minb<PHYS_RMHD, float>() : sweep_m_minb<PHYS_RMHD, double>();
+  if (physics == PHYS_MHD)
+    return mixed ? sweep_m_minb<PHYS_MHD, float>() : sweep_m_minb<PHYS_MHD, double>();
+  return mixed ? sweep_m_minb<PHYS_HD, float>() : sweep_m_minb<PHYS_HD, double>();
+}
 
 #define GP_PART_DECL(name)                                                              \
   int name(const StageDesc& d, const GridDims& g, const SchemeKey& k, int seg,         \
