@@ -779,13 +779,15 @@ int gp_create(const gp_grid_desc* grid, const gp_scheme* scheme, void* stream,
     while (seg > 4 && cols * ((nd + seg - 1) / seg) < 148LL * 1024) seg /= 2;
     const long long resident =
         148LL * gp::sweep_m_blocks_per_sm(scheme->physics, h->mixed);
-    const long long bx = (h->px + 127) / 128;   // SWEEP_THREADS columns per block
+    // blocks of SWEEP_THREADS (128) columns, x and transverse taken together
+    const long long cy = ((long long)h->px * (h->ndim == 3 ? h->pz : 1) + 127) / 128;
+    const long long cz = ((long long)h->px * h->py + 127) / 128;
     auto cost = [&](int S) {
       long long c = 0;
-      const long long by = bx * (h->ndim == 3 ? h->pz : 1) * ((h->py + S - 1) / S);
+      const long long by = cy * ((h->py + S - 1) / S);
       c += (by + resident - 1) / resident * (S + 2);
       if (h->ndim == 3) {
-        const long long bz = bx * h->py * ((h->pz + S - 1) / S);
+        const long long bz = cz * ((h->pz + S - 1) / S);
         c += (bz + resident - 1) / resident * (S + 2);
       }
       return c;

@@ -1096,16 +1096,32 @@ __device__ __forceinline__ void sweep_m_col(const StageArgs<CTT>& a, const Grid3
   if (err) atomicOr(a.err, err);
 }
 
+// t is the transverse index (k for DIR=1, j for DIR=2).  FLAT = false:
+// grid (x-blocks, t * nseg + seg), the block's columns share one t.  FLAT =
+// true (nx not a multiple of the block): a 1-D grid of (column block cb,
+// segment) pairs, segments innermost, with the (x, t) columns numbered
+// together (col = cb * SWEEP_THREADS + thread, i = col % nx, t = col / nx),
+// so that no block is part-empty.
 template <int PHYS, int NV, int NDIM, int RS, int CT, int LIM, int DIR, typename R,
-          typename CTT>
+          typename CTT, bool FLAT>
 __global__ void __launch_bounds__(SWEEP_THREADS, (sweep_m_minb<PHYS, R>()))
     sweep_m_kernel(StageArgs<CTT> a, Grid3 g, int S) {
   __shared__ double stg[sweep_m_stage_doubles<NV>()];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int nd = (DIR == 1) ? g.ny : g.nz;
   const int nseg = (nd + S - 1) / S;
-  const int t = blockIdx.y / nseg;
-  const int seg = blockIdx.y - t * nseg;
+  int i, t, seg;
+  if constexpr (FLAT) {
+    const int nt = (DIR == 1) ? g.nz : g.ny;
+    seg = (int)(blockIdx.x % (unsigned)nseg);
+    const int col = (int)(blockIdx.x / (unsigned)nseg) * SWEEP_THREADS + (int)threadIdx.x;
+    i = col % g.nx;
+    t = col / g.nx;
+    if (t >= nt) i = g.nx;   // past the last column: the thread stays idle
+  } else {
+    i = blockIdx.x * SWEEP_THREADS + threadIdx.x;
+    t = blockIdx.y / nseg;
+    seg = blockIdx.y - t * nseg;
+  }
   sweep_m_col<PHYS, NV, NDIM, RS, CT, LIM, DIR, R, CTT>(a, g, i, t, seg, S, stg, threadIdx.x);
 }
 

@@ -86,18 +86,31 @@ static void run_stage(const StageArgs<CTT>& a, const GridDims& gd, int seg, cuda
     sweep_x_kernel<PHYS, NV, NDIM, RS, CT, LIM, RT, CTT><<<grid, SWEEP_THREADS, 0, s>>>(a, g);
     post();
   }
+  // y/z sweeps: grid (x-blocks, transverse index x pencil segments); when
+  // nx is not a multiple of the block, a 1-D grid over (x, transverse)
+  // columns numbered together, so that no block is part-empty (FLAT)
+  const bool flat = gd.nx % SWEEP_THREADS != 0;
+  auto grid_m = [&](int nt, int nseg) {
+    if (flat)
+      return dim3((unsigned)(((long long)gd.nx * nt + SWEEP_THREADS - 1) / SWEEP_THREADS * nseg));
+    return dim3(gd.nx / SWEEP_THREADS, nt * nseg);
+  };
   {
-    const int nseg = (gd.ny + seg - 1) / seg;
-    dim3 grid((gd.nx + SWEEP_THREADS - 1) / SWEEP_THREADS, gd.nz * nseg);
+    const dim3 grid = grid_m(gd.nz, (gd.ny + seg - 1) / seg);
     pre();
-    sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 1, RT, CTT><<<grid, SWEEP_THREADS, 0, s>>>(a, g, seg);
+    if (flat)
+      sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 1, RT, CTT, true><<<grid, SWEEP_THREADS, 0, s>>>(a, g, seg);
+    else
+      sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 1, RT, CTT, false><<<grid, SWEEP_THREADS, 0, s>>>(a, g, seg);
     post();
   }
   if constexpr (NDIM == 3) {
-    const int nseg = (gd.nz + seg - 1) / seg;
-    dim3 grid((gd.nx + SWEEP_THREADS - 1) / SWEEP_THREADS, gd.ny * nseg);
+    const dim3 grid = grid_m(gd.ny, (gd.nz + seg - 1) / seg);
     pre();
-    sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 2, RT, CTT><<<grid, SWEEP_THREADS, 0, s>>>(a, g, seg);
+    if (flat)
+      sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 2, RT, CTT, true><<<grid, SWEEP_THREADS, 0, s>>>(a, g, seg);
+    else
+      sweep_m_kernel<PHYS, NV, NDIM, RS, CT, LIM, 2, RT, CTT, false><<<grid, SWEEP_THREADS, 0, s>>>(a, g, seg);
     post();
   }
   const unsigned nb = (unsigned)((gd.n + 255) / 256);
