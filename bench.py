@@ -68,14 +68,17 @@ ALG_BYTES_ZONE = 440
 # it must read and write once, 8 B each), indexed by (kernel, stage):
 #   sweep  V(8) + Bs_n(1) -> dU_dir(5) + C_dir(1) + UCT(6)            21 x 8
 #   emf    UCT(18) + Bs(3) -> Ee(3)                                    24 x 8
-#   finish dU(15) + [C(3), stage 1 only] + U0(5) [+ Uc(5)] + Ee(3) + Bs(3)
-#          [+ Bs0(3)] -> Bs'(3) + U(8) + V(8)                 48 x 8 [53 x 8]
+#   finish stage 1: dU(15) + C(3) + U0(5) + Ee(3) + Bs(3)
+#          -> Bs'(3) + U(5: the field components of the intermediate state
+#          are never read, so not stored) + V(8)                        45 x 8
+#   finish stage 2: dU(15) + U0(5) + Uc(5) + Ee(3) + Bs(3) + Bs0(3)
+#          -> Bs'(3) + U(8) + V(8)                                      53 x 8
 KERNEL_BYTES = {
     ("sweep_x", 1): 168, ("sweep_x", 2): 168,
     ("sweep_y", 1): 168, ("sweep_y", 2): 168,
     ("sweep_z", 1): 168, ("sweep_z", 2): 168,
     ("emf", 1): 192, ("emf", 2): 192,
-    ("finish", 1): 384, ("finish", 2): 424,
+    ("finish", 1): 360, ("finish", 2): 424,
 }
 # the same for the mixed form, whose flux differences, inverse-dt terms, UCT
 # data and edge EMFs are 4-byte floats (state, faces and V stay 8 bytes)
