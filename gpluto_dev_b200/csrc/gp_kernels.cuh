@@ -120,10 +120,13 @@ constexpr int SWEEP_THREADS = 128;
 // Resident 128-thread blocks per SM the sweep kernels are compiled for
 // (register budget 65536 / (128 * blocks)), measured at 256^3 on 3-D MHD:
 // FP64 x-sweep 3 (168 registers), FP64 y/z sweeps 4 (128), mixed form 5
-// (102); the relativistic solver (FP64 in both forms) keeps 3.
+// (102).  The relativistic solver (FP64 in both forms) runs its x-sweep at
+// 2 (5.01 -> 4.83 ms FP64, 4.33 -> 4.06 ms mixed at 192^3: fewer warps
+// walking its long code at once) and its y/z sweeps at 3 (at 2 they lost
+// 4%).
 template <int PHYS, typename R>
 constexpr int sweep_x_minb() {
-  return PHYS == PHYS_RMHD ? 3 : (sizeof(R) == 4 ? 5 : 3);
+  return PHYS == PHYS_RMHD ? 2 : (sizeof(R) == 4 ? 5 : 3);
 }
 template <int PHYS, typename R>
 constexpr int sweep_m_minb() {
